@@ -1,0 +1,372 @@
+"""Benchmark: LMM association SNPs/s at n = 20,000 samples, all tests (-lmm 4).
+
+One step = the association hot path over one chunk of SNPs of a resident cohort:
+device decode of packed .bed records -> mean imputation -> eigenvector rotation ->
+per-SNP Score / MLE+LRT / REML+Wald search and statistics.  The cohort's kinship and
+eigendecomposition are set-up work, timed and reported separately (kinship_s, eigh_s).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs its own shard of SNP chunks of a replica cohort (weak
+scaling, no data-path collective); the timed region is bracketed by barriers and the
+max over ranks is reported.  ``--impl reference`` times the CPU oracle (jamma's path
+restated in NumPy/SciPy) on a bounded sample of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+HBM_PEAK_FALLBACK = 6650.0
+
+
+def _peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return json.loads(p.read_text())
+    return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled while the timed region runs."""
+
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows: list[list[str]] = []
+        self._stop = threading.Event()
+        self._t = threading.Thread(target=self._run, daemon=True)
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True,
+                                     text=True, timeout=5).stdout.strip()
+                if out:
+                    self.rows.append([c.strip() for c in out.split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t.start()
+        return self
+
+    def __exit__(self, *exc):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self) -> dict:
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4)
+                          if len(r) > k + 2 and r[k + 2].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(self.rows)}
+
+
+def _dist():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args) -> None:
+    """CPU arm: the oracle (jamma's JAX path restated in NumPy) on a bounded sample."""
+    world, rank, _ = _dist()
+    if rank != 0:
+        return
+    from threadpoolctl import threadpool_info
+
+    from oracle import lmm as OL
+
+    n, m, c = args.n, args.ref_snps, args.n_cvt
+    rng = np.random.default_rng(20261203)
+    t0 = time.perf_counter()
+    # cohort of the same shape: kinship from a SNP sample, FP64 eigh (set-up, not timed)
+    gk = rng.binomial(2, rng.uniform(0.05, 0.5, 2000), size=(n, 2000)).astype(np.float64)
+    gk -= gk.mean(0)
+    K = gk @ gk.T / 2000
+    evals, U = OL.eigh_threshold(K)
+    W = np.column_stack([np.ones(n), rng.normal(size=(n, c - 1))])
+    y = rng.normal(size=n)
+    UT = np.ascontiguousarray(U.T)
+    UtW, Uty = UT @ W, UT @ y
+    lam0, l0 = OL.null_model_mle(evals, UtW, Uty)
+    setup_s = time.perf_counter() - t0
+    per_step = []
+    for it in range(args.warmup + args.steps):
+        g = rng.binomial(2, rng.uniform(0.05, 0.5, m), size=(n, m)).astype(np.float64)
+        g[rng.random((n, m)) < args.miss] = np.nan
+        t = time.perf_counter()
+        mu = np.nanmean(g.astype(np.float32), 0).astype(np.float64)
+        g = np.where(np.isnan(g), mu[None, :], g)
+        OL.lmm_chunk(args.mode, evals, UtW, Uty, UT @ g, l0, lam0)
+        if it >= args.warmup:
+            per_step.append(time.perf_counter() - t)
+    sec = float(np.mean(per_step))
+    value = m / sec
+    cores = max([i.get("num_threads", 0) for i in threadpool_info() if i.get("user_api") == "blas"] or [1])
+    line = {
+        "impl": "reference", "metric": "lmm_assoc_snps_per_s", "value": value, "unit": "SNPs/s",
+        "n_gpus": 0, "steps": args.steps, "warmup": args.warmup, "ms_per_step": sec * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": _config(args, per_step_snps=m),
+        "cpu_baseline": {"value": value, "unit": "SNPs/s", "cores": cores, "kind": "port",
+                         "sample": f"{m} SNPs per step at n={n}, c={c}, -lmm {args.mode}; "
+                                   f"set-up (eigh n={n}) {setup_s:.1f}s untimed"},
+        "e2e": {"value": value, "unit": "SNPs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def _config(args, per_step_snps) -> dict:
+    return {"workload": f"lmm -lmm {args.mode} n={args.n} c={args.n_cvt} phenotypes=1, "
+                        f"{per_step_snps} SNPs per step, {args.miss:.0%} missing calls",
+            "n_samples": args.n, "n_cvt": args.n_cvt, "lmm_mode": args.mode,
+            "snps_per_step": per_step_snps, "precision": args.precision,
+            "l2": "inputs > L2 (each step's imputed FP64 chunk is n*m*8 bytes)",
+            "parallelism": f"replicas{_dist()[0]}"}
+
+
+def _cpu_baseline(args, cohort, evals_h, U_h, UtW_h, Uty_h, lam0, l0) -> dict:
+    """Oracle timed on the host over a bounded sample of the same workload."""
+    from threadpoolctl import threadpool_info
+
+    from oracle import lmm as OL
+
+    m = args.cpu_snps
+    rng = np.random.default_rng(7)
+    g = rng.binomial(2, rng.uniform(0.05, 0.5, m), size=(args.n, m)).astype(np.float64)
+    t = time.perf_counter()
+    OL.lmm_chunk(args.mode, evals_h, UtW_h, Uty_h, U_h.T @ g, l0, lam0)
+    sec = time.perf_counter() - t
+    cores = max([i.get("num_threads", 0) for i in threadpool_info() if i.get("user_api") == "blas"] or [1])
+    return {"value": m / sec, "unit": "SNPs/s", "cores": cores, "kind": "port",
+            "sample": f"{m} SNPs at n={args.n} (rotation on host BLAS + NumPy search, -lmm {args.mode})"}
+
+
+def run_ours(args) -> None:
+    import torch
+    import torch.distributed as dist
+
+    world, rank, local = _dist()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    from jamma_b200 import _build
+
+    if rank == 0:
+        _build.build()
+    if world > 1:
+        dist.barrier()
+    from jamma_b200 import _native, engine as eng, synth
+    from jamma_b200.device import ptr, stream_handle
+    from jamma_b200.kinship import _KinshipAccumulator, snp_stats_from_counts
+
+    n, m, c = args.n, args.chunk, args.n_cvt
+    nsteps = args.warmup + args.steps
+    bps = (n + 3) // 4
+    st = torch.cuda.current_stream()
+
+    # ---------------- cohort set-up: kinship (FP64 Gram) + eigh, timed separately
+    kin_p = args.kin_snps
+    kin_rec = synth.packed_records_device(n, kin_p, args.miss, seed=100 + rank)
+    torch.cuda.synchronize()
+    t = time.perf_counter()
+    acc = _KinshipAccumulator(n, 4096)
+    for s in range(0, kin_p, 16384):
+        codes, cnt = eng.decode_packed(kin_rec[s:s + 16384], n, None, n)
+        cc = cnt.cpu().numpy()
+        poly = snp_stats_from_counts(cc, n)[2]
+        idx = torch.from_numpy(np.where(poly)[0]).cuda()
+        mu = torch.from_numpy(cc[:, 1] / np.maximum(cc[:, 0], 1)).cuda().index_select(0, idx)
+        acc.add(codes.index_select(0, idx), mu)
+    K = acc.finish()
+    torch.cuda.synchronize()
+    kinship_s = time.perf_counter() - t
+    del kin_rec
+    t = time.perf_counter()
+    w, U = eng.eigh_device(K)
+    torch.cuda.synchronize()
+    eigh_s = time.perf_counter() - t
+    rng = np.random.default_rng(5)
+    W = np.column_stack([np.ones(n), rng.normal(size=(n, c - 1))])
+    y = rng.normal(size=n)
+    cohort = eng.DeviceCohort(w, U, W, y, lmm_mode=args.mode)
+
+    # ---------------- SNP chunks (device-resident packed records + pass-1 means)
+    rec = synth.packed_records_device(n, nsteps * m, args.miss, seed=1000 + rank)
+    means = []
+    for s in range(nsteps):
+        _, cnt = eng.decode_packed(rec[s * m:(s + 1) * m], n, None, n)
+        cc = cnt.cpu().numpy().astype(np.float64)
+        means.append(torch.from_numpy((cc[:, 1] / np.maximum(cc[:, 0], 1)).astype(np.float32)
+                                      .astype(np.float64)).cuda())
+    bufs = {"G": eng.empty((m, n)), "UtG": eng.empty((m, n))}
+    outs = cohort.alloc_out(m)
+    codes = torch.empty((m, n), dtype=torch.int8, device="cuda")
+    counts = torch.empty((m, 4), dtype=torch.int32, device="cuda")
+
+    ev = {k: [] for k in ("decode", "impute", "rotate", "lmm")}
+
+    def step(s, record=False):
+        def mark():
+            e = torch.cuda.Event(enable_timing=True)
+            e.record(st)
+            return e
+        e0 = mark()
+        _native.call("jb_decode_bed", ptr(rec[s * m:(s + 1) * m]), bps, m, None, n, ptr(codes), n,
+                     ptr(counts), stream_handle())
+        e1 = mark()
+        _native.call("jb_impute_f64", ptr(codes), n, n, m, ptr(means[s]), ptr(bufs["G"]), n,
+                     stream_handle())
+        e2 = mark()
+        eng.rotate(cohort.U, bufs["G"], out=bufs["UtG"])
+        e3 = mark()
+        cohort.associate_rotated(bufs["UtG"], outs)
+        e4 = mark()
+        if record:
+            for k, a, b in (("decode", e0, e1), ("impute", e1, e2), ("rotate", e2, e3), ("lmm", e3, e4)):
+                ev[k].append((a, b))
+
+    for s in range(args.warmup):
+        step(s)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        start.record(st)
+        for s in range(args.warmup, nsteps):
+            step(s, record=True)
+        end.record(st)
+        torch.cuda.synchronize()
+    ms = start.elapsed_time(end)
+    if world > 1:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+        dist.barrier()
+    kern_ms = {k: float(np.mean([a.elapsed_time(b) for a, b in v])) for k, v in ev.items()}
+    snps = args.steps * m * world
+    value = snps / (ms / 1e3)
+
+    # ---------------- end to end through the public chunk API with host buffers
+    rec_h = rec[:m].cpu().pin_memory()
+    mean_h = means[0].cpu()
+    res_h = {k: torch.empty((1, m), dtype=torch.float64).pin_memory() for k in outs}
+
+    def e2e_step():
+        rd = rec_h.to("cuda", non_blocking=True)
+        md = mean_h.to("cuda", non_blocking=True)
+        cd, _ = eng.decode_packed(rd, n, None, n)
+        o = cohort.associate_codes(cd, md, out=outs, bufs=bufs)
+        for k, v in o.items():
+            res_h[k].copy_(v, non_blocking=True)
+    for _ in range(2):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_steps = max(2, min(args.steps, 5))
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(st)
+    for _ in range(e2e_steps):
+        e2e_step()
+    b.record(st)
+    torch.cuda.synchronize()
+    e2e_ms = a.elapsed_time(b) / e2e_steps
+    if world > 1:
+        tt = torch.tensor([e2e_ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        e2e_ms = float(tt.item())
+
+    if rank == 0:
+        peaks = _peaks()
+        # FP64 rotation roofline (dominant kernel in the plain form): 2 n^2 m flops/step
+        rot_flops = 2.0 * n * n * m
+        fp64_peak = args.fp64_peak_tflops
+        achieved = rot_flops / (kern_ms["rotate"] / 1e3) / 1e12
+        evals_h = w.cpu().numpy()
+        U_h = U.cpu().numpy().T
+        lam0, l0 = cohort.null_model()
+        cpu = None
+        if not args.no_cpu:
+            cpu = _cpu_baseline(args, cohort, evals_h, U_h, U_h.T @ W, U_h.T @ y,
+                                float(lam0[0]) if lam0 is not None else None,
+                                float(l0[0]) if l0 is not None else None)
+        line = {
+            "metric": "lmm_assoc_snps_per_s", "value": value, "unit": "SNPs/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded device RNG; Binomial(2,p) genotypes, p~U(0.05,0.5))",
+            "config": _config(args, m),
+            "gpu_launches": 3 * args.steps,
+            "kernel_ms_per_step": kern_ms,
+            "kinship_s": kinship_s, "kinship_snps": kin_p, "eigh_s": eigh_s,
+            "roofline": {"kernel": "rotation U^T G (cuBLAS DGEMM, plain FP64 form)",
+                         "bound": "tensor", "achieved": achieved, "peak": fp64_peak,
+                         "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": None,
+                         "peak_source": "nominal B200 FP64 (no FP64 figure in MEASURED_PEAKS.json)"},
+            "search_kernel": {"kernel": "lmm_pairs_kernel (FP64 search+stats)",
+                              "ms_per_step": kern_ms["lmm"]},
+            "cpu_baseline": cpu,
+            "e2e": {"value": m / (e2e_ms / 1e3) * world, "unit": "SNPs/s",
+                    "h2d_bytes_per_step": m * bps + m * 8,
+                    "d2h_bytes_per_step": len(outs) * m * 8},
+            "clocks": clk.summary(),
+            "hbm_peak_gbs": peaks.get("hbm_gbs", HBM_PEAK_FALLBACK),
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=20000)
+    ap.add_argument("--n-cvt", type=int, default=1)
+    ap.add_argument("--mode", type=int, default=4)
+    ap.add_argument("--chunk", type=int, default=8192)
+    ap.add_argument("--miss", type=float, default=0.01)
+    ap.add_argument("--kin-snps", type=int, default=65536)
+    ap.add_argument("--precision", default="fp64", choices=["fp64"])
+    ap.add_argument("--cpu-snps", type=int, default=64)
+    ap.add_argument("--ref-snps", type=int, default=64)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--fp64-peak-tflops", type=float, default=40.0)
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

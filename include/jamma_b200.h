@@ -1,0 +1,180 @@
+/*
+ * jamma_b200.h -- C ABI of libjamma_b200.so, the sm_100a implementation of jamma's
+ * GEMMA-style LMM association hot path.
+ *
+ * Conventions
+ *   - Every entry point returns int32 status: 0 = OK, < 0 = error (JB_E_*).  The
+ *     text of the last error on the calling thread is available from jb_last_error.
+ *   - All array arguments are DEVICE pointers owned by the caller (torch tensors in
+ *     the Python host code), with explicit sizes and leading dimensions.  Matrices are
+ *     column-major ("ld" = distance between columns, in elements) unless stated.
+ *   - `stream` is a cudaStream_t passed as uintptr_t (0 = legacy default stream).
+ *     Work is enqueued asynchronously on it; nothing synchronises unless stated.
+ *   - Library-internal scratch comes from a caller-provided workspace where a function
+ *     needs one; the matching *_workspace_size query gives the byte count.
+ *
+ * Each function cites the jamma call site it replaces (paths inside the jamma
+ * project, version 2.0.1).
+ */
+#ifndef JAMMA_B200_H
+#define JAMMA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define JB_OK 0
+#define JB_E_INVALID (-1)   /* bad argument / shape */
+#define JB_E_CUDA (-2)      /* CUDA runtime error */
+#define JB_E_LIBRARY (-3)   /* cuBLAS / cuSOLVER error */
+#define JB_E_UNSUPPORTED (-4)
+#define JB_E_NUMERIC (-5)   /* eigensolver did not converge */
+
+/* Library version as MAJOR*10000 + MINOR*100 + PATCH. */
+int32_t jb_version(void);
+
+/* Copy the last error message of this thread into buf (always NUL-terminated). */
+int32_t jb_last_error(char* buf, size_t len);
+
+/* Compute capability of the current device as major*10+minor (100 for B200). */
+int32_t jb_device_arch(void);
+
+/* ------------------------------------------------------------------ genotypes */
+
+/*
+ * Decode PLINK .bed records (SNP-major, ceil(n_file/4) bytes per SNP, count-A1 codes
+ * 00->2, 01->missing, 10->1, 11->0) for m SNPs into int8 codes, keeping only the
+ * analysed samples sample_idx[0..n) (NULL = identity, n == n_file).
+ *   codes  : m x ld_codes int8, SNP-major (one row of ld_codes bytes per SNP; sample
+ *            s at [j*ld_codes + s]); value 0/1/2, or 3 for a missing call.  Entries
+ *            s in [n, ld_codes) are written as 0 (zero padding for tensor-core tiles).
+ *   counts : m x 4 int32 per SNP: {n_obs, sum of counts, n_het(=#1), n_hom2(=#2)}.
+ * Replaces bed-reader's windowed read (src/jamma/io/plink.py:299) and the pass-1
+ * statistics loop (src/jamma/lmm/runner_streaming.py:246-256).
+ */
+int32_t jb_decode_bed(const uint8_t* packed, int64_t bytes_per_snp, int64_t m,
+                      const int32_t* sample_idx, int64_t n, int8_t* codes,
+                      int64_t ld_codes, int32_t* counts, uintptr_t stream);
+
+/*
+ * Mean-impute (no centering) decoded codes into FP64 genotype columns:
+ * G[i + j*ldg] = code (0/1/2) or mean[j] where the code is 3 (missing).
+ * Replaces the imputation at src/jamma/lmm/runner_streaming.py:427-434.
+ */
+int32_t jb_impute_f64(const int8_t* codes, int64_t ld_codes, int64_t n, int64_t m,
+                      const double* mean, double* G, int64_t ldg, uintptr_t stream);
+
+/* ------------------------------------------------------------------ kinship */
+
+/*
+ * Plain FP64 centered-kinship accumulation: K (n x n, ldk) += Xc * Xc^T over m SNP
+ * columns, where Xc = code - mean[j] for observed codes and 0 for missing ones
+ * (impute_and_center, src/jamma/kinship/missing.py:22-61, then the batch Gram of
+ * _accumulate_kinship, src/jamma/kinship/compute.py:46-57).  Only the lower triangle
+ * of K is updated (cuBLAS DSYRK); workspace holds the FP64 centered batch.
+ */
+int64_t jb_kinship_f64_workspace_size(int64_t n, int64_t m);
+int32_t jb_kinship_accumulate_f64(const int8_t* codes, int64_t ld_codes, int64_t n,
+                                  int64_t m, const double* mean, double* K, int64_t ldk,
+                                  void* workspace, int64_t workspace_bytes,
+                                  uintptr_t stream);
+
+/* Symmetrise from the lower triangle and scale: K = K * scale (ldk). */
+int32_t jb_kinship_finalize(double* K, int64_t n, int64_t ldk, double scale,
+                            uintptr_t stream);
+
+/* ------------------------------------------------------------------ eigen */
+
+/*
+ * FP64 symmetric eigendecomposition (cuSOLVER Xsyevd, lower triangle): on return A
+ * holds the eigenvectors as columns and w the eigenvalues in ascending order, with
+ * |w| < threshold set to 0.  Replaces np.linalg.eigh + thresholding
+ * (src/jamma/lmm/eigen.py:94,118).  workspace: jb_eigh_workspace_size bytes.
+ * Synchronises the stream (cuSOLVER reports convergence on the host).
+ */
+int64_t jb_eigh_workspace_size(int64_t n);
+int32_t jb_eigh_f64(double* A, int64_t n, int64_t lda, double* w, double threshold,
+                    void* workspace, int64_t workspace_bytes, uintptr_t stream);
+
+/* ------------------------------------------------------------------ rotation */
+
+/*
+ * Plain FP64 rotation C (n x m, ldc) = U^T * B with U n x n (ldu) and B n x m (ldb)
+ * (cuBLAS DGEMM).  Replaces the host products UT @ G / UT @ W / UT @ y
+ * (src/jamma/lmm/runner_streaming.py:349-352,409).
+ */
+int32_t jb_rotate_f64(const double* U, int64_t n, int64_t ldu, const double* B,
+                      int64_t m, int64_t ldb, double* C, int64_t ldc, uintptr_t stream);
+
+/* ------------------------------------------------------------------ association */
+
+/* Output arrays of jb_lmm_chunk; each is phi x m (phenotype-major, ld = m) or NULL. */
+typedef struct jb_lmm_out {
+    double* lambda_remle; /* l_remle          (modes 1,4) */
+    double* logl_h1;      /* REML logl at it  (modes 1,4) */
+    double* beta;         /* Wald beta (1,4) or score beta (3) */
+    double* se;
+    double* p_wald;       /* (1,4) */
+    double* lambda_mle;   /* l_mle            (2,4) */
+    double* logl_mle;     /* MLE logl at it   (2,4) */
+    double* p_lrt;        /* (2,4) */
+    double* p_score;      /* (3,4) */
+} jb_lmm_out;
+
+/*
+ * Per-SNP association for one rotated chunk, FP64, all phenotypes of a cohort.
+ *   evals : n eigenvalues (thresholded)
+ *   UtW   : n x n_cvt rotated covariates (ld = ldw)
+ *   Uty   : n x phi rotated phenotypes (ld = ldy)
+ *   UtG   : n x m rotated genotypes (ld = ldg)
+ *   lam0, logl0 : per-phenotype null-model MLE lambda and log-likelihood (modes 2,3,4;
+ *                 may be NULL for mode 1)
+ * Runs, per (SNP, phenotype): the Score statistics at the null H^-1, the MLE grid +
+ * golden-section search and LRT p-value, the REML grid + golden search and the Wald
+ * statistics -- whichever lmm_mode (1 Wald, 2 LRT, 3 Score, 4 all) asks for.
+ * Replaces batch_compute_uab / batch_compute_iab / golden_section_optimize_lambda[_mle]
+ * / batch_calc_wald_stats / batch_calc_score_stats / calc_lrt_pvalue_jax
+ * (src/jamma/lmm/likelihood_jax.py:231-883) as driven by
+ * src/jamma/lmm/runner_streaming.py:469-554.
+ * workspace: jb_lmm_workspace_size bytes, filled by jb_lmm_prepare.
+ */
+int64_t jb_lmm_workspace_size(int64_t n, int32_t n_cvt, int32_t phi, int32_t n_grid);
+
+/*
+ * Fill the association workspace for one cohort + phenotype set: the numpy-style
+ * log-lambda grid (likelihood_jax.py:540-543), the tabulated H = 1/(lambda*eval+1)
+ * rows for every grid lambda and every phenotype's null lambda0, log|H^-1| per grid
+ * point and the SNP-independent weighted sums.  Must precede jb_lmm_chunk calls that
+ * use the same inputs; n_cvt in 1..4.
+ */
+int32_t jb_lmm_prepare(int32_t lmm_mode, int64_t n, int32_t n_cvt, int32_t phi,
+                       const double* evals, const double* UtW, int64_t ldw,
+                       const double* Uty, int64_t ldy, const double* lam0, double l_min,
+                       double l_max, int32_t n_grid, void* workspace,
+                       int64_t workspace_bytes, uintptr_t stream);
+
+int32_t jb_lmm_chunk(int32_t lmm_mode, int64_t n, int32_t n_cvt, int32_t phi, int64_t m,
+                     const double* evals, const double* UtW, int64_t ldw,
+                     const double* Uty, int64_t ldy, const double* UtG, int64_t ldg,
+                     const double* lam0, const double* logl0, double l_min, double l_max,
+                     int32_t n_grid, int32_t n_iter, jb_lmm_out out, void* workspace,
+                     int64_t workspace_bytes, uintptr_t stream);
+
+/*
+ * Null-model MLE (lambda0, logl_H0) per phenotype on the device: the scalar 50-point
+ * grid and 20-step golden search of _golden_section_minimize
+ * (src/jamma/lmm/likelihood.py:395-474) over mle_log_likelihood_null (349-392), as
+ * compute_null_model_mle (571-607) runs it.  lam0, logl0: phi doubles (device).
+ */
+int32_t jb_null_mle(int64_t n, int32_t n_cvt, int32_t phi, const double* evals,
+                    const double* UtW, int64_t ldw, const double* Uty, int64_t ldy,
+                    double l_min, double l_max, int32_t n_grid, int32_t n_iter,
+                    double* lam0, double* logl0, uintptr_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* JAMMA_B200_H */

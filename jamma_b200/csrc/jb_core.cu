@@ -1,0 +1,337 @@
+// libjamma_b200 core: error plumbing, PLINK decode, imputation, plain FP64 kinship,
+// FP64 eigendecomposition (cuSOLVER) and plain FP64 rotation (cuBLAS).
+#include "jb_common.cuh"
+
+#include <mutex>
+#include <vector>
+
+#define JB_VERSION_MAJOR 0
+#define JB_VERSION_MINOR 1
+#define JB_VERSION_PATCH 0
+
+namespace jb {
+
+static thread_local char g_err[1024] = {0};
+
+void set_error(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+int32_t cuda_status(cudaError_t e, const char* what) {
+    set_error("CUDA error %d (%s) in %s", (int)e, cudaGetErrorString(e), what);
+    return JB_E_CUDA;
+}
+
+int32_t cublas_status(cublasStatus_t s, const char* what) {
+    set_error("cuBLAS status %d in %s", (int)s, what);
+    return JB_E_LIBRARY;
+}
+
+int32_t cusolver_status(cusolverStatus_t s, const char* what) {
+    set_error("cuSOLVER status %d in %s", (int)s, what);
+    return JB_E_LIBRARY;
+}
+
+namespace {
+constexpr int kMaxDevices = 64;
+thread_local cublasHandle_t t_cublas[kMaxDevices] = {nullptr};
+thread_local cusolverDnHandle_t t_cusolver[kMaxDevices] = {nullptr};
+}  // namespace
+
+cublasHandle_t cublas_handle() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+    if (!t_cublas[dev]) {
+        if (cublasCreate(&t_cublas[dev]) != CUBLAS_STATUS_SUCCESS) t_cublas[dev] = nullptr;
+    }
+    return t_cublas[dev];
+}
+
+cusolverDnHandle_t cusolver_handle() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+    if (!t_cusolver[dev]) {
+        if (cusolverDnCreate(&t_cusolver[dev]) != CUSOLVER_STATUS_SUCCESS)
+            t_cusolver[dev] = nullptr;
+    }
+    return t_cusolver[dev];
+}
+
+// ---------------------------------------------------------------- kernels
+
+// One CTA per SNP: decode the analysed samples, write int8 codes (3 = missing, zero
+// padding up to ld), and reduce {n_obs, sum, n_het, n_hom2}.
+__global__ void decode_bed_kernel(const uint8_t* __restrict__ packed, int64_t bps, int64_t m,
+                                  const int32_t* __restrict__ sidx, int64_t n,
+                                  int8_t* __restrict__ codes, int64_t ld,
+                                  int32_t* __restrict__ counts) {
+    const int64_t j = blockIdx.x;
+    if (j >= m) return;
+    const uint8_t* rec = packed + j * bps;
+    int8_t* out = codes + j * ld;
+    int obs = 0, sum = 0, het = 0, hom2 = 0;
+    for (int64_t s = threadIdx.x; s < ld; s += blockDim.x) {
+        int8_t v = 0;
+        if (s < n) {
+            const int64_t fi = sidx ? (int64_t)sidx[s] : s;
+            const int code = (rec[fi >> 2] >> (2 * (fi & 3))) & 3;
+            // count-A1: 00 -> 2, 01 -> missing, 10 -> 1, 11 -> 0
+            v = (int8_t)(code == 0 ? 2 : (code == 1 ? 3 : (code == 2 ? 1 : 0)));
+            if (v != 3) {
+                obs += 1;
+                sum += v;
+                het += (v == 1);
+                hom2 += (v == 2);
+            }
+        }
+        out[s] = v;
+    }
+    __shared__ int red[4][32];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    for (int o = 16; o > 0; o >>= 1) {
+        obs += __shfl_xor_sync(0xffffffffu, obs, o);
+        sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        het += __shfl_xor_sync(0xffffffffu, het, o);
+        hom2 += __shfl_xor_sync(0xffffffffu, hom2, o);
+    }
+    if (lane == 0) {
+        red[0][w] = obs;
+        red[1][w] = sum;
+        red[2][w] = het;
+        red[3][w] = hom2;
+    }
+    __syncthreads();
+    if (threadIdx.x < 4) {
+        int acc = 0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) acc += red[threadIdx.x][k];
+        counts[j * 4 + threadIdx.x] = acc;
+    }
+}
+
+__global__ void impute_f64_kernel(const int8_t* __restrict__ codes, int64_t ldc, int64_t n,
+                                  int64_t m, const double* __restrict__ mean,
+                                  double* __restrict__ G, int64_t ldg) {
+    const int64_t j = blockIdx.y;
+    const double mu = mean[j];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int8_t c = codes[j * ldc + i];
+        G[j * ldg + i] = (c == 3) ? mu : (double)c;
+    }
+}
+
+__global__ void center_f64_kernel(const int8_t* __restrict__ codes, int64_t ldc, int64_t n,
+                                  int64_t m, const double* __restrict__ mean,
+                                  double* __restrict__ X) {
+    const int64_t j = blockIdx.y;
+    const double mu = mean[j];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int8_t c = codes[j * ldc + i];
+        X[j * n + i] = (c == 3) ? 0.0 : ((double)c - mu);
+    }
+}
+
+__global__ void symmetrize_scale_kernel(double* K, int64_t n, int64_t ldk, double scale) {
+    const int64_t col = blockIdx.y;
+    for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n;
+         row += (int64_t)gridDim.x * blockDim.x) {
+        if (row >= col) {
+            const double v = K[col * ldk + row] * scale;
+            K[col * ldk + row] = v;
+            if (row != col) K[row * ldk + col] = v;
+        }
+    }
+}
+
+__global__ void threshold_kernel(double* w, int64_t n, double thr) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        if (fabs(w[i]) < thr) w[i] = 0.0;
+    }
+}
+
+static dim3 col_grid(int64_t n, int64_t m) {
+    const int64_t bx = ceil_div(n, 256) < 64 ? ceil_div(n, 256) : 64;
+    return dim3((unsigned)(bx > 0 ? bx : 1), (unsigned)m, 1);
+}
+
+}  // namespace jb
+
+using namespace jb;
+
+extern "C" {
+
+int32_t jb_version(void) {
+    return JB_VERSION_MAJOR * 10000 + JB_VERSION_MINOR * 100 + JB_VERSION_PATCH;
+}
+
+int32_t jb_last_error(char* buf, size_t len) {
+    if (!buf || len == 0) return JB_E_INVALID;
+    strncpy(buf, g_err, len - 1);
+    buf[len - 1] = 0;
+    return JB_OK;
+}
+
+int32_t jb_device_arch(void) {
+    int dev = 0;
+    JB_CUDA(cudaGetDevice(&dev));
+    int major = 0, minor = 0;
+    JB_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev));
+    JB_CUDA(cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev));
+    return major * 10 + minor;
+}
+
+int32_t jb_decode_bed(const uint8_t* packed, int64_t bytes_per_snp, int64_t m,
+                      const int32_t* sample_idx, int64_t n, int8_t* codes, int64_t ld_codes,
+                      int32_t* counts, uintptr_t stream) {
+    JB_CHECK_ARG(m >= 0 && n >= 0, "jb_decode_bed: negative size");
+    JB_CHECK_ARG(ld_codes >= n, "jb_decode_bed: ld_codes (%lld) < n (%lld)",
+                 (long long)ld_codes, (long long)n);
+    JB_CHECK_ARG(sample_idx || n <= 4 * bytes_per_snp,
+                 "jb_decode_bed: n exceeds the record length");
+    if (m == 0) return JB_OK;
+    JB_CHECK_ARG(packed && codes && counts, "jb_decode_bed: null pointer");
+    JB_CHECK_ARG(m < (1ll << 31), "jb_decode_bed: too many SNPs in one call");
+    decode_bed_kernel<<<(unsigned)m, 256, 0, as_stream(stream)>>>(packed, bytes_per_snp, m,
+                                                                 sample_idx, n, codes,
+                                                                 ld_codes, counts);
+    JB_LAUNCH_CHECK("decode_bed_kernel");
+    return JB_OK;
+}
+
+int32_t jb_impute_f64(const int8_t* codes, int64_t ld_codes, int64_t n, int64_t m,
+                      const double* mean, double* G, int64_t ldg, uintptr_t stream) {
+    JB_CHECK_ARG(n >= 0 && m >= 0 && ldg >= n && ld_codes >= n, "jb_impute_f64: bad shape");
+    if (n == 0 || m == 0) return JB_OK;
+    JB_CHECK_ARG(m < 65536, "jb_impute_f64: m must be < 65536 per call");
+    impute_f64_kernel<<<col_grid(n, m), 256, 0, as_stream(stream)>>>(codes, ld_codes, n, m,
+                                                                     mean, G, ldg);
+    JB_LAUNCH_CHECK("impute_f64_kernel");
+    return JB_OK;
+}
+
+int64_t jb_kinship_f64_workspace_size(int64_t n, int64_t m) { return n * m * 8; }
+
+int32_t jb_kinship_accumulate_f64(const int8_t* codes, int64_t ld_codes, int64_t n, int64_t m,
+                                  const double* mean, double* K, int64_t ldk, void* workspace,
+                                  int64_t workspace_bytes, uintptr_t stream) {
+    JB_CHECK_ARG(n > 0 && m >= 0 && ldk >= n && ld_codes >= n, "jb_kinship_accumulate_f64: bad shape");
+    if (m == 0) return JB_OK;
+    JB_CHECK_ARG(m < 65536, "jb_kinship_accumulate_f64: m must be < 65536 per call");
+    JB_CHECK_ARG(workspace_bytes >= jb_kinship_f64_workspace_size(n, m),
+                 "jb_kinship_accumulate_f64: workspace too small");
+    double* X = static_cast<double*>(workspace);
+    center_f64_kernel<<<col_grid(n, m), 256, 0, as_stream(stream)>>>(codes, ld_codes, n, m, mean,
+                                                                    X);
+    JB_LAUNCH_CHECK("center_f64_kernel");
+    cublasHandle_t h = cublas_handle();
+    if (!h) {
+        set_error("cuBLAS handle creation failed");
+        return JB_E_LIBRARY;
+    }
+    cublasStatus_t s = cublasSetStream(h, as_stream(stream));
+    if (s != CUBLAS_STATUS_SUCCESS) return cublas_status(s, "cublasSetStream");
+    const double one = 1.0;
+    s = cublasDsyrk(h, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, (int)n, (int)m, &one, X, (int)n, &one,
+                    K, (int)ldk);
+    if (s != CUBLAS_STATUS_SUCCESS) return cublas_status(s, "cublasDsyrk");
+    return JB_OK;
+}
+
+int32_t jb_kinship_finalize(double* K, int64_t n, int64_t ldk, double scale, uintptr_t stream) {
+    JB_CHECK_ARG(n >= 0 && ldk >= n, "jb_kinship_finalize: bad shape");
+    if (n == 0) return JB_OK;
+    JB_CHECK_ARG(n < 65536 * 4, "jb_kinship_finalize: n too large");
+    const int64_t bx = ceil_div(n, 256) < 64 ? ceil_div(n, 256) : 64;
+    dim3 grid((unsigned)bx, (unsigned)n, 1);
+    symmetrize_scale_kernel<<<grid, 256, 0, as_stream(stream)>>>(K, n, ldk, scale);
+    JB_LAUNCH_CHECK("symmetrize_scale_kernel");
+    return JB_OK;
+}
+
+int64_t jb_eigh_workspace_size(int64_t n) {
+    cusolverDnHandle_t h = cusolver_handle();
+    if (!h || n <= 0) return -1;
+    cusolverDnParams_t params;
+    if (cusolverDnCreateParams(&params) != CUSOLVER_STATUS_SUCCESS) return -1;
+    size_t dev_bytes = 0, host_bytes = 0;
+    cusolverStatus_t s = cusolverDnXsyevd_bufferSize(
+        h, params, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, CUDA_R_64F, nullptr, n,
+        CUDA_R_64F, nullptr, CUDA_R_64F, &dev_bytes, &host_bytes);
+    cusolverDnDestroyParams(params);
+    if (s != CUSOLVER_STATUS_SUCCESS) return -1;
+    return (int64_t)(((dev_bytes + 255) / 256) * 256) + 256;  // + device info word
+}
+
+int32_t jb_eigh_f64(double* A, int64_t n, int64_t lda, double* w, double threshold,
+                    void* workspace, int64_t workspace_bytes, uintptr_t stream) {
+    JB_CHECK_ARG(n > 0 && lda >= n && A && w, "jb_eigh_f64: bad arguments");
+    cusolverDnHandle_t h = cusolver_handle();
+    if (!h) {
+        set_error("cuSOLVER handle creation failed");
+        return JB_E_LIBRARY;
+    }
+    cusolverStatus_t s = cusolverDnSetStream(h, as_stream(stream));
+    if (s != CUSOLVER_STATUS_SUCCESS) return cusolver_status(s, "cusolverDnSetStream");
+    cusolverDnParams_t params;
+    s = cusolverDnCreateParams(&params);
+    if (s != CUSOLVER_STATUS_SUCCESS) return cusolver_status(s, "cusolverDnCreateParams");
+    size_t dev_bytes = 0, host_bytes = 0;
+    s = cusolverDnXsyevd_bufferSize(h, params, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n,
+                                    CUDA_R_64F, A, lda, CUDA_R_64F, w, CUDA_R_64F, &dev_bytes,
+                                    &host_bytes);
+    if (s != CUSOLVER_STATUS_SUCCESS) {
+        cusolverDnDestroyParams(params);
+        return cusolver_status(s, "cusolverDnXsyevd_bufferSize");
+    }
+    const size_t info_off = ((dev_bytes + 255) / 256) * 256;
+    if (workspace_bytes < (int64_t)info_off + 256) {
+        cusolverDnDestroyParams(params);
+        set_error("jb_eigh_f64: workspace %lld < required %lld", (long long)workspace_bytes,
+                  (long long)info_off + 256);
+        return JB_E_INVALID;
+    }
+    uint8_t* ws = static_cast<uint8_t*>(workspace);
+    int* d_info = reinterpret_cast<int*>(ws + info_off);  // after the solver's bytes
+    std::vector<uint8_t> host_ws(host_bytes > 0 ? host_bytes : 1);
+    s = cusolverDnXsyevd(h, params, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n,
+                         CUDA_R_64F, A, lda, CUDA_R_64F, w, CUDA_R_64F, ws, dev_bytes,
+                         host_ws.data(), host_bytes, d_info);
+    cusolverDnDestroyParams(params);
+    if (s != CUSOLVER_STATUS_SUCCESS) return cusolver_status(s, "cusolverDnXsyevd");
+    threshold_kernel<<<64, 256, 0, as_stream(stream)>>>(w, n, threshold);
+    JB_LAUNCH_CHECK("threshold_kernel");
+    int info = 0;
+    JB_CUDA(cudaMemcpyAsync(&info, d_info, sizeof(int), cudaMemcpyDeviceToHost,
+                            as_stream(stream)));
+    JB_CUDA(cudaStreamSynchronize(as_stream(stream)));
+    if (info != 0) {
+        set_error("cusolverDnXsyevd: info = %d (no convergence or bad argument)", info);
+        return JB_E_NUMERIC;
+    }
+    return JB_OK;
+}
+
+int32_t jb_rotate_f64(const double* U, int64_t n, int64_t ldu, const double* B, int64_t m,
+                      int64_t ldb, double* C, int64_t ldc, uintptr_t stream) {
+    JB_CHECK_ARG(n > 0 && m >= 0 && ldu >= n && ldb >= n && ldc >= n, "jb_rotate_f64: bad shape");
+    if (m == 0) return JB_OK;
+    cublasHandle_t h = cublas_handle();
+    if (!h) {
+        set_error("cuBLAS handle creation failed");
+        return JB_E_LIBRARY;
+    }
+    cublasStatus_t s = cublasSetStream(h, as_stream(stream));
+    if (s != CUBLAS_STATUS_SUCCESS) return cublas_status(s, "cublasSetStream");
+    const double one = 1.0, zero = 0.0;
+    s = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, (int)n, (int)m, (int)n, &one, U, (int)ldu, B,
+                    (int)ldb, &zero, C, (int)ldc);
+    if (s != CUBLAS_STATUS_SUCCESS) return cublas_status(s, "cublasDgemm");
+    return JB_OK;
+}
+
+}  // extern "C"

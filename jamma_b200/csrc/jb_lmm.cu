@@ -1,0 +1,845 @@
+// libjamma_b200: per-SNP LMM association (FP64) on B200.
+//
+// One warp owns one (SNP, phenotype) pair and runs its whole pipeline without
+// materialising Uab: the weighted dot products of [W_1..W_c, x, y] are formed on the
+// fly from the rotated vectors while streaming them once per likelihood evaluation.
+//
+//   phase 1  one pass with two fixed weightings: H = 1 (Iab, for REML's logdet term)
+//            and H = H0 (the null-model MLE lambda, for the score test);
+//   phase 2  the shared lambda grid; every grid point's H row is tabulated once per
+//            cohort (SNP independent), the x-free dot products are pre-reduced, so a
+//            grid evaluation only needs the c+2 x-dependent sums; REML and MLE grid
+//            log-likelihoods come from the same sums;
+//   phase 3  JAX-style golden-section refinement for MLE and REML, per-SNP lambda;
+//   epilogue Wald (from the final REML evaluation), LRT and score statistics.
+//
+// The sequence of evaluations, bracket rules and NaN behaviour follow
+// src/jamma/lmm/likelihood_jax.py (148-339 likelihoods, 419-598 search, 601-798
+// statistics) exactly; only the summation order of the length-n reductions differs.
+#include "jb_common.cuh"
+
+#include <cmath>
+
+namespace jb {
+namespace lmm {
+
+constexpr double kPhi = 0.6180339887498949;
+constexpr double kPyyMin = 1e-8;
+constexpr int kMaxCvt = 4;
+
+template <int C>
+struct Lay {
+    static constexpr int R = C + 2;  // vector columns: W_0..W_{C-1}, X = C, Y = C+1
+    static constexpr int NI = R * (R + 1) / 2;
+    static constexpr int NX = C + 2;  // pairs containing X: (W_a,X) a<C, (X,X), (X,Y)
+    static constexpr int NS = NI - NX;
+    // GEMMA GetabIndex on 0-based columns (src/jamma/lmm/likelihood.py:25-43)
+    __host__ __device__ static constexpr int idx(int a, int b) {
+        return a <= b ? (2 * R - (a + 1) + 2) * a / 2 + b - a
+                      : (2 * R - (b + 1) + 2) * b / 2 + a - b;
+    }
+};
+
+struct Params {
+    int mode;
+    int64_t n;
+    int phi;
+    int64_t m;
+    const double* evals;
+    const double* W;
+    int64_t ldw;
+    const double* Y;
+    int64_t ldy;
+    const double* G;
+    int64_t ldg;
+    const double* logl0;
+    int n_grid;
+    int n_iter;
+    const double* loglam;  // n_grid
+    const double* logdet;  // n_grid
+    const double* H;       // (n_grid + phi) x n: grid rows, then null rows
+    const double* S;       // (n_grid + 1 + phi) x phi x NS shared sums
+    double c_reml, c_mle, df, n_d;
+    jb_lmm_out out;
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__device__ __forceinline__ double jnan() { return __longlong_as_double(0x7ff8000000000000ll); }
+__device__ __forceinline__ double jmax(double a, double b) {  // jnp.maximum: NaN propagates
+    return (isnan(a) || isnan(b)) ? jnan() : (a > b ? a : b);
+}
+__device__ __forceinline__ double clamp_pyy(double v) {
+    return (v >= 0.0 && v < kPyyMin) ? kPyyMin : v;
+}
+__device__ __forceinline__ double rlog(double v) { return v > 0 ? log(v) : 0.0; }
+
+// ---------------------------------------------------------------- special functions
+// Regularised incomplete beta I_x(a, b) by the continued fraction of DLMF 8.17.22,
+// evaluated with the modified Lentz method (Numerical Recipes 2nd ed. section 6.4):
+// direct when x < (a+1)/(a+b+2), else through I_x(a,b) = 1 - I_{1-x}(b,a).
+__device__ double betacf(double a, double b, double x) {
+    const double tiny = 1e-300, eps = 1e-16;
+    const double qab = a + b, qap = a + 1.0, qam = a - 1.0;
+    double c = 1.0, d = 1.0 - qab * x / qap;
+    if (fabs(d) < tiny) d = tiny;
+    d = 1.0 / d;
+    double h = d;
+    for (int k = 1; k <= 4000; ++k) {
+        const double k2 = 2.0 * k;
+        double aa = k * (b - k) * x / ((qam + k2) * (a + k2));
+        d = 1.0 + aa * d;
+        if (fabs(d) < tiny) d = tiny;
+        c = 1.0 + aa / c;
+        if (fabs(c) < tiny) c = tiny;
+        d = 1.0 / d;
+        h *= d * c;
+        aa = -(a + k) * (qab + k) * x / ((a + k2) * (qap + k2));
+        d = 1.0 + aa * d;
+        if (fabs(d) < tiny) d = tiny;
+        c = 1.0 + aa / c;
+        if (fabs(c) < tiny) c = tiny;
+        d = 1.0 / d;
+        const double del = d * c;
+        h *= del;
+        if (fabs(del - 1.0) < eps) break;
+    }
+    return h;
+}
+
+__device__ double betainc_reg(double a, double b, double x) {
+    if (isnan(x)) return jnan();
+    if (x <= 0.0) return 0.0;
+    if (x >= 1.0) return 1.0;
+    const double lbt = lgamma(a + b) - lgamma(a) - lgamma(b) + a * log(x) + b * log1p(-x);
+    if (x < (a + 1.0) / (a + b + 2.0)) return exp(lbt) * betacf(a, b, x) / a;
+    return 1.0 - exp(lbt) * betacf(b, a, 1.0 - x) / b;
+}
+
+// F-test p-value as jamma writes it (likelihood_jax.py:668-673,765-771).
+__device__ double f_pvalue(double f, double df, bool valid) {
+    double z;
+    if (isnan(f)) {
+        z = jnan();
+    } else {
+        z = df / (df + (f > 1e-10 ? f : 1e-10));
+        z = z < 0.0 ? 0.0 : (z > 1.0 ? 1.0 : z);
+    }
+    double p = betainc_reg(df / 2.0, 0.5, z);
+    if (f <= 0.0) p = 1.0;
+    return valid ? p : jnan();
+}
+
+// chi-square(1) survival function: P(X > s) = erfc(sqrt(s / 2)).
+__device__ double chi2_1_sf(double s) {
+    if (isnan(s)) return jnan();
+    return erfc(sqrt(0.5 * s));
+}
+
+// ---------------------------------------------------------------- Pab
+template <int C>
+struct PabOut {
+    double xx, xy, yy;  // level c (covariates projected out)
+    double yy1;         // level c+1 (covariates and genotype projected out)
+    double diag[C + 1]; // Pab[i, idx(i,i)], i = 0..c
+};
+
+// GEMMA CalcPab recursion (likelihood_jax.py:148-186); inverse of a zero pivot is 0.
+template <int C>
+__device__ __forceinline__ PabOut<C> pab_reduce(const double (&row0)[Lay<C>::NI]) {
+    using L = Lay<C>;
+    constexpr int R = L::R;
+    double prev[L::NI], cur[L::NI];
+    PabOut<C> o;
+#pragma unroll
+    for (int k = 0; k < L::NI; ++k) prev[k] = cur[k] = row0[k];
+    o.diag[0] = prev[L::idx(0, 0)];
+#pragma unroll
+    for (int p = 1; p <= C + 1; ++p) {
+        const int w = p - 1;
+        const double ww = prev[L::idx(w, w)];
+        const double inv = (ww != 0.0) ? 1.0 / ww : 0.0;
+#pragma unroll
+        for (int a = p; a < R; ++a) {
+#pragma unroll
+            for (int b = a; b < R; ++b) {
+                const double t = __dmul_rn(__dmul_rn(prev[L::idx(a, w)], prev[L::idx(b, w)]), inv);
+                cur[L::idx(a, b)] = __dsub_rn(prev[L::idx(a, b)], t);
+            }
+        }
+        if (p <= C) o.diag[p] = cur[L::idx(p, p)];
+        if (p == C) {
+            o.xx = cur[L::idx(C, C)];
+            o.xy = cur[L::idx(C, C + 1)];
+            o.yy = cur[L::idx(C + 1, C + 1)];
+        }
+#pragma unroll
+        for (int k = 0; k < L::NI; ++k) prev[k] = cur[k];
+    }
+    o.yy1 = prev[L::idx(C + 1, C + 1)];
+    return o;
+}
+
+// REML log-likelihood (_reml_with_precomputed_iab, likelihood_jax.py:280-339).
+template <int C>
+__device__ __forceinline__ double reml_logl(const PabOut<C>& pb, const double (&iab_diag)[C + 1],
+                                            double logdet_h, const Params& p) {
+    double ldw = 0.0;
+#pragma unroll
+    for (int i = 0; i <= C; ++i) {
+        ldw = __dadd_rn(ldw, pb.diag[i] > 0 ? log(pb.diag[i]) : 0.0);
+        ldw = __dsub_rn(ldw, iab_diag[i] > 0 ? log(iab_diag[i]) : 0.0);
+    }
+    const double pyy = clamp_pyy(pb.yy1);
+    double f = __dsub_rn(p.c_reml, __dmul_rn(0.5, logdet_h));
+    f = __dsub_rn(f, __dmul_rn(0.5, ldw));
+    return __dsub_rn(f, __dmul_rn(__dmul_rn(0.5, p.df), log(pyy)));
+}
+
+// MLE log-likelihood (mle_log_likelihood_jax, likelihood_jax.py:189-228).
+template <int C>
+__device__ __forceinline__ double mle_logl(const PabOut<C>& pb, double logdet_h, const Params& p) {
+    const double pyy = clamp_pyy(pb.yy1);
+    const double f = __dsub_rn(p.c_mle, __dmul_rn(0.5, logdet_h));
+    return __dsub_rn(f, __dmul_rn(__dmul_rn(0.5, p.n_d), log(pyy)));
+}
+
+// Assemble a full row 0 from pre-reduced x-free sums and fresh x-dependent sums.
+template <int C>
+__device__ __forceinline__ void assemble(double (&row0)[Lay<C>::NI], const double* shared,
+                                         const double (&xs)[Lay<C>::NX]) {
+    using L = Lay<C>;
+    int s = 0;
+#pragma unroll
+    for (int a = 0; a < L::R; ++a) {
+#pragma unroll
+        for (int b = a; b < L::R; ++b) {
+            if (a == C || b == C) continue;
+            row0[L::idx(a, b)] = shared[s++];
+        }
+    }
+#pragma unroll
+    for (int a = 0; a < C; ++a) row0[L::idx(a, C)] = xs[a];
+    row0[L::idx(C, C)] = xs[C];
+    row0[L::idx(C, C + 1)] = xs[C + 1];
+}
+
+// Full evaluation at a per-SNP lambda: H = 1/(lambda*eval + 1), all NI sums + logdet.
+template <int C>
+__device__ __forceinline__ void eval_full(const Params& p, const double* __restrict__ x,
+                                          const double* __restrict__ y, double lam,
+                                          double (&row0)[Lay<C>::NI], double& logdet) {
+    using L = Lay<C>;
+    double acc[L::NI];
+#pragma unroll
+    for (int k = 0; k < L::NI; ++k) acc[k] = 0.0;
+    double ld = 0.0;
+    const int lane = threadIdx.x & 31;
+    for (int64_t i = lane; i < p.n; i += 32) {
+        const double v = __dadd_rn(__dmul_rn(lam, __ldg(p.evals + i)), 1.0);
+        const double hi = 1.0 / v;
+        ld += log(fabs(v));
+        double vec[L::R];
+#pragma unroll
+        for (int a = 0; a < C; ++a) vec[a] = __ldg(p.W + a * p.ldw + i);
+        vec[C] = x[i];
+        vec[C + 1] = __ldg(y + i);
+#pragma unroll
+        for (int a = 0; a < L::R; ++a) {
+            const double t = hi * vec[a];
+#pragma unroll
+            for (int b = a; b < L::R; ++b) acc[L::idx(a, b)] = fma(t, vec[b], acc[L::idx(a, b)]);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < L::NI; ++k) row0[k] = warp_sum(acc[k]);
+    logdet = warp_sum(ld);
+}
+
+template <int C, bool REML>
+__device__ __forceinline__ double eval_logl(const Params& p, const double* x, const double* y,
+                                            double log_lam, const double (&iab_diag)[C + 1],
+                                            PabOut<C>* keep) {
+    double row0[Lay<C>::NI];
+    double logdet;
+    eval_full<C>(p, x, y, exp(log_lam), row0, logdet);
+    const PabOut<C> pb = pab_reduce<C>(row0);
+    if (keep) *keep = pb;
+    return REML ? reml_logl<C>(pb, iab_diag, logdet, p) : mle_logl<C>(pb, logdet, p);
+}
+
+// Grid bracket + golden section (_golden_section_refine, likelihood_jax.py:419-488).
+template <int C, bool REML>
+__device__ void golden(const Params& p, const double* x, const double* y, int best,
+                       const double (&iab_diag)[C + 1], double& lam_out, double& logl_out,
+                       PabOut<C>& pb_out) {
+    const int lo = best - 1 > 0 ? best - 1 : 0;
+    const int hi = best + 1 < p.n_grid - 1 ? best + 1 : p.n_grid - 1;
+    double a = p.loglam[lo], b = p.loglam[hi];
+    double c = __dsub_rn(b, __dmul_rn(kPhi, __dsub_rn(b, a)));
+    double d = __dadd_rn(a, __dmul_rn(kPhi, __dsub_rn(b, a)));
+    double fc = eval_logl<C, REML>(p, x, y, c, iab_diag, nullptr);
+    double fd = eval_logl<C, REML>(p, x, y, d, iab_diag, nullptr);
+    for (int it = 0; it < p.n_iter; ++it) {
+        const bool keep_left = fc > fd;
+        const double na = keep_left ? a : c;
+        const double nb = keep_left ? d : b;
+        const double nc = __dsub_rn(nb, __dmul_rn(kPhi, __dsub_rn(nb, na)));
+        const double nd = __dadd_rn(na, __dmul_rn(kPhi, __dsub_rn(nb, na)));
+        const double nl = eval_logl<C, REML>(p, x, y, keep_left ? nc : nd, iab_diag, nullptr);
+        const double nfc = keep_left ? nl : fd;
+        const double nfd = keep_left ? fc : nl;
+        a = na; b = nb; c = nc; d = nd; fc = nfc; fd = nfd;
+    }
+    const double log_opt = __dmul_rn(__dadd_rn(a, b), 0.5);
+    lam_out = exp(log_opt);
+    logl_out = eval_logl<C, REML>(p, x, y, log_opt, iab_diag, &pb_out);
+}
+
+// jnp.argmax semantics: first maximum, NaN wins (first NaN).
+struct ArgMax {
+    int idx = -1;
+    double v = 0.0;
+    __device__ void push(int i, double x) {
+        if (idx < 0) { idx = i; v = x; return; }
+        if (isnan(v)) return;
+        if (isnan(x) || x > v) { idx = i; v = x; }
+    }
+};
+
+template <int C>
+__device__ __forceinline__ void beta_se(const PabOut<C>& pb, double px_yy, double df, bool& valid,
+                                        double& beta, double& tau, double& se) {
+    valid = pb.xx > 0;
+    const double safe_xx = valid ? pb.xx : 1.0;
+    beta = valid ? pb.xy / safe_xx : jnan();
+    tau = df / px_yy;
+    double var = valid ? 1.0 / (tau * safe_xx) : jnan();
+    var = fabs(var) < 0.001 ? fabs(var) : var;
+    se = valid ? sqrt(var) : jnan();
+}
+
+template <int C, int GB>
+__global__ void __launch_bounds__(256) lmm_pairs_kernel(const Params p) {
+    using L = Lay<C>;
+    const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (wid >= p.m * p.phi) return;
+    const int lane = threadIdx.x & 31;
+    const int64_t j = wid / p.phi;
+    const int f = (int)(wid % p.phi);
+    const double* __restrict__ x = p.G + j * p.ldg;
+    const double* __restrict__ y = p.Y + (int64_t)f * p.ldy;
+    const bool need_reml = p.mode == 1 || p.mode == 4;
+    const bool need_mle = p.mode == 2 || p.mode == 4;
+    const bool need_score = p.mode == 3 || p.mode == 4;
+    const int64_t o = (int64_t)f * p.m + j;
+    const int64_t srow = (int64_t)p.phi * L::NS;  // stride of one S row
+
+    // ---------------- phase 1: H = 1 (Iab) and H = H0 (score)
+    double iab_diag[C + 1];
+#pragma unroll
+    for (int i = 0; i <= C; ++i) iab_diag[i] = 0.0;
+    {
+        double a1[L::NX], a2[L::NX];
+#pragma unroll
+        for (int k = 0; k < L::NX; ++k) a1[k] = a2[k] = 0.0;
+        const double* h0 = p.H + (int64_t)(p.n_grid + f) * p.n;
+        for (int64_t i = lane; i < p.n; i += 32) {
+            const double xv = x[i];
+            const double yv = __ldg(y + i);
+            const double t2 = need_score ? __ldg(h0 + i) * xv : 0.0;
+#pragma unroll
+            for (int a = 0; a < C; ++a) {
+                const double w = __ldg(p.W + a * p.ldw + i);
+                a1[a] = fma(xv, w, a1[a]);
+                a2[a] = fma(t2, w, a2[a]);
+            }
+            a1[C] = fma(xv, xv, a1[C]);
+            a2[C] = fma(t2, xv, a2[C]);
+            a1[C + 1] = fma(xv, yv, a1[C + 1]);
+            a2[C + 1] = fma(t2, yv, a2[C + 1]);
+        }
+#pragma unroll
+        for (int k = 0; k < L::NX; ++k) {
+            a1[k] = warp_sum(a1[k]);
+            a2[k] = warp_sum(a2[k]);
+        }
+        if (need_reml) {
+            double row0[L::NI];
+            assemble<C>(row0, p.S + (int64_t)p.n_grid * srow + (int64_t)f * L::NS, a1);
+            const PabOut<C> pb = pab_reduce<C>(row0);
+#pragma unroll
+            for (int i = 0; i <= C; ++i) iab_diag[i] = pb.diag[i];
+        }
+        if (need_score) {
+            double row0[L::NI];
+            assemble<C>(row0, p.S + (int64_t)(p.n_grid + 1 + f) * srow + (int64_t)f * L::NS, a2);
+            const PabOut<C> pb = pab_reduce<C>(row0);
+            bool valid;
+            double beta, tau, se;
+            beta_se<C>(pb, clamp_pyy(pb.yy1), p.df, valid, beta, tau, se);
+            const double fstat = p.n_d * (pb.xy * pb.xy) / (pb.yy * (valid ? pb.xx : 1.0));
+            const double pv = f_pvalue(fstat, p.df, valid);
+            if (lane == 0) {
+                if (p.out.p_score) p.out.p_score[o] = pv;
+                if (p.mode == 3) {
+                    if (p.out.beta) p.out.beta[o] = beta;
+                    if (p.out.se) p.out.se[o] = se;
+                }
+            }
+        }
+    }
+    if (!need_reml && !need_mle) return;
+
+    // ---------------- phase 2: shared lambda grid
+    ArgMax best_reml, best_mle;
+    for (int g0 = 0; g0 < p.n_grid; g0 += GB) {
+        double acc[GB][L::NX];
+#pragma unroll
+        for (int g = 0; g < GB; ++g)
+#pragma unroll
+            for (int k = 0; k < L::NX; ++k) acc[g][k] = 0.0;
+        const int ng = p.n_grid - g0 < GB ? p.n_grid - g0 : GB;
+        for (int64_t i = lane; i < p.n; i += 32) {
+            const double xv = x[i];
+            const double yv = __ldg(y + i);
+            double w[C > 0 ? C : 1];
+#pragma unroll
+            for (int a = 0; a < C; ++a) w[a] = __ldg(p.W + a * p.ldw + i);
+#pragma unroll
+            for (int g = 0; g < GB; ++g) {
+                if (g < ng) {
+                    const double t = __ldg(p.H + (int64_t)(g0 + g) * p.n + i) * xv;
+#pragma unroll
+                    for (int a = 0; a < C; ++a) acc[g][a] = fma(t, w[a], acc[g][a]);
+                    acc[g][C] = fma(t, xv, acc[g][C]);
+                    acc[g][C + 1] = fma(t, yv, acc[g][C + 1]);
+                }
+            }
+        }
+#pragma unroll
+        for (int g = 0; g < GB; ++g) {
+            if (g < ng) {
+#pragma unroll
+                for (int k = 0; k < L::NX; ++k) acc[g][k] = warp_sum(acc[g][k]);
+                double row0[L::NI];
+                assemble<C>(row0, p.S + (int64_t)(g0 + g) * srow + (int64_t)f * L::NS, acc[g]);
+                const PabOut<C> pb = pab_reduce<C>(row0);
+                const double ldh = p.logdet[g0 + g];
+                if (need_reml) best_reml.push(g0 + g, reml_logl<C>(pb, iab_diag, ldh, p));
+                if (need_mle) best_mle.push(g0 + g, mle_logl<C>(pb, ldh, p));
+            }
+        }
+    }
+
+    // ---------------- phase 3: golden sections + statistics
+    if (need_mle) {
+        double lam, logl;
+        PabOut<C> pb;
+        golden<C, false>(p, x, y, best_mle.idx, iab_diag, lam, logl, pb);
+        if (lane == 0) {
+            if (p.out.lambda_mle) p.out.lambda_mle[o] = lam;
+            if (p.out.logl_mle) p.out.logl_mle[o] = logl;
+            const double stat = jmax(2.0 * (logl - p.logl0[f]), 0.0);
+            if (p.out.p_lrt) p.out.p_lrt[o] = chi2_1_sf(stat);
+        }
+    }
+    if (need_reml) {
+        double lam, logl;
+        PabOut<C> pb;
+        golden<C, true>(p, x, y, best_reml.idx, iab_diag, lam, logl, pb);
+        bool valid;
+        double beta, tau, se;
+        const double px_yy = clamp_pyy(pb.yy1);
+        beta_se<C>(pb, px_yy, p.df, valid, beta, tau, se);
+        const double fstat = (pb.yy - px_yy) * tau;
+        const double pv = f_pvalue(fstat, p.df, valid);
+        if (lane == 0) {
+            if (p.out.lambda_remle) p.out.lambda_remle[o] = lam;
+            if (p.out.logl_h1) p.out.logl_h1[o] = logl;
+            if (p.out.beta) p.out.beta[o] = beta;
+            if (p.out.se) p.out.se[o] = se;
+            if (p.out.p_wald) p.out.p_wald[o] = pv;
+        }
+    }
+}
+
+// ---------------------------------------------------------------- tables
+// H rows: grid lambda_g = exp(loglam[g]) for g < n_grid, then the null lambda0[f];
+// logdet[g] = sum_i log|lambda_g * eval_i + 1| for grid rows.
+__global__ void lmm_table_kernel(int64_t n, int n_grid, int phi, const double* __restrict__ evals,
+                                 const double* __restrict__ loglam, const double* __restrict__ lam0,
+                                 double* __restrict__ H, double* __restrict__ logdet) {
+    const int r = blockIdx.x;
+    const double lam = r < n_grid ? exp(loglam[r]) : lam0[r - n_grid];
+    double ld = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const double v = __dadd_rn(__dmul_rn(lam, evals[i]), 1.0);
+        H[(int64_t)r * n + i] = 1.0 / v;
+        ld += log(fabs(v));
+    }
+    if (r >= n_grid) return;
+    __shared__ double red[32];
+    ld = warp_sum(ld);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = ld;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += red[k];
+        logdet[r] = s;
+    }
+}
+
+// x-free weighted sums S[row][f][s] = sum_i h_row,i * v_a,i * v_b,i over pairs without X,
+// rows: grid (H), ones, null rows (H0_f).
+template <int C>
+__global__ void lmm_shared_kernel(int64_t n, int n_grid, int phi, const double* __restrict__ W,
+                                  int64_t ldw, const double* __restrict__ Y, int64_t ldy,
+                                  const double* __restrict__ H, double* __restrict__ S) {
+    using L = Lay<C>;
+    const int r = blockIdx.x;
+    const int f = blockIdx.y;
+    const double* h = r < n_grid ? H + (int64_t)r * n
+                                 : (r == n_grid ? nullptr : H + (int64_t)(r - 1) * n);
+    double acc[L::NS];
+#pragma unroll
+    for (int s = 0; s < L::NS; ++s) acc[s] = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const double hi = h ? h[i] : 1.0;
+        double vec[L::R];
+#pragma unroll
+        for (int a = 0; a < C; ++a) vec[a] = W[a * ldw + i];
+        vec[C] = 0.0;
+        vec[C + 1] = Y[(int64_t)f * ldy + i];
+        int s = 0;
+#pragma unroll
+        for (int a = 0; a < L::R; ++a) {
+#pragma unroll
+            for (int b = a; b < L::R; ++b) {
+                if (a == C || b == C) continue;
+                acc[s] = fma(hi * vec[a], vec[b], acc[s]);
+                ++s;
+            }
+        }
+    }
+    __shared__ double red[L::NS][8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int s = 0; s < L::NS; ++s) {
+        const double v = warp_sum(acc[s]);
+        if (lane == 0) red[s][w] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < L::NS) {
+        double t = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += red[threadIdx.x][k];
+        S[((int64_t)r * phi + f) * L::NS + threadIdx.x] = t;
+    }
+}
+
+// ---------------------------------------------------------------- null model
+// One CTA per phenotype runs _golden_section_minimize (likelihood.py:395-474) over
+// -mle_log_likelihood_null (349-392): all threads evaluate, thread-uniform control.
+template <int C>
+__device__ double null_mle_eval(int64_t n, const double* W, int64_t ldw, const double* y,
+                                const double* evals, double lam, double c_mle, double* red) {
+    using L = Lay<C>;
+    double acc[L::NS];
+#pragma unroll
+    for (int s = 0; s < L::NS; ++s) acc[s] = 0.0;
+    double ld = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const double v = __dadd_rn(__dmul_rn(lam, evals[i]), 1.0);
+        const double hi = 1.0 / v;
+        ld += log(fabs(v));
+        double vec[L::R];
+#pragma unroll
+        for (int a = 0; a < C; ++a) vec[a] = W[a * ldw + i];
+        vec[C] = 0.0;
+        vec[C + 1] = y[i];
+        int s = 0;
+#pragma unroll
+        for (int a = 0; a < L::R; ++a) {
+#pragma unroll
+            for (int b = a; b < L::R; ++b) {
+                if (a == C || b == C) continue;
+                acc[s] = fma(hi * vec[a], vec[b], acc[s]);
+                ++s;
+            }
+        }
+    }
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < L::NS; ++s) {
+        const double v = warp_sum(acc[s]);
+        if (lane == 0) red[s * 32 + w] = v;
+    }
+    {
+        const double v = warp_sum(ld);
+        if (lane == 0) red[L::NS * 32 + w] = v;
+    }
+    __syncthreads();
+    double tot[L::NS + 1];
+#pragma unroll
+    for (int s = 0; s <= L::NS; ++s) {
+        double t = 0.0;
+        for (int k = 0; k < nw; ++k) t += red[s * 32 + k];
+        tot[s] = t;
+    }
+    double row0[L::NI];
+    double xs[L::NX];
+#pragma unroll
+    for (int k = 0; k < L::NX; ++k) xs[k] = 0.0;
+    assemble<C>(row0, tot, xs);
+    const PabOut<C> pb = pab_reduce<C>(row0);
+    const double pyy = clamp_pyy(pb.yy);  // level n_cvt for the null model
+    const double f = __dsub_rn(c_mle, __dmul_rn(0.5, tot[L::NS]));
+    return __dsub_rn(f, __dmul_rn(__dmul_rn(0.5, (double)n), log(pyy)));
+}
+
+template <int C>
+__global__ void null_mle_kernel(int64_t n, const double* W, int64_t ldw, const double* Y,
+                                int64_t ldy, const double* evals, double lo, double step,
+                                int n_grid, int n_iter, double log_hi, double c_mle, double* lam0,
+                                double* logl0) {
+    __shared__ double red[(Lay<C>::NS + 1) * 32];
+    const int f = blockIdx.x;
+    const double* y = Y + (int64_t)f * ldy;
+    auto func = [&](double lam) {
+        return -null_mle_eval<C>(n, W, ldw, y, evals, lam, c_mle, red);
+    };
+    int best_i = 0;
+    double best_v = func(exp(lo));
+    for (int i = 1; i < n_grid; ++i) {
+        const double v = func(exp(__dadd_rn(lo, __dmul_rn((double)i, step))));
+        if (v < best_v) {
+            best_v = v;
+            best_i = i;
+        }
+    }
+    const int il = best_i - 1 > 0 ? best_i - 1 : 0;
+    const int ih = best_i + 1 < n_grid - 1 ? best_i + 1 : n_grid - 1;
+    double a = __dadd_rn(lo, __dmul_rn((double)il, step));
+    double b = __dadd_rn(lo, __dmul_rn((double)ih, step));
+    double c = __dsub_rn(b, __dmul_rn(kPhi, __dsub_rn(b, a)));
+    double d = __dadd_rn(a, __dmul_rn(kPhi, __dsub_rn(b, a)));
+    double fc = func(exp(c)), fd = func(exp(d));
+    for (int it = 0; it < n_iter; ++it) {
+        if (fc < fd) {
+            b = d;
+            d = c;
+            fd = fc;
+            c = __dsub_rn(b, __dmul_rn(kPhi, __dsub_rn(b, a)));
+            fc = func(exp(c));
+        } else {
+            a = c;
+            c = d;
+            fc = fd;
+            d = __dadd_rn(a, __dmul_rn(kPhi, __dsub_rn(b, a)));
+            fd = func(exp(d));
+        }
+    }
+    const double opt = exp(__dmul_rn(__dadd_rn(a, b), 0.5));
+    const double v = func(opt);
+    if (threadIdx.x == 0) {
+        lam0[f] = opt;
+        logl0[f] = -v;
+    }
+}
+
+// ---------------------------------------------------------------- host helpers
+struct WsLayout {
+    int64_t loglam, logdet, H, S, total;
+};
+
+inline int64_t align256(int64_t b) { return (b + 255) / 256 * 256; }
+
+inline int ns_of(int c) { return (c + 2) * (c + 1) / 2; }
+
+inline WsLayout ws_layout(int64_t n, int c, int phi, int n_grid) {
+    WsLayout w;
+    int64_t off = 0;
+    w.loglam = off;
+    off += align256(8 * (int64_t)n_grid);
+    w.logdet = off;
+    off += align256(8 * (int64_t)n_grid);
+    w.H = off;
+    off += align256(8 * (int64_t)(n_grid + phi) * n);
+    w.S = off;
+    off += align256(8 * (int64_t)(n_grid + 1 + phi) * phi * ns_of(c));
+    w.total = off;
+    return w;
+}
+
+// numpy.linspace(start, stop, num): start + i*step, last element = stop.
+__global__ void linspace_kernel(double* out, double start, double stop, int num) {
+    const int i = threadIdx.x + blockIdx.x * blockDim.x;
+    if (i >= num) return;
+    if (num == 1) {
+        out[0] = start;
+        return;
+    }
+    const double step = (stop - start) / (double)(num - 1);
+    out[i] = (i == num - 1) ? stop : __dadd_rn(__dmul_rn((double)i, step), start);
+}
+
+template <int C>
+int32_t launch_pairs(const Params& p, cudaStream_t st) {
+    constexpr int GB = (C <= 1) ? 8 : (C == 2 ? 6 : 5);
+    const int64_t warps = p.m * p.phi;
+    const int64_t blocks = ceil_div(warps * 32, 256);
+    lmm_pairs_kernel<C, GB><<<(unsigned)blocks, 256, 0, st>>>(p);
+    JB_LAUNCH_CHECK("lmm_pairs_kernel");
+    return JB_OK;
+}
+
+template <int C>
+int32_t launch_prepare(int64_t n, int phi, int n_grid, const double* evals, const double* W,
+                       int64_t ldw, const double* Y, int64_t ldy, const double* lam0,
+                       double l_min, double l_max, uint8_t* ws, cudaStream_t st) {
+    const WsLayout L = ws_layout(n, C, phi, n_grid);
+    double* loglam = reinterpret_cast<double*>(ws + L.loglam);
+    double* logdet = reinterpret_cast<double*>(ws + L.logdet);
+    double* H = reinterpret_cast<double*>(ws + L.H);
+    double* S = reinterpret_cast<double*>(ws + L.S);
+    linspace_kernel<<<(n_grid + 127) / 128, 128, 0, st>>>(loglam, std::log(l_min), std::log(l_max),
+                                                        n_grid);
+    JB_LAUNCH_CHECK("linspace_kernel");
+    const int rows_h = n_grid + (lam0 ? phi : 0);
+    lmm_table_kernel<<<rows_h, 256, 0, st>>>(n, n_grid, phi, evals, loglam, lam0, H, logdet);
+    JB_LAUNCH_CHECK("lmm_table_kernel");
+    const int rows_s = n_grid + 1 + (lam0 ? phi : 0);
+    lmm_shared_kernel<C><<<dim3(rows_s, phi), 256, 0, st>>>(n, n_grid, phi, W, ldw, Y, ldy, H, S);
+    JB_LAUNCH_CHECK("lmm_shared_kernel");
+    return JB_OK;
+}
+
+}  // namespace lmm
+}  // namespace jb
+
+using namespace jb;
+using namespace jb::lmm;
+
+extern "C" {
+
+int64_t jb_lmm_workspace_size(int64_t n, int32_t n_cvt, int32_t phi, int32_t n_grid) {
+    if (n <= 0 || n_cvt < 1 || phi < 1 || n_grid < 1) return -1;
+    return ws_layout(n, n_cvt, phi, n_grid).total;
+}
+
+int32_t jb_lmm_prepare(int32_t lmm_mode, int64_t n, int32_t n_cvt, int32_t phi,
+                       const double* evals, const double* UtW, int64_t ldw, const double* Uty,
+                       int64_t ldy, const double* lam0, double l_min, double l_max,
+                       int32_t n_grid, void* workspace, int64_t workspace_bytes,
+                       uintptr_t stream) {
+    JB_CHECK_ARG(lmm_mode >= 1 && lmm_mode <= 4, "jb_lmm_prepare: lmm_mode must be 1..4");
+    JB_CHECK_ARG(n > 0 && phi >= 1 && n_grid >= 2, "jb_lmm_prepare: bad sizes");
+    JB_CHECK_ARG(n_cvt >= 1 && n_cvt <= kMaxCvt, "jb_lmm_prepare: n_cvt must be in 1..%d", kMaxCvt);
+    JB_CHECK_ARG(n > n_cvt + 1, "jb_lmm_prepare: n must exceed n_cvt + 1");
+    JB_CHECK_ARG(ldw >= n && ldy >= n, "jb_lmm_prepare: bad leading dimension");
+    JB_CHECK_ARG(l_min > 0 && l_max > l_min, "jb_lmm_prepare: need 0 < l_min < l_max");
+    JB_CHECK_ARG(lmm_mode == 1 || lam0, "jb_lmm_prepare: modes 2-4 need lam0");
+    JB_CHECK_ARG(workspace_bytes >= jb_lmm_workspace_size(n, n_cvt, phi, n_grid),
+                 "jb_lmm_prepare: workspace too small");
+    JB_CHECK_ARG(phi <= 65535, "jb_lmm_prepare: too many phenotypes");
+    cudaStream_t st = as_stream(stream);
+    uint8_t* ws = static_cast<uint8_t*>(workspace);
+    const double* l0 = lmm_mode == 1 ? nullptr : lam0;
+    switch (n_cvt) {
+        case 1: return launch_prepare<1>(n, phi, n_grid, evals, UtW, ldw, Uty, ldy, l0, l_min, l_max, ws, st);
+        case 2: return launch_prepare<2>(n, phi, n_grid, evals, UtW, ldw, Uty, ldy, l0, l_min, l_max, ws, st);
+        case 3: return launch_prepare<3>(n, phi, n_grid, evals, UtW, ldw, Uty, ldy, l0, l_min, l_max, ws, st);
+        case 4: return launch_prepare<4>(n, phi, n_grid, evals, UtW, ldw, Uty, ldy, l0, l_min, l_max, ws, st);
+    }
+    return JB_E_UNSUPPORTED;
+}
+
+int32_t jb_lmm_chunk(int32_t lmm_mode, int64_t n, int32_t n_cvt, int32_t phi, int64_t m,
+                     const double* evals, const double* UtW, int64_t ldw, const double* Uty,
+                     int64_t ldy, const double* UtG, int64_t ldg, const double* lam0,
+                     const double* logl0, double l_min, double l_max, int32_t n_grid,
+                     int32_t n_iter, jb_lmm_out out, void* workspace, int64_t workspace_bytes,
+                     uintptr_t stream) {
+    (void)lam0;
+    JB_CHECK_ARG(lmm_mode >= 1 && lmm_mode <= 4, "jb_lmm_chunk: lmm_mode must be 1..4");
+    JB_CHECK_ARG(n > 0 && phi >= 1 && m >= 0 && n_grid >= 2 && n_iter >= 0, "jb_lmm_chunk: bad sizes");
+    JB_CHECK_ARG(n_cvt >= 1 && n_cvt <= kMaxCvt, "jb_lmm_chunk: n_cvt must be in 1..%d", kMaxCvt);
+    JB_CHECK_ARG(n > n_cvt + 1, "jb_lmm_chunk: n must exceed n_cvt + 1");
+    JB_CHECK_ARG(ldw >= n && ldy >= n && ldg >= n, "jb_lmm_chunk: bad leading dimension");
+    JB_CHECK_ARG(l_min > 0 && l_max > l_min, "jb_lmm_chunk: need 0 < l_min < l_max");
+    JB_CHECK_ARG(lmm_mode != 2 && lmm_mode != 4 ? true : logl0 != nullptr,
+                 "jb_lmm_chunk: modes 2 and 4 need logl0");
+    JB_CHECK_ARG(workspace_bytes >= jb_lmm_workspace_size(n, n_cvt, phi, n_grid),
+                 "jb_lmm_chunk: workspace too small");
+    if (m == 0) return JB_OK;
+    const WsLayout L = ws_layout(n, n_cvt, phi, n_grid);
+    uint8_t* ws = static_cast<uint8_t*>(workspace);
+    Params p;
+    p.mode = lmm_mode;
+    p.n = n;
+    p.phi = phi;
+    p.m = m;
+    p.evals = evals;
+    p.W = UtW;
+    p.ldw = ldw;
+    p.Y = Uty;
+    p.ldy = ldy;
+    p.G = UtG;
+    p.ldg = ldg;
+    p.logl0 = logl0;
+    p.n_grid = n_grid;
+    p.n_iter = n_iter;
+    p.loglam = reinterpret_cast<const double*>(ws + L.loglam);
+    p.logdet = reinterpret_cast<const double*>(ws + L.logdet);
+    p.H = reinterpret_cast<const double*>(ws + L.H);
+    p.S = reinterpret_cast<const double*>(ws + L.S);
+    const double df = (double)(n - n_cvt - 1);
+    p.df = df;
+    p.n_d = (double)n;
+    p.c_reml = 0.5 * df * (std::log(df) - std::log(2 * M_PI) - 1.0);
+    p.c_mle = 0.5 * (double)n * (std::log((double)n) - std::log(2 * M_PI) - 1.0);
+    p.out = out;
+    cudaStream_t st = as_stream(stream);
+    switch (n_cvt) {
+        case 1: return launch_pairs<1>(p, st);
+        case 2: return launch_pairs<2>(p, st);
+        case 3: return launch_pairs<3>(p, st);
+        case 4: return launch_pairs<4>(p, st);
+    }
+    return JB_E_UNSUPPORTED;
+}
+
+int32_t jb_null_mle(int64_t n, int32_t n_cvt, int32_t phi, const double* evals, const double* UtW,
+                    int64_t ldw, const double* Uty, int64_t ldy, double l_min, double l_max,
+                    int32_t n_grid, int32_t n_iter, double* lam0, double* logl0,
+                    uintptr_t stream) {
+    JB_CHECK_ARG(n > 0 && phi >= 1 && n_grid >= 2 && n_iter >= 0, "jb_null_mle: bad sizes");
+    JB_CHECK_ARG(n_cvt >= 1 && n_cvt <= kMaxCvt, "jb_null_mle: n_cvt must be in 1..%d", kMaxCvt);
+    JB_CHECK_ARG(ldw >= n && ldy >= n, "jb_null_mle: bad leading dimension");
+    JB_CHECK_ARG(l_min > 0 && l_max > l_min, "jb_null_mle: need 0 < l_min < l_max");
+    const double lo = std::log(l_min), hi = std::log(l_max);
+    const double step = (hi - lo) / (double)(n_grid - 1);
+    const double c_mle = 0.5 * (double)n * (std::log((double)n) - std::log(2 * M_PI) - 1.0);
+    cudaStream_t st = as_stream(stream);
+    switch (n_cvt) {
+#define JB_NULL_CASE(CC)                                                                     \
+    case CC:                                                                                 \
+        null_mle_kernel<CC><<<phi, 256, 0, st>>>(n, UtW, ldw, Uty, ldy, evals, lo, step,     \
+                                                 n_grid, n_iter, hi, c_mle, lam0, logl0);    \
+        JB_LAUNCH_CHECK("null_mle_kernel");                                                  \
+        return JB_OK;
+        JB_NULL_CASE(1)
+        JB_NULL_CASE(2)
+        JB_NULL_CASE(3)
+        JB_NULL_CASE(4)
+#undef JB_NULL_CASE
+    }
+    return JB_E_UNSUPPORTED;
+}
+
+}  // extern "C"

@@ -1,0 +1,171 @@
+"""Device-resident association engine.
+
+A :class:`DeviceCohort` keeps one cohort on the GPU -- eigenvalues, eigenvectors,
+rotated covariates and phenotypes, the per-phenotype null model and the prepared
+lambda-grid tables -- so that any number of SNP chunks (and, in the serving loop,
+new phenotypes or jobs) reuse them without another eigendecomposition.
+
+Per chunk the pipeline is: packed .bed records -> ``jb_decode_bed`` (int8 codes +
+per-SNP counts) -> ``jb_impute_f64`` (mean imputation, no centering) ->
+``jb_rotate_f64`` (U^T G) -> ``jb_lmm_chunk`` (per-SNP search and statistics).
+This restates ``run_lmm_association_streaming``'s device loop
+(src/jamma/lmm/runner_streaming.py:412-586) with every step on the GPU.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from jamma_b200 import _native
+from jamma_b200.device import colmajor, empty, ptr, require_cuda, stream_handle, workspace
+
+OUT_KEYS = ("lambda_remle", "logl_h1", "beta", "se", "p_wald", "lambda_mle", "logl_mle",
+            "p_lrt", "p_score")
+MODE_KEYS = {
+    1: ("lambda_remle", "logl_h1", "beta", "se", "p_wald"),
+    2: ("lambda_mle", "logl_mle", "p_lrt"),
+    3: ("beta", "se", "p_score"),
+    4: OUT_KEYS,
+}
+MAX_CVT = 4
+
+# The null model always runs with jamma's defaults: compute_null_model_mle is called
+# without the user's lambda range (src/jamma/lmm/prepare.py:143).
+NULL_L_MIN, NULL_L_MAX, NULL_N_GRID, NULL_N_ITER = 1e-5, 1e5, 50, 20
+
+
+def eigh_device(K: torch.Tensor, threshold: float = 1e-10) -> tuple[torch.Tensor, torch.Tensor]:
+    """In-place FP64 eigendecomposition of a device (n, n) symmetric matrix.
+
+    Returns (eigenvalues (n,), eigenvectors as a column-major (n, n) tensor)."""
+    require_cuda()
+    n = K.shape[0]
+    w = empty((n,))
+    ws = workspace(_native.load().jb_eigh_workspace_size(n))
+    _native.call("jb_eigh_f64", ptr(K), n, n, ptr(w), float(threshold), ptr(ws), ws.numel(),
+                 stream_handle())
+    return w, K
+
+
+def rotate(U: torch.Tensor, B: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+    """U^T B for column-major U (n, n) and B (m, n) -> (m, n) column-major result."""
+    n = U.shape[0]
+    m = B.shape[0]
+    if out is None:
+        out = empty((m, n))
+    _native.call("jb_rotate_f64", ptr(U), n, n, ptr(B), m, n, ptr(out), n, stream_handle())
+    return out
+
+
+class DeviceCohort:
+    """One cohort's resident state for association testing.
+
+    Args:
+        eigenvalues: (n,) thresholded eigenvalues (host array or device tensor).
+        eigenvectors: (n, n) host array with eigenvectors as columns, or a device tensor
+            already in column-major layout (as returned by :func:`eigh_device`).
+        covariates: (n, c) host matrix W (c in 1..4), or None for an intercept.
+        phenotypes: (n,) or (n, phi) host phenotypes (already restricted to analysed
+            samples; every phenotype shares the sample set).
+    """
+
+    def __init__(self, eigenvalues, eigenvectors, covariates, phenotypes, lmm_mode=1,
+                 l_min=1e-5, l_max=1e5, n_grid=50, n_refine=10):
+        require_cuda()
+        if lmm_mode not in (1, 2, 3, 4):
+            raise ValueError(f"lmm_mode must be 1, 2, 3 or 4, got {lmm_mode}")
+        y = np.asarray(phenotypes, dtype=np.float64)
+        if y.ndim == 1:
+            y = y[:, None]
+        n, phi = y.shape
+        W = np.ones((n, 1)) if covariates is None else np.asarray(covariates, dtype=np.float64)
+        if W.ndim == 1:
+            W = W[:, None]
+        c = W.shape[1]
+        if n <= c + 1:
+            raise ValueError(
+                f"Over-parameterized model: {n} samples with {c} covariates leaves "
+                f"df={n - c - 1} (need at least {c + 2} samples)"
+            )
+        if c > MAX_CVT:
+            raise ValueError(f"at most {MAX_CVT} covariate columns are supported, got {c}")
+        self.n, self.c, self.phi, self.mode = n, c, phi, lmm_mode
+        self.l_min, self.l_max, self.n_grid = float(l_min), float(l_max), int(n_grid)
+        self.n_iter = max(int(n_refine), 20)
+        self.evals = (eigenvalues if isinstance(eigenvalues, torch.Tensor)
+                      else colmajor(np.asarray(eigenvalues, dtype=np.float64)))
+        self.U = (eigenvectors if isinstance(eigenvectors, torch.Tensor)
+                  else colmajor(np.asarray(eigenvectors, dtype=np.float64)))
+        if self.U.shape != (n, n) or self.evals.shape != (n,):
+            raise ValueError("eigendecomposition does not match the number of samples")
+        self.UtW = rotate(self.U, colmajor(W))
+        self.Uty = rotate(self.U, colmajor(y))
+        self.lam0 = self.logl0 = None
+        st = stream_handle()
+        if lmm_mode in (2, 3, 4):
+            self.lam0 = empty((phi,))
+            self.logl0 = empty((phi,))
+            _native.call("jb_null_mle", n, c, phi, ptr(self.evals), ptr(self.UtW), n, ptr(self.Uty),
+                         n, NULL_L_MIN, NULL_L_MAX, NULL_N_GRID, NULL_N_ITER, ptr(self.lam0),
+                         ptr(self.logl0), st)
+        self.ws = workspace(_native.load().jb_lmm_workspace_size(n, c, phi, self.n_grid))
+        _native.call("jb_lmm_prepare", lmm_mode, n, c, phi, ptr(self.evals), ptr(self.UtW), n,
+                     ptr(self.Uty), n, ptr(self.lam0), self.l_min, self.l_max, self.n_grid,
+                     ptr(self.ws), self.ws.numel(), st)
+
+    # ------------------------------------------------------------ null model
+    def null_model(self) -> tuple[np.ndarray | None, np.ndarray | None]:
+        if self.lam0 is None:
+            return None, None
+        return self.lam0.cpu().numpy(), self.logl0.cpu().numpy()
+
+    # ------------------------------------------------------------ per chunk
+    def alloc_out(self, m: int) -> dict[str, torch.Tensor]:
+        return {k: empty((self.phi, m)) for k in MODE_KEYS[self.mode]}
+
+    def associate_rotated(self, UtG: torch.Tensor, out: dict | None = None) -> dict:
+        """Statistics for a rotated chunk UtG (m, n) column-major; outputs (phi, m)."""
+        m = UtG.shape[0]
+        out = out if out is not None else self.alloc_out(m)
+        o = _native.LmmOut(**{k: ptr(out.get(k)) for k in OUT_KEYS})
+        _native.call("jb_lmm_chunk", self.mode, self.n, self.c, self.phi, m, ptr(self.evals),
+                     ptr(self.UtW), self.n, ptr(self.Uty), self.n, ptr(UtG), self.n,
+                     ptr(self.lam0), ptr(self.logl0), self.l_min, self.l_max, self.n_grid,
+                     self.n_iter, o, ptr(self.ws), self.ws.numel(), stream_handle())
+        return out
+
+    def associate_genotypes(self, G: torch.Tensor, out: dict | None = None,
+                            scratch: torch.Tensor | None = None) -> dict:
+        """Rotate imputed genotypes G (m, n) and run the statistics."""
+        UtG = rotate(self.U, G, out=scratch)
+        return self.associate_rotated(UtG, out)
+
+    def associate_codes(self, codes: torch.Tensor, means: torch.Tensor, out: dict | None = None,
+                        bufs: dict | None = None) -> dict:
+        """Decoded int8 codes (m, ld) + per-SNP imputation means (m,) -> statistics."""
+        m, ld = codes.shape
+        bufs = bufs if bufs is not None else {}
+        G = bufs.get("G")
+        if G is None or G.shape[0] < m:
+            G = empty((m, self.n))
+        G = G[:m]
+        _native.call("jb_impute_f64", ptr(codes), ld, self.n, m, ptr(means), ptr(G), self.n,
+                     stream_handle())
+        UtG = bufs.get("UtG")
+        UtG = UtG[:m] if UtG is not None and UtG.shape[0] >= m else None
+        return self.associate_genotypes(G, out, UtG)
+
+
+def decode_packed(packed: torch.Tensor, n_file: int, sample_idx: torch.Tensor | None, n: int,
+                  ld: int | None = None) -> tuple[torch.Tensor, torch.Tensor]:
+    """Device decode of (m, bytes_per_snp) packed records -> codes (m, ld) + counts (m, 4)."""
+    m, bps = packed.shape
+    ld = n if ld is None else ld
+    codes = torch.empty((m, ld), dtype=torch.int8, device="cuda")
+    counts = torch.empty((m, 4), dtype=torch.int32, device="cuda")
+    if sample_idx is None and n != n_file:
+        raise ValueError("sample_idx is required when n differs from the file's sample count")
+    _native.call("jb_decode_bed", ptr(packed), bps, m, ptr(sample_idx), n, ptr(codes), ld,
+                 ptr(counts), stream_handle())
+    return codes, counts

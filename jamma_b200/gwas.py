@@ -1,0 +1,91 @@
+"""One-call GWAS pipeline with jamma's ``gwas()`` signature (src/jamma/gwas.py:40-167).
+
+Steps follow ``PipelineRunner.run`` (src/jamma/pipeline.py:426-609): phenotypes from
+the .fam column, kinship from file or computed from the .bed (all samples, streamed),
+covariates, then the streaming association written to ``{output_dir}/{prefix}.assoc.txt``.
+"""
+
+from __future__ import annotations
+
+import time
+from dataclasses import dataclass, field
+from pathlib import Path
+
+import numpy as np
+
+from jamma_b200.io import (
+    AssocResult,
+    get_plink_metadata,
+    read_covariate_file,
+    read_kinship_matrix,
+    read_phenotypes,
+    write_kinship_matrix,
+)
+from jamma_b200.kinship import compute_kinship_from_bed
+from jamma_b200.lmm import run_lmm_association_streaming
+
+
+@dataclass
+class GWASResult:
+    associations: list[AssocResult]
+    n_samples: int
+    n_snps_tested: int
+    timing: dict[str, float] = field(default_factory=dict)
+
+
+def _read_snp_list(path) -> list[str]:
+    with open(path) as f:
+        return [line.split()[0] for line in f if line.strip()]
+
+
+def gwas(bfile, *, kinship_file=None, covariate_file=None, lmm_mode: int = 1, maf: float = 0.01,
+         miss: float = 0.05, output_dir="output", output_prefix: str = "result",
+         save_kinship: bool = False, check_memory: bool = True, show_progress: bool = True,
+         loco: bool = False, eigenvalue_file=None, eigenvector_file=None, write_eigen: bool = False,
+         phenotype_column: int = 1, snps_file=None, ksnps_file=None, hwe: float = 0.0) -> GWASResult:
+    if lmm_mode not in (1, 2, 3, 4):
+        raise ValueError(f"lmm_mode must be 1, 2, 3 or 4, got {lmm_mode}")
+    if loco and kinship_file is not None:
+        raise ValueError("kinship_file and loco are mutually exclusive")
+    if (eigenvalue_file is None) != (eigenvector_file is None):
+        raise ValueError("eigenvalue_file and eigenvector_file must be provided together")
+    if loco:
+        raise NotImplementedError("LOCO association is not available in this build")
+    t0 = time.perf_counter()
+    bfile = Path(bfile)
+    meta = get_plink_metadata(bfile)
+    n = meta["n_samples"]
+    y = read_phenotypes(bfile, phenotype_column)
+    sid = list(meta["sid"])
+    pos = {s: i for i, s in enumerate(sid)}
+    snps_idx = None
+    if snps_file is not None:
+        snps_idx = np.array(sorted(pos[s] for s in _read_snp_list(snps_file) if s in pos), dtype=np.int64)
+    evals = evecs = K = None
+    if eigenvalue_file is not None:
+        evals = np.loadtxt(eigenvalue_file, dtype=np.float64)
+        evecs = np.loadtxt(eigenvector_file, dtype=np.float64)
+    elif kinship_file is not None:
+        K = read_kinship_matrix(kinship_file, n_samples=n)
+    else:
+        if ksnps_file is not None:
+            raise NotImplementedError("-ksnps kinship restriction is not available in this build")
+        K = compute_kinship_from_bed(bfile)
+        if save_kinship:
+            write_kinship_matrix(K, Path(output_dir) / f"{output_prefix}.cXX.txt")
+    t_k = time.perf_counter()
+    cov = None
+    if covariate_file is not None:
+        cov, _ = read_covariate_file(covariate_file)
+        if cov.shape[0] != n:
+            raise ValueError(f"Covariate file has {cov.shape[0]} rows but .fam has {n} samples")
+    out = Path(output_dir) / f"{output_prefix}.assoc.txt"
+    timing: dict = {}
+    res = run_lmm_association_streaming(
+        bfile, y, kinship=K, covariates=cov, eigenvalues=evals, eigenvectors=evecs,
+        maf_threshold=maf, miss_threshold=miss, output_path=out, lmm_mode=lmm_mode,
+        snps_indices=snps_idx, hwe_threshold=hwe, timing=timing)
+    t_end = time.perf_counter()
+    n_valid = int(np.sum(~np.isnan(y) & (y != -9.0)))
+    return GWASResult(res, n_valid, meta["n_snps"],
+                      {"kinship_s": t_k - t0, "lmm_s": t_end - t_k, "total_s": t_end - t0, **timing})

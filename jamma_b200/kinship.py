@@ -1,0 +1,135 @@
+"""Centered kinship (GEMMA -gk 1) on the GPU.
+
+``compute_centered_kinship`` keeps jamma's signature and semantics
+(src/jamma/kinship/compute.py:93-226): SNPs are filtered by MAF / missing rate /
+monomorphism with statistics in the input dtype, each kept SNP is mean-imputed and
+centred with its float64 mean over observed samples, and K = Xc Xc^T / p_kept.
+Genotypes travel to the device as packed 2-bit records and are decoded there.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from jamma_b200 import _native
+from jamma_b200.device import empty, ptr, require_cuda, stream_handle, workspace
+from jamma_b200.engine import decode_packed
+from jamma_b200.io import BedFile, pack_genotypes
+
+
+def snp_stats_from_counts(counts: np.ndarray, n: int, dtype=np.float32):
+    """(mean, miss, polymorphic) from device counts {n_obs, sum, n_het, n_hom2}.
+
+    The mean is NumPy's ``nanmean`` in ``dtype``: the integer sum divided by the count
+    in float64, then stored in ``dtype`` (0 for all-missing SNPs).  ``polymorphic`` is
+    ``nanvar > 0``: at least two different observed genotypes.
+    """
+    n_obs = counts[:, 0].astype(np.int64)
+    s = counts[:, 1].astype(np.float64)
+    het = counts[:, 2].astype(np.int64)
+    hom2 = counts[:, 3].astype(np.int64)
+    hom0 = n_obs - het - hom2
+    with np.errstate(invalid="ignore", divide="ignore"):
+        mean = np.where(n_obs > 0, s / np.maximum(n_obs, 1), 0.0).astype(dtype)
+    poly = ((hom0 > 0).astype(int) + (het > 0) + (hom2 > 0)) >= 2
+    return mean, (n - n_obs).astype(np.int64), poly
+
+
+def filter_mask(mean, miss, poly, n, maf_threshold, miss_threshold):
+    """``compute_snp_filter_mask`` (src/jamma/core/snp_filter.py:59-91)."""
+    af = np.asarray(mean, dtype=np.float64) / 2.0
+    maf = np.minimum(af, 1.0 - af)
+    keep = (maf >= maf_threshold) & ((miss / n) <= miss_threshold) & poly
+    return keep, af
+
+
+class _KinshipAccumulator:
+    """FP64 centered Gram accumulated over SNP batches (``_accumulate_kinship``)."""
+
+    def __init__(self, n: int, batch: int):
+        self.n, self.batch = n, batch
+        self.K = torch.zeros((n, n), dtype=torch.float64, device="cuda")
+        self.ws = workspace(_native.load().jb_kinship_f64_workspace_size(n, batch))
+        self.p = 0
+
+    def add(self, codes: torch.Tensor, means64: torch.Tensor) -> None:
+        m, ld = codes.shape
+        for s in range(0, m, self.batch):
+            e = min(s + self.batch, m)
+            _native.call("jb_kinship_accumulate_f64", ptr(codes[s:e]), ld, self.n, e - s,
+                         ptr(means64[s:e]), ptr(self.K), self.n, ptr(self.ws), self.ws.numel(),
+                         stream_handle())
+        self.p += m
+
+    def finish(self) -> torch.Tensor:
+        _native.call("jb_kinship_finalize", ptr(self.K), self.n, self.n, 1.0 / self.p,
+                     stream_handle())
+        return self.K
+
+
+def _kinship_from_packed(packed_dev: torch.Tensor, n: int, batch_size: int, maf_threshold: float,
+                         miss_threshold: float, stat_dtype) -> tuple[torch.Tensor, int]:
+    codes, counts = decode_packed(packed_dev, n, None, n)
+    mean, miss, poly = snp_stats_from_counts(counts.cpu().numpy(), n, stat_dtype)
+    keep, _ = filter_mask(mean, miss, poly, n, maf_threshold, miss_threshold)
+    idx = np.where(keep)[0]
+    if idx.size == 0:
+        raise ValueError(
+            f"No SNPs passed filtering (maf>={maf_threshold}, miss<={miss_threshold}, "
+            f"polymorphic). Original SNP count: {packed_dev.shape[0]}"
+        )
+    c = counts.cpu().numpy()[idx]
+    mu64 = torch.from_numpy(c[:, 1] / np.maximum(c[:, 0], 1)).to("cuda")  # float64 nanmean
+    sel = torch.from_numpy(idx).to("cuda")
+    acc = _KinshipAccumulator(n, max(1, min(batch_size, 8192)))
+    acc.add(codes.index_select(0, sel), mu64)
+    return acc.finish(), idx.size
+
+
+def compute_centered_kinship(genotypes: np.ndarray, batch_size: int = 10000,
+                             maf_threshold: float = 0.0, miss_threshold: float = 1.0,
+                             check_memory: bool = True) -> np.ndarray:
+    """GEMMA -gk 1 relatedness matrix of an in-memory (n, p) genotype matrix."""
+    require_cuda()
+    g = np.asarray(genotypes)
+    n = g.shape[0]
+    stat_dtype = np.float32 if g.dtype == np.float32 else np.float64
+    packed = torch.from_numpy(pack_genotypes(g)).to("cuda")
+    K, _ = _kinship_from_packed(packed, n, batch_size, maf_threshold, miss_threshold, stat_dtype)
+    return K.cpu().numpy()
+
+
+def compute_kinship_from_bed(bfile, maf_threshold: float = 0.0, miss_threshold: float = 1.0,
+                             chunk_size: int = 10000, sample_idx: np.ndarray | None = None,
+                             as_device: bool = False):
+    """Centered kinship streamed from a .bed file (``compute_kinship_streaming``,
+    src/jamma/kinship/compute.py:502-690): pass 1 statistics, pass 2 accumulation,
+    both decoded on the device.  Pass-1 means are float32 as in jamma's streaming path.
+    """
+    require_cuda()
+    bed = BedFile(bfile)
+    n = bed.n_samples if sample_idx is None else len(sample_idx)
+    sidx = None if sample_idx is None else torch.from_numpy(
+        np.asarray(sample_idx, dtype=np.int32)).to("cuda")
+    counts = []
+    for s in range(0, bed.n_snps, chunk_size):
+        rec = torch.from_numpy(bed.read(s, min(s + chunk_size, bed.n_snps))).to("cuda")
+        _, cnt = decode_packed(rec, bed.n_samples, sidx, n)
+        counts.append(cnt.cpu().numpy())
+    counts = np.concatenate(counts)
+    mean, miss, poly = snp_stats_from_counts(counts, n, np.float32)
+    keep, _ = filter_mask(mean, miss, poly, n, maf_threshold, miss_threshold)
+    idx = np.where(keep)[0]
+    if idx.size == 0:
+        raise ValueError("No SNPs passed filtering")
+    acc = _KinshipAccumulator(n, min(chunk_size, 8192))
+    for s in range(0, idx.size, chunk_size):
+        sub = idx[s : s + chunk_size]
+        rec = torch.from_numpy(bed.take(sub)).to("cuda")
+        codes, _ = decode_packed(rec, bed.n_samples, sidx, n)
+        c = counts[sub]
+        mu64 = torch.from_numpy(c[:, 1] / np.maximum(c[:, 0], 1)).to("cuda")
+        acc.add(codes, mu64)
+    K = acc.finish()
+    return K if as_device else K.cpu().numpy()
