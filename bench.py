@@ -183,29 +183,54 @@ def run_ours(args) -> None:
         dist.barrier()
     from jamma_b200 import _native, engine as eng, synth
     from jamma_b200.device import ptr, stream_handle
-    from jamma_b200.kinship import _KinshipAccumulator, snp_stats_from_counts
+    from jamma_b200.kinship import _KinshipAccumulator, _KinshipI8, snp_stats_from_counts
 
     n, m, c = args.n, args.chunk, args.n_cvt
     nsteps = args.warmup + args.steps
     bps = (n + 3) // 4
     st = torch.cuda.current_stream()
 
-    # ---------------- cohort set-up: kinship (FP64 Gram) + eigh, timed separately
+    # ---------------- cohort set-up: kinship (INT8 Gram and plain FP64 Gram) + eigh
     kin_p = args.kin_snps
     kin_rec = synth.packed_records_device(n, kin_p, args.miss, seed=100 + rank)
+    kc = 16384
+    kin_counts = []
+    for s in range(0, kin_p, kc):
+        _, cnt = eng.decode_packed(kin_rec[s:s + kc], n, None, n)
+        kin_counts.append(cnt.cpu().numpy())
+    kin_counts = np.concatenate(kin_counts)
+    poly = snp_stats_from_counts(kin_counts, n)[2]
+    keep = np.where(poly)[0]
+
+    def kinship(form: str):
+        acc = _KinshipI8(n, keep.size) if form == "int8" else _KinshipAccumulator(n, 4096)
+        for s in range(0, keep.size, kc):
+            sub = keep[s:s + kc]
+            codes_k, _ = eng.decode_packed(kin_rec.index_select(0, torch.from_numpy(sub).cuda()),
+                                           n, None, n)
+            cc = kin_counts[sub]
+            mu = torch.from_numpy(cc[:, 1] / np.maximum(cc[:, 0], 1)).cuda()
+            if form == "int8":
+                acc.add(codes_k, mu, bool(np.any(cc[:, 0] < n)))
+            else:
+                acc.add(codes_k, mu)
+        return acc.finish()
+
     torch.cuda.synchronize()
     t = time.perf_counter()
-    acc = _KinshipAccumulator(n, 4096)
-    for s in range(0, kin_p, 16384):
-        codes, cnt = eng.decode_packed(kin_rec[s:s + 16384], n, None, n)
-        cc = cnt.cpu().numpy()
-        poly = snp_stats_from_counts(cc, n)[2]
-        idx = torch.from_numpy(np.where(poly)[0]).cuda()
-        mu = torch.from_numpy(cc[:, 1] / np.maximum(cc[:, 0], 1)).cuda().index_select(0, idx)
-        acc.add(codes.index_select(0, idx), mu)
-    K = acc.finish()
+    K = kinship("int8")
     torch.cuda.synchronize()
     kinship_s = time.perf_counter() - t
+    kinship_fp64_s = None
+    if not args.skip_fp64_kinship:
+        t = time.perf_counter()
+        K64 = kinship("fp64")
+        torch.cuda.synchronize()
+        kinship_fp64_s = time.perf_counter() - t
+        kin_maxdiff = float((K64 - K).abs().max().item() / K64.abs().max().item())
+        del K64
+    else:
+        kin_maxdiff = None
     del kin_rec
     t = time.perf_counter()
     w, U = eng.eigh_device(K)
@@ -224,66 +249,85 @@ def run_ours(args) -> None:
         cc = cnt.cpu().numpy().astype(np.float64)
         means.append(torch.from_numpy((cc[:, 1] / np.maximum(cc[:, 0], 1)).astype(np.float32)
                                       .astype(np.float64)).cuda())
-    bufs = {"G": eng.empty((m, n)), "UtG": eng.empty((m, n))}
-    outs = cohort.alloc_out(m)
-    codes = torch.empty((m, n), dtype=torch.int8, device="cuda")
+    ld = (n + 127) // 128 * 128
+    G = eng.empty((m, n))
+    UtG = eng.empty((m, n))
+    codes = torch.empty((m, ld), dtype=torch.int8, device="cuda")
     counts = torch.empty((m, 4), dtype=torch.int32, device="cuda")
+    has_missing = args.miss > 0
 
-    ev = {k: [] for k in ("decode", "impute", "rotate", "lmm")}
+    def run_form(precision: str, steps: int):
+        """Warm up, then time `steps` chunks of one precision form with CUDA events."""
+        c = cohort_mixed if precision == "mixed" else cohort
+        outs = c.alloc_out(m)
+        ev = {k: [] for k in ("decode", "rotate", "lmm")}
 
-    def step(s, record=False):
         def mark():
             e = torch.cuda.Event(enable_timing=True)
             e.record(st)
             return e
-        e0 = mark()
-        _native.call("jb_decode_bed", ptr(rec[s * m:(s + 1) * m]), bps, m, None, n, ptr(codes), n,
-                     ptr(counts), stream_handle())
-        e1 = mark()
-        _native.call("jb_impute_f64", ptr(codes), n, n, m, ptr(means[s]), ptr(bufs["G"]), n,
-                     stream_handle())
-        e2 = mark()
-        eng.rotate(cohort.U, bufs["G"], out=bufs["UtG"])
-        e3 = mark()
-        cohort.associate_rotated(bufs["UtG"], outs)
-        e4 = mark()
-        if record:
-            for k, a, b in (("decode", e0, e1), ("impute", e1, e2), ("rotate", e2, e3), ("lmm", e3, e4)):
-                ev[k].append((a, b))
 
-    for s in range(args.warmup):
-        step(s)
-    torch.cuda.synchronize()
-    if world > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clk:
-        start.record(st)
-        for s in range(args.warmup, nsteps):
-            step(s, record=True)
-        end.record(st)
+        def step(s, record):
+            e0 = mark()
+            _native.call("jb_decode_bed", ptr(rec[s * m:(s + 1) * m]), bps, m, None, n, ptr(codes),
+                         ld, ptr(counts), stream_handle())
+            e1 = mark()
+            if precision == "mixed":
+                c.rotate_codes_i8(codes, means[s], has_missing, out=UtG)
+            else:
+                _native.call("jb_impute_f64", ptr(codes), ld, n, m, ptr(means[s]), ptr(G), n,
+                             stream_handle())
+                eng.rotate(c.U, G, out=UtG)
+            e2 = mark()
+            c.associate_rotated(UtG, outs)
+            e3 = mark()
+            if record:
+                for k, a, b in (("decode", e0, e1), ("rotate", e1, e2), ("lmm", e2, e3)):
+                    ev[k].append((a, b))
+
+        for s in range(args.warmup):
+            step(s, False)
         torch.cuda.synchronize()
-    ms = start.elapsed_time(end)
-    if world > 1:
-        tt = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
-        dist.barrier()
-    kern_ms = {k: float(np.mean([a.elapsed_time(b) for a, b in v])) for k, v in ev.items()}
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local) as clk:
+            a.record(st)
+            for s in range(args.warmup, args.warmup + steps):
+                step(s, True)
+            b.record(st)
+            torch.cuda.synchronize()
+        ms = a.elapsed_time(b)
+        if world > 1:
+            tt = torch.tensor([ms], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            ms = float(tt.item())
+            dist.barrier()
+        kern = {k: float(np.mean([x.elapsed_time(y) for x, y in v])) for k, v in ev.items()}
+        return ms, kern, clk.summary(), outs
+
+    cohort_mixed = eng.DeviceCohort(w, U, W, y, lmm_mode=args.mode, precision="mixed")
+    ms, kern_ms, clocks, outs = run_form("mixed", args.steps)
+    if c_status := cohort_mixed.rotate_status():
+        raise RuntimeError(f"INT8 rotation pipeline status {c_status}")
     snps = args.steps * m * world
     value = snps / (ms / 1e3)
+    fp64_steps = max(1, min(args.steps, args.fp64_steps))
+    ms64, kern64, _, _ = run_form("fp64", fp64_steps)
+    value64 = fp64_steps * m * world / (ms64 / 1e3)
 
-    # ---------------- end to end through the public chunk API with host buffers
+    # ---------------- end to end through the public chunk API with host buffers (mixed form)
     rec_h = rec[:m].cpu().pin_memory()
     mean_h = means[0].cpu()
     res_h = {k: torch.empty((1, m), dtype=torch.float64).pin_memory() for k in outs}
+    bufs = {"UtG": UtG}
 
     def e2e_step():
         rd = rec_h.to("cuda", non_blocking=True)
         md = mean_h.to("cuda", non_blocking=True)
-        cd, _ = eng.decode_packed(rd, n, None, n)
-        o = cohort.associate_codes(cd, md, out=outs, bufs=bufs)
+        cd, _ = eng.decode_packed(rd, n, None, n, ld=ld)
+        o = cohort_mixed.associate_codes(cd, md, out=outs, bufs=bufs, has_missing=has_missing)
         for k, v in o.items():
             res_h[k].copy_(v, non_blocking=True)
     for _ in range(2):
@@ -304,10 +348,12 @@ def run_ours(args) -> None:
 
     if rank == 0:
         peaks = _peaks()
-        # FP64 rotation roofline (dominant kernel in the plain form): 2 n^2 m flops/step
-        rot_flops = 2.0 * n * n * m
-        fp64_peak = args.fp64_peak_tflops
-        achieved = rot_flops / (kern_ms["rotate"] / 1e3) / 1e12
+        # dominant kernel of the mixed form: the INT8 tcgen05 rotation, 4 digit planes x
+        # (calls + missing masks) -> 2 * n^2 * m * 4 * (2 if missing) int8 ops per step
+        planes = 4 * (2 if has_missing else 1)
+        rot_ops = 2.0 * n * n * m * planes
+        i8_peak = args.int8_peak_tops
+        achieved = rot_ops / (kern_ms["rotate"] / 1e3) / 1e12
         evals_h = w.cpu().numpy()
         U_h = U.cpu().numpy().T
         lam0, l0 = cohort.null_model()
@@ -319,23 +365,27 @@ def run_ours(args) -> None:
         line = {
             "metric": "lmm_assoc_snps_per_s", "value": value, "unit": "SNPs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8+f64",
             "data": "synthetic (seeded device RNG; Binomial(2,p) genotypes, p~U(0.05,0.5))",
             "config": _config(args, m),
-            "gpu_launches": 3 * args.steps,
+            "gpu_launches": 4 * args.steps,
             "kernel_ms_per_step": kern_ms,
-            "kinship_s": kinship_s, "kinship_snps": kin_p, "eigh_s": eigh_s,
-            "roofline": {"kernel": "rotation U^T G (cuBLAS DGEMM, plain FP64 form)",
-                         "bound": "tensor", "achieved": achieved, "peak": fp64_peak,
-                         "unit": "TFLOP/s", "frac": achieved / fp64_peak, "traffic": None,
-                         "peak_source": "nominal B200 FP64 (no FP64 figure in MEASURED_PEAKS.json)"},
-            "search_kernel": {"kernel": "lmm_pairs_kernel (FP64 search+stats)",
+            "fp64_form": {"value": value64, "unit": "SNPs/s", "steps": fp64_steps,
+                          "kernel_ms_per_step": kern64, "speedup_mixed_vs_fp64": value / value64},
+            "kinship_s": kinship_s, "kinship_form": "int8 tcgen05 Gram + FP64 corrections",
+            "kinship_fp64_s": kinship_fp64_s, "kinship_snps": int(keep.size),
+            "kinship_int8_vs_fp64_max_rel_diff": kin_maxdiff, "eigh_s": eigh_s,
+            "roofline": {"kernel": "i8_gemm_kernel<rotate> (tcgen05 kind::i8, 4 digit planes)",
+                         "bound": "tensor", "achieved": achieved, "peak": i8_peak,
+                         "unit": "TOP/s", "frac": achieved / i8_peak, "traffic": None,
+                         "peak_source": args.int8_peak_source},
+            "search_kernel": {"kernel": "lmm_pairs_kernel (FP64 search + statistics)",
                               "ms_per_step": kern_ms["lmm"]},
             "cpu_baseline": cpu,
             "e2e": {"value": m / (e2e_ms / 1e3) * world, "unit": "SNPs/s",
                     "h2d_bytes_per_step": m * bps + m * 8,
                     "d2h_bytes_per_step": len(outs) * m * 8},
-            "clocks": clk.summary(),
+            "clocks": clocks,
             "hbm_peak_gbs": peaks.get("hbm_gbs", HBM_PEAK_FALLBACK),
         }
         print(json.dumps(line), flush=True)
@@ -355,12 +405,16 @@ def main():
     ap.add_argument("--mode", type=int, default=4)
     ap.add_argument("--chunk", type=int, default=8192)
     ap.add_argument("--miss", type=float, default=0.01)
-    ap.add_argument("--kin-snps", type=int, default=65536)
-    ap.add_argument("--precision", default="fp64", choices=["fp64"])
+    ap.add_argument("--kin-snps", type=int, default=500000)
+    ap.add_argument("--skip-fp64-kinship", action="store_true")
+    ap.add_argument("--precision", default="mixed", choices=["mixed"])
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--int8-peak-tops", type=float, default=4500.0)
+    ap.add_argument("--int8-peak-source", default="nominal B200 dense INT8 (4.5 POP/s); "
+                    "MEASURED_PEAKS.json has no INT8 figure")
     ap.add_argument("--cpu-snps", type=int, default=64)
     ap.add_argument("--ref-snps", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--fp64-peak-tflops", type=float, default=40.0)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

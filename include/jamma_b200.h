@@ -86,6 +86,42 @@ int32_t jb_kinship_accumulate_f64(const int8_t* codes, int64_t ld_codes, int64_t
 int32_t jb_kinship_finalize(double* K, int64_t n, int64_t ldk, double scale,
                             uintptr_t stream);
 
+/*
+ * Mixed-precision centered kinship.  Replaces the FP64 batch Gram of
+ * _accumulate_kinship (src/jamma/kinship/compute.py:46-57) with an exact INT8 tensor-core
+ * Gram plus FP64 corrections that reproduce impute_and_center
+ * (src/jamma/kinship/missing.py:22-61):
+ *   p K = Z Z^T - a 1^T - 1 a^T + (sum mu^2) 1 1^T - b 1^T - 1 b^T + R + R^T + T
+ * with Z the int8 calls (0 where missing), mu the per-SNP float64 means, M the missing
+ * mask, a = Z mu, b = M mu^2, R = Z diag(mu) M^T, T = M diag(mu^2) M^T.
+ *
+ * jb_codes_to_sample_major: transpose SNP-major codes (m x ld_codes) into the
+ *   sample-major Gram operand Zs[i*ldz + col0 + j] (missing -> 0; ldz multiple of 16)
+ *   and, if Cs != NULL, the raw sample-major codes Cs[i*ldcs + j] of this chunk.
+ * jb_gram_i8: C[j*ldc + i] = sum_k Zs[i,k] Zs[j,k] for i <= j (int32, exact; tcgen05
+ *   kind::i8).  Zs: n x p, row stride ldz bytes.  workspace: jb_gram_i8_workspace_size;
+ *   its first int32 is a status word (non-zero if a pipeline wait timed out), read with
+ *   jb_gram_status (synchronises the stream).
+ * jb_kinship_i8_corrections: accumulate a, b (n doubles each) and, when Cs is given
+ *   (the chunk has missing calls), R and T into RT (column-major n x 2n, ld ldr).
+ * jb_kinship_i8_finalize: K (n x n, ldk) = symmetric combination above / p_kept.
+ */
+int64_t jb_gram_i8_workspace_size(int64_t n);
+int32_t jb_gram_i8(const int8_t* Zs, int64_t n, int64_t p, int64_t ldz, int32_t* C,
+                   int64_t ldc, void* workspace, int64_t workspace_bytes, uintptr_t stream);
+int32_t jb_gram_status(const void* workspace, int32_t* out, uintptr_t stream);
+int32_t jb_codes_to_sample_major(const int8_t* codes, int64_t ld_codes, int64_t n,
+                                 int64_t m, int8_t* Zs, int64_t ldz, int64_t col0,
+                                 int8_t* Cs, int64_t ldcs, uintptr_t stream);
+int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes, const int8_t* Cs,
+                                  int64_t ldcs, int64_t n, int64_t m, const double* mu,
+                                  double* a, double* b, double* RT, int64_t ldr,
+                                  uintptr_t stream);
+int32_t jb_kinship_i8_finalize(const int32_t* C, int64_t ldc, int64_t n, const double* a,
+                               const double* b, double sum_mu2, const double* RT,
+                               int64_t ldr, int64_t p_kept, double* K, int64_t ldk,
+                               uintptr_t stream);
+
 /* ------------------------------------------------------------------ eigen */
 
 /*
@@ -108,6 +144,28 @@ int32_t jb_eigh_f64(double* A, int64_t n, int64_t lda, double* w, double thresho
  */
 int32_t jb_rotate_f64(const double* U, int64_t n, int64_t ldu, const double* B,
                       int64_t m, int64_t ldb, double* C, int64_t ldc, uintptr_t stream);
+
+/*
+ * Mixed-precision rotation on INT8 tensor cores (replaces the host UT @ G of
+ * src/jamma/lmm/runner_streaming.py:409).  jb_ozaki_prepare splits the eigenvectors U
+ * (n x n, column-major, ldu) once per cohort into four exact int8 digit planes with a
+ * per-eigenvector scale (ozaki workspace: jb_ozaki_workspace_size).  jb_rotate_i8 then
+ * forms X = U^T G for m SNPs given as decoded codes (SNP-major, ld_codes a multiple of
+ * 16; 3 = missing, mean-imputed with mean[j] without centring): every digit product
+ * accumulates exactly in int32 on tcgen05 and the epilogue recombines in FP64
+ * (|error| <= ~2^-29 max|U_col| * sum|g|).  has_missing = 0 promises the chunk holds
+ * no missing call.  workspace: jb_rotate_i8_workspace_size(n, m); its first int32 is a
+ * pipeline status word (0 = OK), read with jb_rotate_status (synchronises).
+ */
+int64_t jb_ozaki_workspace_size(int64_t n);
+int32_t jb_ozaki_prepare(const double* U, int64_t n, int64_t ldu, void* ozaki_ws,
+                         int64_t ozaki_bytes, uintptr_t stream);
+int64_t jb_rotate_i8_workspace_size(int64_t n, int64_t m);
+int32_t jb_rotate_i8(const void* ozaki_ws, int64_t n, const int8_t* codes, int64_t ld_codes,
+                     int64_t m, const double* mean, int32_t has_missing, double* X,
+                     int64_t ldx, void* workspace, int64_t workspace_bytes,
+                     uintptr_t stream);
+int32_t jb_rotate_status(const void* workspace, int32_t* out, uintptr_t stream);
 
 /* ------------------------------------------------------------------ association */
 
@@ -140,6 +198,12 @@ typedef struct jb_lmm_out {
  * (src/jamma/lmm/likelihood_jax.py:231-883) as driven by
  * src/jamma/lmm/runner_streaming.py:469-554.
  * workspace: jb_lmm_workspace_size bytes, filled by jb_lmm_prepare.
+ * precision: 0 = every likelihood evaluation is a direct FP64 reduction (plain form);
+ * 1 = the golden-section probes take log|H^-1| and the genotype-free weighted sums from
+ * per-bracket Chebyshev expansions (degree 24, built by jb_lmm_prepare with precision 1
+ * from exact FP64 node values) and reduce only the c+2 genotype-dependent sums over n;
+ * grid points, the final evaluation and all statistics stay direct FP64.  Use 1 only
+ * when 1 + l_max * min(eval) > 0.5 (no pole of log|1 + lambda eval| near the range).
  */
 int64_t jb_lmm_workspace_size(int64_t n, int32_t n_cvt, int32_t phi, int32_t n_grid);
 
@@ -150,13 +214,14 @@ int64_t jb_lmm_workspace_size(int64_t n, int32_t n_cvt, int32_t phi, int32_t n_g
  * point and the SNP-independent weighted sums.  Must precede jb_lmm_chunk calls that
  * use the same inputs; n_cvt in 1..4.
  */
-int32_t jb_lmm_prepare(int32_t lmm_mode, int64_t n, int32_t n_cvt, int32_t phi,
-                       const double* evals, const double* UtW, int64_t ldw,
+int32_t jb_lmm_prepare(int32_t lmm_mode, int32_t precision, int64_t n, int32_t n_cvt,
+                       int32_t phi, const double* evals, const double* UtW, int64_t ldw,
                        const double* Uty, int64_t ldy, const double* lam0, double l_min,
                        double l_max, int32_t n_grid, void* workspace,
                        int64_t workspace_bytes, uintptr_t stream);
 
-int32_t jb_lmm_chunk(int32_t lmm_mode, int64_t n, int32_t n_cvt, int32_t phi, int64_t m,
+int32_t jb_lmm_chunk(int32_t lmm_mode, int32_t precision, int64_t n, int32_t n_cvt,
+                     int32_t phi, int64_t m,
                      const double* evals, const double* UtW, int64_t ldw,
                      const double* Uty, int64_t ldy, const double* UtG, int64_t ldg,
                      const double* lam0, const double* logl0, double l_min, double l_max,

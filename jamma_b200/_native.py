@@ -53,13 +53,24 @@ SIGNATURES: dict[str, tuple] = {
     "jb_lmm_workspace_size": (_i64, [_i64, _i32, _i32, _i32]),
     "jb_lmm_prepare": (
         _i32,
-        [_i32, _i64, _i32, _i32, _p, _p, _i64, _p, _i64, _p, _f64, _f64, _i32, _p, _i64, _u],
+        [_i32, _i32, _i64, _i32, _i32, _p, _p, _i64, _p, _i64, _p, _f64, _f64, _i32, _p, _i64, _u],
     ),
     "jb_lmm_chunk": (
         _i32,
-        [_i32, _i64, _i32, _i32, _i64, _p, _p, _i64, _p, _i64, _p, _i64, _p, _p, _f64, _f64,
-         _i32, _i32, LmmOut, _p, _i64, _u],
+        [_i32, _i32, _i64, _i32, _i32, _i64, _p, _p, _i64, _p, _i64, _p, _i64, _p, _p, _f64,
+         _f64, _i32, _i32, LmmOut, _p, _i64, _u],
     ),
+    "jb_gram_i8_workspace_size": (_i64, [_i64]),
+    "jb_gram_i8": (_i32, [_p, _i64, _i64, _i64, _p, _i64, _p, _i64, _u]),
+    "jb_gram_status": (_i32, [_p, _p, _u]),
+    "jb_codes_to_sample_major": (_i32, [_p, _i64, _i64, _i64, _p, _i64, _i64, _p, _i64, _u]),
+    "jb_kinship_i8_corrections": (_i32, [_p, _i64, _p, _i64, _i64, _i64, _p, _p, _p, _p, _i64, _u]),
+    "jb_kinship_i8_finalize": (_i32, [_p, _i64, _i64, _p, _p, _f64, _p, _i64, _i64, _p, _i64, _u]),
+    "jb_ozaki_workspace_size": (_i64, [_i64]),
+    "jb_ozaki_prepare": (_i32, [_p, _i64, _i64, _p, _i64, _u]),
+    "jb_rotate_i8_workspace_size": (_i64, [_i64, _i64]),
+    "jb_rotate_i8": (_i32, [_p, _i64, _p, _i64, _i64, _p, _i32, _p, _i64, _p, _i64, _u]),
+    "jb_rotate_status": (_i32, [_p, _p, _u]),
     "jb_null_mle": (
         _i32,
         [_i64, _i32, _i32, _p, _p, _i64, _p, _i64, _f64, _f64, _i32, _i32, _p, _p, _u],

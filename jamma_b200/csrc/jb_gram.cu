@@ -1,0 +1,353 @@
+// INT8 tensor-core kinship Gram (mixed-precision form of GEMMA -gk 1) and its FP64
+// centring / missing-genotype corrections.
+//
+// Genotype calls 0/1/2 are exact in int8 and Z Z^T accumulates exactly in int32, so the
+// Gram is bit-exact whatever the tiling.  With mu_j the float64 mean of SNP j over
+// observed samples and M the missing-call mask (Z = 0 where missing), the centred,
+// mean-imputed matrix of jamma's impute_and_center (src/jamma/kinship/missing.py:22-61)
+// is Xc = Z - 1 mu^T + M diag(mu), hence
+//
+//   p K = Z Z^T - a 1^T - 1 a^T + (sum mu^2) 1 1^T - b 1^T - 1 b^T + R + R^T + T
+//   a = Z mu,  b = M mu^2,  R = Z diag(mu) M^T,  T = M diag(mu^2) M^T
+//
+// The dense Z Z^T runs on tcgen05 (kind::i8); the vectors and the sparse R, T terms are
+// FP64 on the CUDA cores.
+#include "jb_common.cuh"
+#include "jb_gemm_i8.cuh"
+
+#include <mutex>
+#include <vector>
+
+namespace jb {
+namespace tc {
+
+// ---------------------------------------------------------------- tensor maps
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    });
+    return fn;
+}
+
+// K-major int8 matrix `rows x k` with row stride ld bytes; box = 128 (K) x box_rows.
+int32_t make_map_i8(CUtensorMap* map, const void* base, int64_t rows, int64_t k, int64_t ld,
+                    int box_rows) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) {
+        set_error("cuTensorMapEncodeTiled is unavailable from the driver");
+        return JB_E_CUDA;
+    }
+    if ((reinterpret_cast<uintptr_t>(base) & 15) || (ld & 15)) {
+        set_error("TMA operand needs a 16-byte aligned base and row stride (ld=%lld)",
+                  (long long)ld);
+        return JB_E_INVALID;
+    }
+    cuuint64_t dims[2] = {(cuuint64_t)k, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)ld};
+    cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides,
+                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        set_error("cuTensorMapEncodeTiled failed (%d)", (int)r);
+        return JB_E_CUDA;
+    }
+    return JB_OK;
+}
+
+int num_sms() {
+    int dev = 0, n = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n;
+}
+
+// ---------------------------------------------------------------- Gram epilogue
+struct GramEpi {
+    static constexpr int kSmem = 0;
+    int32_t* C;
+    int64_t ldc;
+    int n;
+    __device__ __forceinline__ void run(int mb, int nb, uint32_t taddr, int q, int lane,
+                                        uint8_t*) const {
+        const int i = mb * kBM + 32 * q + lane;
+#pragma unroll 1
+        for (int c0 = 0; c0 < 256; c0 += 32) {
+            uint32_t v[32];
+            tmem_ld32(taddr + (uint32_t)c0, v);
+            const int j0 = nb * 256 + c0;
+            if (i < n) {
+#pragma unroll
+                for (int t = 0; t < 32; ++t) {
+                    if (j0 + t < n) C[(int64_t)(j0 + t) * ldc + i] = (int32_t)v[t];
+                }
+            }
+        }
+    }
+};
+
+// Upper-triangle tiles (128-row x 256-column blocks touching col >= row), visited in
+// groups of GM x GN tiles so that concurrently running CTAs share A and B row blocks.
+__host__ __device__ inline int gram_tiles(int MB, int NB, Tile* out) {
+    const int GM = 16, GN = 8;
+    int k = 0;
+    for (int gm = 0; gm < MB; gm += GM)
+        for (int gn = 0; gn < NB; gn += GN)
+            for (int nb = gn; nb < NB && nb < gn + GN; ++nb)
+                for (int mb = gm; mb < MB && mb < gm + GM; ++mb)
+                    if (kBM * mb <= 256 * nb + 255) {
+                        if (out) out[k] = Tile{mb, nb};
+                        ++k;
+                    }
+    return k;
+}
+
+__global__ void gram_tiles_kernel(int MB, int NB, Tile* out) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) gram_tiles(MB, NB, out);
+}
+
+// ---------------------------------------------------------------- layout kernels
+// SNP-major codes (m x ldc, 3 = missing) -> sample-major int8 calls Zs[i, col0 + j]
+// (missing -> 0), through 32x32 shared-memory tiles.
+// Optionally also the raw codes Cs[i, j] (3 kept) of this chunk, sample-major.
+__global__ void codes_to_sample_major_kernel(const int8_t* __restrict__ codes, int64_t ldc,
+                                             int64_t n, int64_t m, int8_t* __restrict__ Zs,
+                                             int64_t ldz, int64_t col0, int8_t* __restrict__ Cs,
+                                             int64_t ldcs) {
+    __shared__ int8_t t[32][33];
+    const int64_t j0 = (int64_t)blockIdx.x * 32, i0 = (int64_t)blockIdx.y * 32;
+    const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
+    for (int r = ty; r < 32; r += 8) {
+        const int64_t j = j0 + r, i = i0 + tx;
+        t[r][tx] = (j < m && i < n) ? codes[j * ldc + i] : (int8_t)0;
+    }
+    __syncthreads();
+    for (int r = ty; r < 32; r += 8) {
+        const int64_t i = i0 + r, j = j0 + tx;
+        if (i < n && j < m) {
+            const int8_t v = t[tx][r];
+            if (Zs) Zs[i * ldz + col0 + j] = (v == 3) ? (int8_t)0 : v;
+            if (Cs) Cs[i * ldcs + j] = v;
+        }
+    }
+}
+
+// a_i = sum_j Z_ij mu_j and b_i = sum_{j missing at i} mu_j^2 from SNP-major codes.
+__global__ void kin_vectors_kernel(const int8_t* __restrict__ codes, int64_t ldc, int64_t n,
+                                   int64_t m, const double* __restrict__ mu,
+                                   double* __restrict__ a, double* __restrict__ b) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double sa = 0.0, sb = 0.0;
+    for (int64_t j = 0; j < m; ++j) {
+        const int8_t c = codes[j * ldc + i];
+        const double u = __ldg(mu + j);
+        if (c == 3)
+            sb = fma(u, u, sb);
+        else
+            sa = fma((double)c, u, sa);
+    }
+    a[i] += sa;
+    b[i] += sb;
+}
+
+// Sparse terms for one SNP chunk.  For every sample k and every SNP j of the chunk that
+// is missing at k: R[:, k] += mu_j Z[:, j] and T[:, k] += mu_j^2 M[:, j].  One CTA per
+// (k, block of 2048 samples i); each thread keeps 8 rows of both sums in registers.
+__global__ void __launch_bounds__(256) kin_sparse_kernel(const int8_t* __restrict__ codes,
+                                                          int64_t ldc, const int8_t* __restrict__ Cs,
+                                                          int64_t ldcs, int64_t n, int64_t m,
+                                                          const double* __restrict__ mu,
+                                                          double* __restrict__ RT,
+                                                          int64_t ldr) {
+    const int64_t k = blockIdx.x;
+    const int64_t i0 = (int64_t)blockIdx.y * 2048;
+    __shared__ int32_t list[1024];
+    __shared__ int cnt;
+    double r[8], tt[8];
+#pragma unroll
+    for (int e = 0; e < 8; ++e) r[e] = tt[e] = 0.0;
+    for (int64_t jb = 0; jb < m; jb += 1024) {
+        if (threadIdx.x == 0) cnt = 0;
+        __syncthreads();
+        for (int64_t j = jb + threadIdx.x; j < m && j < jb + 1024; j += blockDim.x) {
+            if (Cs[k * ldcs + j] == 3) list[atomicAdd(&cnt, 1)] = (int32_t)j;
+        }
+        __syncthreads();
+        const int c = cnt;
+        for (int e = 0; e < c; ++e) {
+            const int64_t j = list[e];
+            const double u = mu[j];
+            const int8_t* row = codes + j * ldc;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                const int64_t i = i0 + threadIdx.x + 256 * q;
+                if (i < n) {
+                    const int8_t v = row[i];
+                    if (v == 3)
+                        tt[q] = fma(u, u, tt[q]);
+                    else
+                        r[q] = fma((double)v, u, r[q]);
+                }
+            }
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const int64_t i = i0 + threadIdx.x + 256 * q;
+        if (i < n) {
+            RT[k * ldr + i] += r[q];            // R[i, k] (column-major, column k)
+            RT[(n + k) * ldr + i] += tt[q];     // T[i, k]
+        }
+    }
+}
+
+// K = (C - a_i - a_j + s - b_i - b_j + R_ij + R_ji + T_ij) / p, symmetric, column-major.
+__global__ void kin_finalize_i8_kernel(const int32_t* __restrict__ C, int64_t ldc, int64_t n,
+                                       const double* __restrict__ a, const double* __restrict__ b,
+                                       double s, const double* __restrict__ RT, int64_t ldr,
+                                       double inv_p, double* __restrict__ K, int64_t ldk) {
+    const int64_t j = blockIdx.y;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= j && i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        // the int32 Gram holds the upper triangle (row i <= column j) at C[j*ldc + i]
+        double v = (double)C[j * ldc + i] - a[i] - a[j] + s - b[i] - b[j];
+        if (RT) v += RT[j * ldr + i] + RT[i * ldr + j] + RT[(n + j) * ldr + i];
+        v *= inv_p;
+        K[j * ldk + i] = v;
+        K[i * ldk + j] = v;
+    }
+}
+
+}  // namespace tc
+}  // namespace jb
+
+using namespace jb;
+using namespace jb::tc;
+
+namespace {
+constexpr int kGramBN = 256;
+constexpr int kGramStages = 4;
+using GramSmem = GemmSmem<kGramBN, kGramStages, 0>;
+
+struct GramWs {
+    int64_t status, tiles, total;
+};
+GramWs gram_ws(int64_t n) {
+    const int64_t MB = ceil_div(n, kBM), NB = ceil_div(n, kGramBN);
+    GramWs w;
+    w.status = 0;
+    w.tiles = 256;
+    w.total = w.tiles + ((MB * NB * (int64_t)sizeof(Tile) + 255) / 256) * 256;
+    return w;
+}
+}  // namespace
+
+extern "C" {
+
+int64_t jb_gram_i8_workspace_size(int64_t n) {
+    if (n <= 0) return -1;
+    return gram_ws(n).total;
+}
+
+int32_t jb_gram_i8(const int8_t* Z, int64_t n, int64_t p, int64_t ldz, int32_t* C, int64_t ldc,
+                   void* workspace, int64_t workspace_bytes, uintptr_t stream) {
+    JB_CHECK_ARG(n > 0 && p > 0 && ldz >= p && ldc >= n, "jb_gram_i8: bad shape");
+    JB_CHECK_ARG(n < (1ll << 31) && p < (1ll << 31), "jb_gram_i8: size too large");
+    JB_CHECK_ARG(4ll * p < (1ll << 31), "jb_gram_i8: p too large for exact int32 accumulation");
+    const GramWs L = gram_ws(n);
+    JB_CHECK_ARG(workspace && workspace_bytes >= L.total, "jb_gram_i8: workspace too small");
+    cudaStream_t st = as_stream(stream);
+    uint8_t* ws = static_cast<uint8_t*>(workspace);
+    int* status = reinterpret_cast<int*>(ws + L.status);
+    Tile* tiles = reinterpret_cast<Tile*>(ws + L.tiles);
+    const int MB = (int)ceil_div(n, kBM), NB = (int)ceil_div(n, kGramBN);
+    const int n_tiles = gram_tiles(MB, NB, nullptr);
+    CUtensorMap ta, tb;
+    int32_t rc = make_map_i8(&ta, Z, n, p, ldz, kBM);
+    if (rc) return rc;
+    rc = make_map_i8(&tb, Z, n, p, ldz, kGramBN);
+    if (rc) return rc;
+    JB_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
+    gram_tiles_kernel<<<1, 32, 0, st>>>(MB, NB, tiles);
+    JB_LAUNCH_CHECK("gram_tiles_kernel");
+    auto kern = i8_gemm_kernel<kGramBN, kGramStages, GramEpi>;
+    JB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 GramSmem::TOTAL));
+    GramEpi epi{C, ldc, (int)n};
+    const int grid = n_tiles < num_sms() ? n_tiles : num_sms();
+    const int num_kb = (int)ceil_div(p, kBK);
+    kern<<<grid, kThreads, GramSmem::TOTAL, st>>>(ta, tb, tiles, n_tiles, num_kb, epi, status);
+    JB_LAUNCH_CHECK("i8_gemm_kernel<gram>");
+    return JB_OK;
+}
+
+int32_t jb_gram_status(const void* workspace, int32_t* out, uintptr_t stream) {
+    JB_CHECK_ARG(workspace && out, "jb_gram_status: null pointer");
+    JB_CUDA(cudaMemcpyAsync(out, workspace, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                            as_stream(stream)));
+    JB_CUDA(cudaStreamSynchronize(as_stream(stream)));
+    return JB_OK;
+}
+
+int32_t jb_codes_to_sample_major(const int8_t* codes, int64_t ld_codes, int64_t n, int64_t m,
+                                 int8_t* Zs, int64_t ldz, int64_t col0, int8_t* Cs, int64_t ldcs,
+                                 uintptr_t stream) {
+    JB_CHECK_ARG(n >= 0 && m >= 0 && ld_codes >= n && col0 >= 0,
+                 "jb_codes_to_sample_major: bad shape");
+    JB_CHECK_ARG(!Zs || ldz >= col0 + m, "jb_codes_to_sample_major: ldz too small");
+    JB_CHECK_ARG(!Cs || ldcs >= m, "jb_codes_to_sample_major: ldcs too small");
+    if (n == 0 || m == 0) return JB_OK;
+    JB_CHECK_ARG(ceil_div(n, 32) < 65536, "jb_codes_to_sample_major: n too large");
+    dim3 grid((unsigned)ceil_div(m, 32), (unsigned)ceil_div(n, 32), 1);
+    codes_to_sample_major_kernel<<<grid, dim3(32, 8), 0, as_stream(stream)>>>(codes, ld_codes, n,
+                                                                              m, Zs, ldz, col0, Cs, ldcs);
+    JB_LAUNCH_CHECK("codes_to_sample_major_kernel");
+    return JB_OK;
+}
+
+int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes, const int8_t* Cs,
+                                  int64_t ldcs, int64_t n, int64_t m, const double* mu, double* a,
+                                  double* b, double* RT, int64_t ldr, uintptr_t stream) {
+    JB_CHECK_ARG(n > 0 && m >= 0 && ld_codes >= n, "jb_kinship_i8_corrections: bad shape");
+    if (m == 0) return JB_OK;
+    cudaStream_t st = as_stream(stream);
+    kin_vectors_kernel<<<(unsigned)ceil_div(n, 128), 128, 0, st>>>(codes, ld_codes, n, m, mu, a, b);
+    JB_LAUNCH_CHECK("kin_vectors_kernel");
+    if (Cs) {
+        JB_CHECK_ARG(RT && ldr >= n && ldcs >= m, "jb_kinship_i8_corrections: RT buffer needed");
+        JB_CHECK_ARG(ceil_div(n, 2048) < 65536, "jb_kinship_i8_corrections: n too large");
+        dim3 grid((unsigned)n, (unsigned)ceil_div(n, 2048), 1);
+        kin_sparse_kernel<<<grid, 256, 0, st>>>(codes, ld_codes, Cs, ldcs, n, m, mu, RT, ldr);
+        JB_LAUNCH_CHECK("kin_sparse_kernel");
+    }
+    return JB_OK;
+}
+
+int32_t jb_kinship_i8_finalize(const int32_t* C, int64_t ldc, int64_t n, const double* a,
+                               const double* b, double sum_mu2, const double* RT, int64_t ldr,
+                               int64_t p_kept, double* K, int64_t ldk, uintptr_t stream) {
+    JB_CHECK_ARG(n > 0 && ldc >= n && ldk >= n && p_kept > 0, "jb_kinship_i8_finalize: bad shape");
+    JB_CHECK_ARG(n < 65536 * 4, "jb_kinship_i8_finalize: n too large");
+    dim3 grid((unsigned)(ceil_div(n, 256) < 64 ? ceil_div(n, 256) : 64), (unsigned)n, 1);
+    kin_finalize_i8_kernel<<<grid, 256, 0, as_stream(stream)>>>(C, ldc, n, a, b, sum_mu2, RT, ldr,
+                                                               1.0 / (double)p_kept, K, ldk);
+    JB_LAUNCH_CHECK("kin_finalize_i8_kernel");
+    return JB_OK;
+}
+
+}  // extern "C"

@@ -61,7 +61,13 @@ struct Params {
     const double* S;       // (n_grid + 1 + phi) x phi x NS shared sums
     double c_reml, c_mle, df, n_d;
     jb_lmm_out out;
+    // mixed form: Chebyshev expansions of the SNP-independent terms per grid bracket
+    const double* cheb;    // [n_grid][1 + phi*NS][kChebN] coefficients (NULL: direct)
+    const double* cheb_mid;
+    const double* cheb_half;
 };
+
+constexpr int kChebN = 25;  // interpolation nodes (degree 24) per bracket
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -241,7 +247,7 @@ __device__ __forceinline__ void eval_full(const Params& p, const double* __restr
     const int lane = threadIdx.x & 31;
     for (int64_t i = lane; i < p.n; i += 32) {
         const double v = __dadd_rn(__dmul_rn(lam, __ldg(p.evals + i)), 1.0);
-        const double hi = 1.0 / v;
+        const double hi = __drcp_rn(v);  // correctly rounded, = 1.0 / v
         ld += log(fabs(v));
         double vec[L::R];
 #pragma unroll
@@ -272,25 +278,81 @@ __device__ __forceinline__ double eval_logl(const Params& p, const double* x, co
     return REML ? reml_logl<C>(pb, iab_diag, logdet, p) : mle_logl<C>(pb, logdet, p);
 }
 
-// Grid bracket + golden section (_golden_section_refine, likelihood_jax.py:419-488).
+// Chebyshev series sum_j c_j T_j(t) by Clenshaw's recurrence.
+__device__ __forceinline__ double cheb_eval(const double* __restrict__ c, double t) {
+    double b1 = 0.0, b2 = 0.0;
+    const double t2 = 2.0 * t;
+#pragma unroll 5
+    for (int j = kChebN - 1; j >= 1; --j) {
+        const double b0 = fma(t2, b1, c[j] - b2);
+        b2 = b1;
+        b1 = b0;
+    }
+    return fma(t, b1, c[0] - b2);
+}
+
+// Mixed-form evaluation inside the golden bracket of grid index `best`: the length-n
+// reduction is restricted to the c+2 genotype-dependent sums; log|H^-1| and the x-free
+// sums (smooth in log lambda, analytic in a strip of half-width pi) come from degree-24
+// Chebyshev expansions over the bracket, built from exact FP64 values at the nodes.
 template <int C, bool REML>
-__device__ void golden(const Params& p, const double* x, const double* y, int best,
+__device__ __forceinline__ double eval_logl_interp(const Params& p, const double* __restrict__ x,
+                                                   const double* __restrict__ y, double log_lam,
+                                                   int best, int f,
+                                                   const double (&iab_diag)[C + 1]) {
+    using L = Lay<C>;
+    const double lam = exp(log_lam);
+    double acc[L::NX];
+#pragma unroll
+    for (int k = 0; k < L::NX; ++k) acc[k] = 0.0;
+    const int lane = threadIdx.x & 31;
+    for (int64_t i = lane; i < p.n; i += 32) {
+        const double v = __dadd_rn(__dmul_rn(lam, __ldg(p.evals + i)), 1.0);
+        const double xv = x[i];
+        const double t = __drcp_rn(v) * xv;
+#pragma unroll
+        for (int a = 0; a < C; ++a) acc[a] = fma(t, __ldg(p.W + a * p.ldw + i), acc[a]);
+        acc[C] = fma(t, xv, acc[C]);
+        acc[C + 1] = fma(t, __ldg(y + i), acc[C + 1]);
+    }
+#pragma unroll
+    for (int k = 0; k < L::NX; ++k) acc[k] = warp_sum(acc[k]);
+    const int nf = 1 + p.phi * L::NS;
+    const double* cb = p.cheb + (int64_t)best * nf * kChebN;
+    const double tt = (log_lam - p.cheb_mid[best]) / p.cheb_half[best];
+    const double logdet = cheb_eval(cb, tt);
+    double shared[L::NS];
+#pragma unroll
+    for (int k = 0; k < L::NS; ++k) shared[k] = cheb_eval(cb + (1 + f * L::NS + k) * kChebN, tt);
+    double row0[L::NI];
+    assemble<C>(row0, shared, acc);
+    const PabOut<C> pb = pab_reduce<C>(row0);
+    return REML ? reml_logl<C>(pb, iab_diag, logdet, p) : mle_logl<C>(pb, logdet, p);
+}
+
+// Grid bracket + golden section (_golden_section_refine, likelihood_jax.py:419-488).
+template <int C, bool REML, bool INTERP>
+__device__ void golden(const Params& p, const double* x, const double* y, int best, int f,
                        const double (&iab_diag)[C + 1], double& lam_out, double& logl_out,
                        PabOut<C>& pb_out) {
     const int lo = best - 1 > 0 ? best - 1 : 0;
     const int hi = best + 1 < p.n_grid - 1 ? best + 1 : p.n_grid - 1;
+    auto probe = [&](double s) {
+        return INTERP ? eval_logl_interp<C, REML>(p, x, y, s, best, f, iab_diag)
+                      : eval_logl<C, REML>(p, x, y, s, iab_diag, nullptr);
+    };
     double a = p.loglam[lo], b = p.loglam[hi];
     double c = __dsub_rn(b, __dmul_rn(kPhi, __dsub_rn(b, a)));
     double d = __dadd_rn(a, __dmul_rn(kPhi, __dsub_rn(b, a)));
-    double fc = eval_logl<C, REML>(p, x, y, c, iab_diag, nullptr);
-    double fd = eval_logl<C, REML>(p, x, y, d, iab_diag, nullptr);
+    double fc = probe(c);
+    double fd = probe(d);
     for (int it = 0; it < p.n_iter; ++it) {
         const bool keep_left = fc > fd;
         const double na = keep_left ? a : c;
         const double nb = keep_left ? d : b;
         const double nc = __dsub_rn(nb, __dmul_rn(kPhi, __dsub_rn(nb, na)));
         const double nd = __dadd_rn(na, __dmul_rn(kPhi, __dsub_rn(nb, na)));
-        const double nl = eval_logl<C, REML>(p, x, y, keep_left ? nc : nd, iab_diag, nullptr);
+        const double nl = probe(keep_left ? nc : nd);
         const double nfc = keep_left ? nl : fd;
         const double nfd = keep_left ? fc : nl;
         a = na; b = nb; c = nc; d = nd; fc = nfc; fd = nfd;
@@ -323,7 +385,7 @@ __device__ __forceinline__ void beta_se(const PabOut<C>& pb, double px_yy, doubl
     se = valid ? sqrt(var) : jnan();
 }
 
-template <int C, int GB>
+template <int C, int GB, bool INTERP>
 __global__ void __launch_bounds__(256) lmm_pairs_kernel(const Params p) {
     using L = Lay<C>;
     const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -440,7 +502,7 @@ __global__ void __launch_bounds__(256) lmm_pairs_kernel(const Params p) {
     if (need_mle) {
         double lam, logl;
         PabOut<C> pb;
-        golden<C, false>(p, x, y, best_mle.idx, iab_diag, lam, logl, pb);
+        golden<C, false, INTERP>(p, x, y, best_mle.idx, f, iab_diag, lam, logl, pb);
         if (lane == 0) {
             if (p.out.lambda_mle) p.out.lambda_mle[o] = lam;
             if (p.out.logl_mle) p.out.logl_mle[o] = logl;
@@ -451,7 +513,7 @@ __global__ void __launch_bounds__(256) lmm_pairs_kernel(const Params p) {
     if (need_reml) {
         double lam, logl;
         PabOut<C> pb;
-        golden<C, true>(p, x, y, best_reml.idx, iab_diag, lam, logl, pb);
+        golden<C, true, INTERP>(p, x, y, best_reml.idx, f, iab_diag, lam, logl, pb);
         bool valid;
         double beta, tau, se;
         const double px_yy = clamp_pyy(pb.yy1);
@@ -539,6 +601,87 @@ __global__ void lmm_shared_kernel(int64_t n, int n_grid, int phi, const double* 
         for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += red[threadIdx.x][k];
         S[((int64_t)r * phi + f) * L::NS + threadIdx.x] = t;
     }
+}
+
+// Chebyshev node values for the mixed form: block (bracket b, node k) x phenotype f
+// evaluates log|H^-1| (f == 0) and the x-free weighted sums of phenotype f exactly in
+// FP64 at lambda = exp(s_k), s_k the k-th Chebyshev node of bracket b.
+template <int C>
+__global__ void lmm_cheb_nodes_kernel(int64_t n, int n_grid, int phi,
+                                      const double* __restrict__ evals, const double* __restrict__ W,
+                                      int64_t ldw, const double* __restrict__ Y, int64_t ldy,
+                                      const double* __restrict__ loglam, double* __restrict__ vals,
+                                      double* __restrict__ mid, double* __restrict__ half) {
+    using L = Lay<C>;
+    const int b = blockIdx.x / kChebN, k = blockIdx.x % kChebN, f = blockIdx.y;
+    const int lo = b - 1 > 0 ? b - 1 : 0, hi = b + 1 < n_grid - 1 ? b + 1 : n_grid - 1;
+    const double A = loglam[lo], B = loglam[hi];
+    const double m = 0.5 * (A + B), h = 0.5 * (B - A);
+    const double s = m + h * cos(M_PI * (k + 0.5) / kChebN);
+    const double lam = exp(s);
+    double acc[L::NS];
+#pragma unroll
+    for (int q = 0; q < L::NS; ++q) acc[q] = 0.0;
+    double ld = 0.0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+        const double v = __dadd_rn(__dmul_rn(lam, evals[i]), 1.0);
+        const double hv = __drcp_rn(v);
+        if (f == 0) ld += log(fabs(v));
+        double vec[L::R];
+#pragma unroll
+        for (int a = 0; a < C; ++a) vec[a] = W[a * ldw + i];
+        vec[C] = 0.0;
+        vec[C + 1] = Y[(int64_t)f * ldy + i];
+        int q = 0;
+#pragma unroll
+        for (int a = 0; a < L::R; ++a) {
+#pragma unroll
+            for (int bb = a; bb < L::R; ++bb) {
+                if (a == C || bb == C) continue;
+                acc[q] = fma(hv * vec[a], vec[bb], acc[q]);
+                ++q;
+            }
+        }
+    }
+    __shared__ double red[L::NS + 1][8];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < L::NS; ++q) {
+        const double v = warp_sum(acc[q]);
+        if (lane == 0) red[q][w] = v;
+    }
+    {
+        const double v = warp_sum(ld);
+        if (lane == 0) red[L::NS][w] = v;
+    }
+    __syncthreads();
+    const int nf = 1 + phi * L::NS;
+    double* out = vals + ((int64_t)b * kChebN + k) * nf;
+    if (threadIdx.x <= L::NS) {
+        double t = 0.0;
+        for (int q = 0; q < (int)(blockDim.x >> 5); ++q) t += red[threadIdx.x][q];
+        if (threadIdx.x < L::NS)
+            out[1 + f * L::NS + threadIdx.x] = t;
+        else if (f == 0)
+            out[0] = t;
+    }
+    if (threadIdx.x == 0 && k == 0 && f == 0) {
+        mid[b] = m;
+        half[b] = h;
+    }
+}
+
+// Chebyshev coefficients c_j = (2/N) sum_k f(s_k) cos(pi j (k + 1/2) / N), c_0 halved.
+__global__ void lmm_cheb_coef_kernel(int nf, const double* __restrict__ vals,
+                                     double* __restrict__ coef) {
+    const int b = blockIdx.x, fi = blockIdx.y, j = threadIdx.x;
+    if (j >= kChebN) return;
+    double c = 0.0;
+    for (int k = 0; k < kChebN; ++k)
+        c += vals[((int64_t)b * kChebN + k) * nf + fi] * cos(M_PI * j * (k + 0.5) / kChebN);
+    c *= 2.0 / kChebN;
+    if (j == 0) c *= 0.5;
+    coef[((int64_t)b * nf + fi) * kChebN + j] = c;
 }
 
 // ---------------------------------------------------------------- null model
@@ -654,7 +797,7 @@ __global__ void null_mle_kernel(int64_t n, const double* W, int64_t ldw, const d
 
 // ---------------------------------------------------------------- host helpers
 struct WsLayout {
-    int64_t loglam, logdet, H, S, total;
+    int64_t loglam, logdet, H, S, cheb, cmid, chalf, cvals, total;
 };
 
 inline int64_t align256(int64_t b) { return (b + 255) / 256 * 256; }
@@ -672,6 +815,15 @@ inline WsLayout ws_layout(int64_t n, int c, int phi, int n_grid) {
     off += align256(8 * (int64_t)(n_grid + phi) * n);
     w.S = off;
     off += align256(8 * (int64_t)(n_grid + 1 + phi) * phi * ns_of(c));
+    const int64_t nf = 1 + (int64_t)phi * ns_of(c);
+    w.cheb = off;
+    off += align256(8 * (int64_t)n_grid * nf * kChebN);
+    w.cmid = off;
+    off += align256(8 * (int64_t)n_grid);
+    w.chalf = off;
+    off += align256(8 * (int64_t)n_grid);
+    w.cvals = off;
+    off += align256(8 * (int64_t)n_grid * nf * kChebN);
     w.total = off;
     return w;
 }
@@ -693,7 +845,10 @@ int32_t launch_pairs(const Params& p, cudaStream_t st) {
     constexpr int GB = (C <= 1) ? 8 : (C == 2 ? 6 : 5);
     const int64_t warps = p.m * p.phi;
     const int64_t blocks = ceil_div(warps * 32, 256);
-    lmm_pairs_kernel<C, GB><<<(unsigned)blocks, 256, 0, st>>>(p);
+    if (p.cheb)
+        lmm_pairs_kernel<C, GB, true><<<(unsigned)blocks, 256, 0, st>>>(p);
+    else
+        lmm_pairs_kernel<C, GB, false><<<(unsigned)blocks, 256, 0, st>>>(p);
     JB_LAUNCH_CHECK("lmm_pairs_kernel");
     return JB_OK;
 }
@@ -701,7 +856,7 @@ int32_t launch_pairs(const Params& p, cudaStream_t st) {
 template <int C>
 int32_t launch_prepare(int64_t n, int phi, int n_grid, const double* evals, const double* W,
                        int64_t ldw, const double* Y, int64_t ldy, const double* lam0,
-                       double l_min, double l_max, uint8_t* ws, cudaStream_t st) {
+                       double l_min, double l_max, uint8_t* ws, cudaStream_t st, bool interp) {
     const WsLayout L = ws_layout(n, C, phi, n_grid);
     double* loglam = reinterpret_cast<double*>(ws + L.loglam);
     double* logdet = reinterpret_cast<double*>(ws + L.logdet);
@@ -716,6 +871,17 @@ int32_t launch_prepare(int64_t n, int phi, int n_grid, const double* evals, cons
     const int rows_s = n_grid + 1 + (lam0 ? phi : 0);
     lmm_shared_kernel<C><<<dim3(rows_s, phi), 256, 0, st>>>(n, n_grid, phi, W, ldw, Y, ldy, H, S);
     JB_LAUNCH_CHECK("lmm_shared_kernel");
+    if (interp) {
+        const int nf = 1 + phi * Lay<C>::NS;
+        double* vals = reinterpret_cast<double*>(ws + L.cvals);
+        double* coef = reinterpret_cast<double*>(ws + L.cheb);
+        lmm_cheb_nodes_kernel<C><<<dim3(n_grid * kChebN, phi), 256, 0, st>>>(
+            n, n_grid, phi, evals, W, ldw, Y, ldy, loglam, vals,
+            reinterpret_cast<double*>(ws + L.cmid), reinterpret_cast<double*>(ws + L.chalf));
+        JB_LAUNCH_CHECK("lmm_cheb_nodes_kernel");
+        lmm_cheb_coef_kernel<<<dim3(n_grid, nf), 32, 0, st>>>(nf, vals, coef);
+        JB_LAUNCH_CHECK("lmm_cheb_coef_kernel");
+    }
     return JB_OK;
 }
 
@@ -732,11 +898,12 @@ int64_t jb_lmm_workspace_size(int64_t n, int32_t n_cvt, int32_t phi, int32_t n_g
     return ws_layout(n, n_cvt, phi, n_grid).total;
 }
 
-int32_t jb_lmm_prepare(int32_t lmm_mode, int64_t n, int32_t n_cvt, int32_t phi,
-                       const double* evals, const double* UtW, int64_t ldw, const double* Uty,
-                       int64_t ldy, const double* lam0, double l_min, double l_max,
-                       int32_t n_grid, void* workspace, int64_t workspace_bytes,
+int32_t jb_lmm_prepare(int32_t lmm_mode, int32_t precision, int64_t n, int32_t n_cvt,
+                       int32_t phi, const double* evals, const double* UtW, int64_t ldw,
+                       const double* Uty, int64_t ldy, const double* lam0, double l_min,
+                       double l_max, int32_t n_grid, void* workspace, int64_t workspace_bytes,
                        uintptr_t stream) {
+    JB_CHECK_ARG(precision == 0 || precision == 1, "jb_lmm_prepare: precision must be 0 or 1");
     JB_CHECK_ARG(lmm_mode >= 1 && lmm_mode <= 4, "jb_lmm_prepare: lmm_mode must be 1..4");
     JB_CHECK_ARG(n > 0 && phi >= 1 && n_grid >= 2, "jb_lmm_prepare: bad sizes");
     JB_CHECK_ARG(n_cvt >= 1 && n_cvt <= kMaxCvt, "jb_lmm_prepare: n_cvt must be in 1..%d", kMaxCvt);
@@ -751,15 +918,16 @@ int32_t jb_lmm_prepare(int32_t lmm_mode, int64_t n, int32_t n_cvt, int32_t phi,
     uint8_t* ws = static_cast<uint8_t*>(workspace);
     const double* l0 = lmm_mode == 1 ? nullptr : lam0;
     switch (n_cvt) {
-        case 1: return launch_prepare<1>(n, phi, n_grid, evals, UtW, ldw, Uty, ldy, l0, l_min, l_max, ws, st);
-        case 2: return launch_prepare<2>(n, phi, n_grid, evals, UtW, ldw, Uty, ldy, l0, l_min, l_max, ws, st);
-        case 3: return launch_prepare<3>(n, phi, n_grid, evals, UtW, ldw, Uty, ldy, l0, l_min, l_max, ws, st);
-        case 4: return launch_prepare<4>(n, phi, n_grid, evals, UtW, ldw, Uty, ldy, l0, l_min, l_max, ws, st);
+        case 1: return launch_prepare<1>(n, phi, n_grid, evals, UtW, ldw, Uty, ldy, l0, l_min, l_max, ws, st, precision == 1);
+        case 2: return launch_prepare<2>(n, phi, n_grid, evals, UtW, ldw, Uty, ldy, l0, l_min, l_max, ws, st, precision == 1);
+        case 3: return launch_prepare<3>(n, phi, n_grid, evals, UtW, ldw, Uty, ldy, l0, l_min, l_max, ws, st, precision == 1);
+        case 4: return launch_prepare<4>(n, phi, n_grid, evals, UtW, ldw, Uty, ldy, l0, l_min, l_max, ws, st, precision == 1);
     }
     return JB_E_UNSUPPORTED;
 }
 
-int32_t jb_lmm_chunk(int32_t lmm_mode, int64_t n, int32_t n_cvt, int32_t phi, int64_t m,
+int32_t jb_lmm_chunk(int32_t lmm_mode, int32_t precision, int64_t n, int32_t n_cvt, int32_t phi,
+                     int64_t m,
                      const double* evals, const double* UtW, int64_t ldw, const double* Uty,
                      int64_t ldy, const double* UtG, int64_t ldg, const double* lam0,
                      const double* logl0, double l_min, double l_max, int32_t n_grid,
@@ -804,6 +972,10 @@ int32_t jb_lmm_chunk(int32_t lmm_mode, int64_t n, int32_t n_cvt, int32_t phi, in
     p.c_reml = 0.5 * df * (std::log(df) - std::log(2 * M_PI) - 1.0);
     p.c_mle = 0.5 * (double)n * (std::log((double)n) - std::log(2 * M_PI) - 1.0);
     p.out = out;
+    JB_CHECK_ARG(precision == 0 || precision == 1, "jb_lmm_chunk: precision must be 0 or 1");
+    p.cheb = precision == 1 ? reinterpret_cast<const double*>(ws + L.cheb) : nullptr;
+    p.cheb_mid = reinterpret_cast<const double*>(ws + L.cmid);
+    p.cheb_half = reinterpret_cast<const double*>(ws + L.chalf);
     cudaStream_t st = as_stream(stream);
     switch (n_cvt) {
         case 1: return launch_pairs<1>(p, st);

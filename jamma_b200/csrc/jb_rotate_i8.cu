@@ -1,0 +1,293 @@
+// Mixed-precision eigenvector rotation x~ = U^T g on INT8 tensor cores.
+//
+// Each eigenvector u_i (column i of U) is scaled by s_i = max_k |U_ki| / 127 and split
+// into four signed 8-bit digit planes, U_ki = s_i * sum_{t<4} q_t(k,i) 128^-t (+ error
+// below s_i * 2^-22); the split is exact arithmetic in FP64.  Genotype calls are exact
+// int8 values, so every digit product  C_t = q_t^T z  accumulates exactly in int32 on
+// tcgen05 (kind::i8), and the epilogue recombines  x~_i = s_i * sum_t 128^-t C_t  in FP64.
+//
+// Missing calls are mean-imputed without centring (src/jamma/lmm/runner_streaming.py:
+// 427-434): g_j = z_j + mu_j m_j with m_j the missing mask, so  x~ = U^T z + mu_j U^T m.
+// The B operand therefore pairs, per block of 128 SNPs, their 128 call rows with their
+// 128 mask rows; the epilogue forms  C^z + mu_j C^m  before recombining.  Chunks without
+// missing calls use the calls directly (256 SNPs per tile).
+//
+// A-operand layout (digits along M): tile row r of eigenvector block b holds digit
+// t = r / 32 of eigenvector 32 b + r % 32, so one 128 x 256 accumulator carries all four
+// digits of 32 eigenvectors; TMEM lane quarter q = digit q, and the four epilogue warps
+// exchange their FP64 digit contributions through shared memory.
+#include "jb_common.cuh"
+#include "jb_gemm_i8.cuh"
+
+namespace jb {
+namespace tc {
+
+int32_t make_map_i8(CUtensorMap* map, const void* base, int64_t rows, int64_t k, int64_t ld,
+                    int box_rows);
+int num_sms();
+
+constexpr int kRotBN = 256;
+constexpr int kRotStages = 4;
+constexpr int kRotEpiSmem = 4 * 32 * 32 * 8;  // [digit][column][eigvec] doubles
+
+// ---------------------------------------------------------------- digit split
+__global__ void ozaki_scale_kernel(const double* __restrict__ U, int64_t n, int64_t ldu,
+                                   double* __restrict__ scale) {
+    const int64_t i = blockIdx.x;
+    const double* col = U + i * ldu;
+    double mx = 0.0;
+    for (int64_t k = threadIdx.x; k < n; k += blockDim.x) mx = fmax(mx, fabs(col[k]));
+    __shared__ double red[32];
+    for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) m = fmax(m, red[w]);
+        scale[i] = m;  // max |U_ki|; 0 for an all-zero column
+    }
+}
+
+__global__ void ozaki_split_kernel(const double* __restrict__ U, int64_t n, int64_t ldu,
+                                   const double* __restrict__ smax, int8_t* __restrict__ A,
+                                   int64_t lda) {
+    const int64_t i = blockIdx.x;  // eigenvector
+    const double s = smax[i];
+    const double inv = s > 0.0 ? 127.0 / s : 0.0;
+    const int64_t base = (i / 32) * 128 + (i % 32);
+    for (int64_t k = threadIdx.x; k < lda; k += blockDim.x) {
+        int8_t q[4] = {0, 0, 0, 0};
+        if (k < n) {
+            double a = U[i * ldu + k] * inv;  // |a| <= 127
+#pragma unroll
+            for (int t = 0; t < 4; ++t) {
+                const double r = rint(a);
+                q[t] = (int8_t)r;
+                a = (a - r) * 128.0;  // exact; |a| <= 64
+            }
+        }
+#pragma unroll
+        for (int t = 0; t < 4; ++t) A[(base + 32 * t) * lda + k] = q[t];
+    }
+}
+
+// ---------------------------------------------------------------- B operand
+// Paired layout: block b of 128 SNPs occupies B rows [256 b, 256 b + 128) with the calls
+// (missing -> 0) and [256 b + 128, 256 b + 256) with the missing masks.
+__global__ void rot_pack_pairs_kernel(const int8_t* __restrict__ codes, int64_t ldc, int64_t n,
+                                      int64_t m, int8_t* __restrict__ B, int64_t ldb) {
+    const int64_t j = blockIdx.x;
+    const int64_t rz = (j / 128) * 256 + (j % 128);
+    const int64_t rm = rz + 128;
+    for (int64_t k = threadIdx.x; k < ldb; k += blockDim.x) {
+        int8_t z = 0, mk = 0;
+        if (j < m && k < n) {
+            const int8_t c = codes[j * ldc + k];
+            z = (c == 3) ? 0 : c;
+            mk = (c == 3);
+        }
+        B[rz * ldb + k] = z;
+        B[rm * ldb + k] = mk;
+    }
+}
+
+// ---------------------------------------------------------------- epilogue
+template <bool PAIRED>
+struct RotEpi {
+    static constexpr int kSmem = kRotEpiSmem;
+    double* X;             // x~ (n x m, column-major, ld ldx)
+    int64_t ldx;
+    const double* smax;    // per-eigenvector max |U_ki|
+    const double* mu;      // per-SNP imputation mean (PAIRED only)
+    int n;
+    int m;
+    __device__ __forceinline__ void run(int mb, int nb, uint32_t taddr, int q, int lane,
+                                        uint8_t* smem) const {
+        double* S = reinterpret_cast<double*>(smem);  // [4][32][32]
+        const int i = mb * 32 + lane;                 // eigenvector of this lane (any digit)
+        constexpr int kCols = PAIRED ? 128 : 256;
+        const int j_base = nb * kCols;
+        const double w = ldexp(1.0, -7 * q);          // 128^-q
+        double sc = 0.0;
+        if (i < n) sc = smax[i] * (1.0 / 127.0);
+#pragma unroll 1
+        for (int c0 = 0; c0 < kCols; c0 += 32) {
+            uint32_t vz[32];
+            tmem_ld32(taddr + (uint32_t)c0, vz);
+            double val[32];
+#pragma unroll
+            for (int t = 0; t < 32; ++t) val[t] = (double)(int32_t)vz[t] * w;
+            if (PAIRED) {
+                uint32_t vm[32];
+                tmem_ld32(taddr + 128u + (uint32_t)c0, vm);
+#pragma unroll
+                for (int t = 0; t < 32; ++t) {
+                    const int j = j_base + c0 + t;
+                    const double u = j < m ? __ldg(mu + j) : 0.0;
+                    val[t] = fma(u, (double)(int32_t)vm[t] * w, val[t]);
+                }
+            }
+#pragma unroll
+            for (int t = 0; t < 32; ++t) S[(q * 32 + t) * 32 + lane] = val[t];
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+#pragma unroll
+            for (int cc = 0; cc < 8; ++cc) {
+                const int t = q * 8 + cc;
+                const int j = j_base + c0 + t;
+                // smallest digit first: ((d3 + d2) + d1) + d0
+                const double x = ((S[(3 * 32 + t) * 32 + lane] + S[(2 * 32 + t) * 32 + lane]) +
+                                  S[(1 * 32 + t) * 32 + lane]) +
+                                 S[(0 * 32 + t) * 32 + lane];
+                if (i < n && j < m) X[(int64_t)j * ldx + i] = x * sc;
+            }
+            asm volatile("bar.sync 1, 128;" ::: "memory");
+        }
+    }
+};
+
+// Tiles over (eigenvector blocks of 32, SNP blocks) in groups of GM x GN.
+__global__ void rot_tiles_kernel(int MB, int NB, Tile* out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const int GM = 9, GN = 16;
+    int k = 0;
+    for (int gn = 0; gn < NB; gn += GN)
+        for (int gm = 0; gm < MB; gm += GM)
+            for (int mb = gm; mb < MB && mb < gm + GM; ++mb)
+                for (int nb = gn; nb < NB && nb < gn + GN; ++nb) out[k++] = Tile{mb, nb};
+}
+
+}  // namespace tc
+}  // namespace jb
+
+using namespace jb;
+using namespace jb::tc;
+
+namespace {
+using RotSmem = GemmSmem<kRotBN, kRotStages, kRotEpiSmem>;
+
+struct OzakiLayout {
+    int64_t lda, rows, a_off, s_off, total;
+};
+OzakiLayout ozaki_layout(int64_t n) {
+    OzakiLayout L;
+    L.lda = (n + 127) / 128 * 128;
+    L.rows = ceil_div(n, 32) * 128;
+    L.a_off = 0;
+    L.s_off = ((L.rows * L.lda + 255) / 256) * 256;
+    L.total = L.s_off + ((n * 8 + 255) / 256) * 256;
+    return L;
+}
+
+struct RotChunkLayout {
+    int64_t status, tiles, b_off, ldb, total;
+};
+RotChunkLayout rot_chunk_layout(int64_t n, int64_t m) {
+    RotChunkLayout L;
+    L.ldb = (n + 127) / 128 * 128;
+    const int64_t MB = ceil_div(n, 32), NB = ceil_div(m, 128);
+    L.status = 0;
+    L.tiles = 256;
+    L.b_off = L.tiles + ((MB * NB * (int64_t)sizeof(Tile) + 255) / 256) * 256;
+    L.total = L.b_off + NB * 256 * L.ldb;
+    return L;
+}
+}  // namespace
+
+extern "C" {
+
+int64_t jb_ozaki_workspace_size(int64_t n) {
+    if (n <= 0) return -1;
+    return ozaki_layout(n).total;
+}
+
+int32_t jb_ozaki_prepare(const double* U, int64_t n, int64_t ldu, void* ozaki_ws,
+                         int64_t ozaki_bytes, uintptr_t stream) {
+    JB_CHECK_ARG(n > 0 && ldu >= n && U, "jb_ozaki_prepare: bad arguments");
+    JB_CHECK_ARG(n < (1ll << 31), "jb_ozaki_prepare: n too large");
+    const OzakiLayout L = ozaki_layout(n);
+    JB_CHECK_ARG(ozaki_ws && ozaki_bytes >= L.total, "jb_ozaki_prepare: workspace too small");
+    uint8_t* ws = static_cast<uint8_t*>(ozaki_ws);
+    cudaStream_t st = as_stream(stream);
+    double* smax = reinterpret_cast<double*>(ws + L.s_off);
+    int8_t* A = reinterpret_cast<int8_t*>(ws + L.a_off);
+    // rows of eigenvector blocks past n stay zero
+    JB_CUDA(cudaMemsetAsync(A, 0, (size_t)(L.rows * L.lda), st));
+    ozaki_scale_kernel<<<(unsigned)n, 256, 0, st>>>(U, n, ldu, smax);
+    JB_LAUNCH_CHECK("ozaki_scale_kernel");
+    ozaki_split_kernel<<<(unsigned)n, 256, 0, st>>>(U, n, ldu, smax, A, L.lda);
+    JB_LAUNCH_CHECK("ozaki_split_kernel");
+    return JB_OK;
+}
+
+int64_t jb_rotate_i8_workspace_size(int64_t n, int64_t m) {
+    if (n <= 0 || m <= 0) return -1;
+    return rot_chunk_layout(n, m).total;
+}
+
+int32_t jb_rotate_i8(const void* ozaki_ws, int64_t n, const int8_t* codes, int64_t ld_codes,
+                     int64_t m, const double* mean, int32_t has_missing, double* X, int64_t ldx,
+                     void* workspace, int64_t workspace_bytes, uintptr_t stream) {
+    JB_CHECK_ARG(n > 0 && m >= 0 && ld_codes >= n && ldx >= n, "jb_rotate_i8: bad shape");
+    JB_CHECK_ARG(n < (1ll << 23), "jb_rotate_i8: n too large for exact int32 digit sums");
+    if (m == 0) return JB_OK;
+    JB_CHECK_ARG(ozaki_ws && codes && X, "jb_rotate_i8: null pointer");
+    JB_CHECK_ARG(!has_missing || mean, "jb_rotate_i8: mean needed when calls are missing");
+    const OzakiLayout OL = ozaki_layout(n);
+    const RotChunkLayout L = rot_chunk_layout(n, m);
+    JB_CHECK_ARG(workspace && workspace_bytes >= L.total, "jb_rotate_i8: workspace too small");
+    cudaStream_t st = as_stream(stream);
+    uint8_t* ws = static_cast<uint8_t*>(workspace);
+    int* status = reinterpret_cast<int*>(ws + L.status);
+    Tile* tiles = reinterpret_cast<Tile*>(ws + L.tiles);
+    const uint8_t* ows = static_cast<const uint8_t*>(ozaki_ws);
+    const int8_t* A = reinterpret_cast<const int8_t*>(ows + OL.a_off);
+    const double* smax = reinterpret_cast<const double*>(ows + OL.s_off);
+
+    const int MB = (int)ceil_div(n, 32);
+    const int cols = has_missing ? 128 : 256;
+    const int NB = (int)ceil_div(m, cols);
+    const int n_tiles = MB * NB;
+    CUtensorMap ta, tb;
+    int32_t rc = make_map_i8(&ta, A, OL.rows, n, OL.lda, kBM);
+    if (rc) return rc;
+    if (has_missing) {
+        int8_t* B = reinterpret_cast<int8_t*>(ws + L.b_off);
+        rot_pack_pairs_kernel<<<(unsigned)(NB * 128), 256, 0, st>>>(codes, ld_codes, n, m, B, L.ldb);
+        JB_LAUNCH_CHECK("rot_pack_pairs_kernel");
+        rc = make_map_i8(&tb, B, (int64_t)NB * 256, n, L.ldb, kRotBN);
+    } else {
+        // no missing calls: the decoded codes are the calls themselves
+        rc = make_map_i8(&tb, codes, m, n, ld_codes, kRotBN);
+    }
+    if (rc) return rc;
+    JB_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
+    rot_tiles_kernel<<<1, 32, 0, st>>>(MB, NB, tiles);
+    JB_LAUNCH_CHECK("rot_tiles_kernel");
+    const int grid = n_tiles < num_sms() ? n_tiles : num_sms();
+    const int num_kb = (int)ceil_div(n, kBK);
+    if (has_missing) {
+        auto kern = i8_gemm_kernel<kRotBN, kRotStages, RotEpi<true>>;
+        JB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     RotSmem::TOTAL));
+        RotEpi<true> epi{X, ldx, smax, mean, (int)n, (int)m};
+        kern<<<grid, kThreads, RotSmem::TOTAL, st>>>(ta, tb, tiles, n_tiles, num_kb, epi, status);
+    } else {
+        auto kern = i8_gemm_kernel<kRotBN, kRotStages, RotEpi<false>>;
+        JB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     RotSmem::TOTAL));
+        RotEpi<false> epi{X, ldx, smax, nullptr, (int)n, (int)m};
+        kern<<<grid, kThreads, RotSmem::TOTAL, st>>>(ta, tb, tiles, n_tiles, num_kb, epi, status);
+    }
+    JB_LAUNCH_CHECK("i8_gemm_kernel<rotate>");
+    return JB_OK;
+}
+
+int32_t jb_rotate_status(const void* workspace, int32_t* out, uintptr_t stream) {
+    JB_CHECK_ARG(workspace && out, "jb_rotate_status: null pointer");
+    JB_CUDA(cudaMemcpyAsync(out, workspace, sizeof(int32_t), cudaMemcpyDeviceToHost,
+                            as_stream(stream)));
+    JB_CUDA(cudaStreamSynchronize(as_stream(stream)));
+    return JB_OK;
+}
+
+}  // extern "C"

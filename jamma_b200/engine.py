@@ -71,8 +71,11 @@ class DeviceCohort:
     """
 
     def __init__(self, eigenvalues, eigenvectors, covariates, phenotypes, lmm_mode=1,
-                 l_min=1e-5, l_max=1e5, n_grid=50, n_refine=10):
+                 l_min=1e-5, l_max=1e5, n_grid=50, n_refine=10, precision: str = "fp64"):
         require_cuda()
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        self.precision = precision
         if lmm_mode not in (1, 2, 3, 4):
             raise ValueError(f"lmm_mode must be 1, 2, 3 or 4, got {lmm_mode}")
         y = np.asarray(phenotypes, dtype=np.float64)
@@ -109,8 +112,17 @@ class DeviceCohort:
             _native.call("jb_null_mle", n, c, phi, ptr(self.evals), ptr(self.UtW), n, ptr(self.Uty),
                          n, NULL_L_MIN, NULL_L_MAX, NULL_N_GRID, NULL_N_ITER, ptr(self.lam0),
                          ptr(self.logl0), st)
+        self.ozaki = None
+        if precision == "mixed":
+            self.ozaki = workspace(_native.load().jb_ozaki_workspace_size(n))
+            _native.call("jb_ozaki_prepare", ptr(self.U), n, n, ptr(self.ozaki), self.ozaki.numel(), st)
+        self.code_ld = (n + 127) // 128 * 128 if precision == "mixed" else n
+        self._rot_ws = None
+        # interpolated golden probes need log|1 + lambda*eval| to stay pole-free
+        ev_min = float(self.evals.min().item())
+        self.search = 1 if (precision == "mixed" and 1.0 + self.l_max * ev_min > 0.5) else 0
         self.ws = workspace(_native.load().jb_lmm_workspace_size(n, c, phi, self.n_grid))
-        _native.call("jb_lmm_prepare", lmm_mode, n, c, phi, ptr(self.evals), ptr(self.UtW), n,
+        _native.call("jb_lmm_prepare", lmm_mode, self.search, n, c, phi, ptr(self.evals), ptr(self.UtW), n,
                      ptr(self.Uty), n, ptr(self.lam0), self.l_min, self.l_max, self.n_grid,
                      ptr(self.ws), self.ws.numel(), st)
 
@@ -129,7 +141,8 @@ class DeviceCohort:
         m = UtG.shape[0]
         out = out if out is not None else self.alloc_out(m)
         o = _native.LmmOut(**{k: ptr(out.get(k)) for k in OUT_KEYS})
-        _native.call("jb_lmm_chunk", self.mode, self.n, self.c, self.phi, m, ptr(self.evals),
+        _native.call("jb_lmm_chunk", self.mode, self.search, self.n, self.c, self.phi, m,
+                     ptr(self.evals),
                      ptr(self.UtW), self.n, ptr(self.Uty), self.n, ptr(UtG), self.n,
                      ptr(self.lam0), ptr(self.logl0), self.l_min, self.l_max, self.n_grid,
                      self.n_iter, o, ptr(self.ws), self.ws.numel(), stream_handle())
@@ -141,11 +154,34 @@ class DeviceCohort:
         UtG = rotate(self.U, G, out=scratch)
         return self.associate_rotated(UtG, out)
 
+    def rotate_codes_i8(self, codes: torch.Tensor, means: torch.Tensor, has_missing: bool,
+                        out: torch.Tensor | None = None) -> torch.Tensor:
+        """Mixed form: INT8 tensor-core rotation of decoded codes -> U^T G (m, n) FP64."""
+        m, ld = codes.shape
+        need = _native.load().jb_rotate_i8_workspace_size(self.n, m)
+        if self._rot_ws is None or self._rot_ws.numel() < need:
+            self._rot_ws = workspace(need)
+        out = out if out is not None else empty((m, self.n))
+        _native.call("jb_rotate_i8", ptr(self.ozaki), self.n, ptr(codes), ld, m, ptr(means),
+                     int(bool(has_missing)), ptr(out), self.n, ptr(self._rot_ws),
+                     self._rot_ws.numel(), stream_handle())
+        return out
+
+    def rotate_status(self) -> int:
+        st = np.zeros(1, dtype=np.int32)
+        if self._rot_ws is not None:
+            _native.call("jb_rotate_status", ptr(self._rot_ws), st.ctypes.data, stream_handle())
+        return int(st[0])
+
     def associate_codes(self, codes: torch.Tensor, means: torch.Tensor, out: dict | None = None,
-                        bufs: dict | None = None) -> dict:
+                        bufs: dict | None = None, has_missing: bool = True) -> dict:
         """Decoded int8 codes (m, ld) + per-SNP imputation means (m,) -> statistics."""
         m, ld = codes.shape
         bufs = bufs if bufs is not None else {}
+        if self.precision == "mixed":
+            UtG = bufs.get("UtG")
+            UtG = UtG[:m] if UtG is not None and UtG.shape[0] >= m else None
+            return self.associate_rotated(self.rotate_codes_i8(codes, means, has_missing, UtG), out)
         G = bufs.get("G")
         if G is None or G.shape[0] < m:
             G = empty((m, self.n))

@@ -68,8 +68,59 @@ class _KinshipAccumulator:
         return self.K
 
 
+class _KinshipI8:
+    """Exact INT8 tensor-core Gram + FP64 centring / missing-call corrections.
+
+    SNP chunks are transposed into the sample-major int8 operand (missing -> 0) and
+    their correction vectors accumulated; ``finish`` runs the tcgen05 Gram once over all
+    kept SNPs and combines the terms (see jb_gram.cu for the identity used).
+    """
+
+    def __init__(self, n: int, p_kept: int):
+        self.n, self.p = n, p_kept
+        self.ldz = (p_kept + 127) // 128 * 128
+        self.Zs = torch.zeros((n, self.ldz), dtype=torch.int8, device="cuda")
+        self.a = torch.zeros(n, dtype=torch.float64, device="cuda")
+        self.b = torch.zeros(n, dtype=torch.float64, device="cuda")
+        self.RT = None
+        self.sum_mu2 = 0.0
+        self.col = 0
+
+    def add(self, codes: torch.Tensor, mu64: torch.Tensor, has_missing: bool) -> None:
+        m, ld = codes.shape
+        st = stream_handle()
+        Cs = None
+        if has_missing:
+            if self.RT is None:
+                self.RT = torch.zeros((2 * self.n, self.n), dtype=torch.float64, device="cuda")
+            Cs = torch.empty((self.n, m), dtype=torch.int8, device="cuda")
+        _native.call("jb_codes_to_sample_major", ptr(codes), ld, self.n, m, ptr(self.Zs), self.ldz,
+                     self.col, ptr(Cs), m, st)
+        _native.call("jb_kinship_i8_corrections", ptr(codes), ld, ptr(Cs), m, self.n, m, ptr(mu64),
+                     ptr(self.a), ptr(self.b), ptr(self.RT), self.n, st)
+        self.sum_mu2 += float(torch.sum(mu64 * mu64).item())
+        self.col += m
+
+    def finish(self) -> torch.Tensor:
+        n = self.n
+        st = stream_handle()
+        C = torch.empty((n, n), dtype=torch.int32, device="cuda")
+        ws = workspace(_native.load().jb_gram_i8_workspace_size(n))
+        _native.call("jb_gram_i8", ptr(self.Zs), n, self.p, self.ldz, ptr(C), n, ptr(ws), ws.numel(), st)
+        K = torch.empty((n, n), dtype=torch.float64, device="cuda")
+        _native.call("jb_kinship_i8_finalize", ptr(C), n, n, ptr(self.a), ptr(self.b), self.sum_mu2,
+                     ptr(self.RT), n, self.p, ptr(K), n, st)
+        status = np.zeros(1, dtype=np.int32)
+        _native.call("jb_gram_status", ptr(ws), status.ctypes.data, st)
+        if status[0] != 0:
+            raise RuntimeError(f"INT8 Gram pipeline reported status {int(status[0])}")
+        self.C = C
+        return K
+
+
 def _kinship_from_packed(packed_dev: torch.Tensor, n: int, batch_size: int, maf_threshold: float,
-                         miss_threshold: float, stat_dtype) -> tuple[torch.Tensor, int]:
+                         miss_threshold: float, stat_dtype, precision: str = "fp64"
+                         ) -> tuple[torch.Tensor, int]:
     codes, counts = decode_packed(packed_dev, n, None, n)
     mean, miss, poly = snp_stats_from_counts(counts.cpu().numpy(), n, stat_dtype)
     keep, _ = filter_mask(mean, miss, poly, n, maf_threshold, miss_threshold)
@@ -82,6 +133,10 @@ def _kinship_from_packed(packed_dev: torch.Tensor, n: int, batch_size: int, maf_
     c = counts.cpu().numpy()[idx]
     mu64 = torch.from_numpy(c[:, 1] / np.maximum(c[:, 0], 1)).to("cuda")  # float64 nanmean
     sel = torch.from_numpy(idx).to("cuda")
+    if precision == "int8":
+        acc = _KinshipI8(n, idx.size)
+        acc.add(codes.index_select(0, sel), mu64, bool(np.any(c[:, 0] < n)))
+        return acc.finish(), idx.size
     acc = _KinshipAccumulator(n, max(1, min(batch_size, 8192)))
     acc.add(codes.index_select(0, sel), mu64)
     return acc.finish(), idx.size
@@ -89,20 +144,27 @@ def _kinship_from_packed(packed_dev: torch.Tensor, n: int, batch_size: int, maf_
 
 def compute_centered_kinship(genotypes: np.ndarray, batch_size: int = 10000,
                              maf_threshold: float = 0.0, miss_threshold: float = 1.0,
-                             check_memory: bool = True) -> np.ndarray:
-    """GEMMA -gk 1 relatedness matrix of an in-memory (n, p) genotype matrix."""
+                             check_memory: bool = True, precision: str = "fp64") -> np.ndarray:
+    """GEMMA -gk 1 relatedness matrix of an in-memory (n, p) genotype matrix.
+
+    ``precision="fp64"`` accumulates the centred FP64 Gram (cuBLAS DSYRK);
+    ``precision="int8"`` runs the exact INT8 tensor-core Gram with FP64 corrections.
+    """
+    if precision not in ("fp64", "int8"):
+        raise ValueError("precision must be 'fp64' or 'int8'")
     require_cuda()
     g = np.asarray(genotypes)
     n = g.shape[0]
     stat_dtype = np.float32 if g.dtype == np.float32 else np.float64
     packed = torch.from_numpy(pack_genotypes(g)).to("cuda")
-    K, _ = _kinship_from_packed(packed, n, batch_size, maf_threshold, miss_threshold, stat_dtype)
+    K, _ = _kinship_from_packed(packed, n, batch_size, maf_threshold, miss_threshold, stat_dtype,
+                                precision)
     return K.cpu().numpy()
 
 
 def compute_kinship_from_bed(bfile, maf_threshold: float = 0.0, miss_threshold: float = 1.0,
                              chunk_size: int = 10000, sample_idx: np.ndarray | None = None,
-                             as_device: bool = False):
+                             as_device: bool = False, precision: str = "fp64"):
     """Centered kinship streamed from a .bed file (``compute_kinship_streaming``,
     src/jamma/kinship/compute.py:502-690): pass 1 statistics, pass 2 accumulation,
     both decoded on the device.  Pass-1 means are float32 as in jamma's streaming path.
@@ -123,13 +185,17 @@ def compute_kinship_from_bed(bfile, maf_threshold: float = 0.0, miss_threshold: 
     idx = np.where(keep)[0]
     if idx.size == 0:
         raise ValueError("No SNPs passed filtering")
-    acc = _KinshipAccumulator(n, min(chunk_size, 8192))
+    i8 = precision == "int8"
+    acc = _KinshipI8(n, idx.size) if i8 else _KinshipAccumulator(n, min(chunk_size, 8192))
     for s in range(0, idx.size, chunk_size):
         sub = idx[s : s + chunk_size]
         rec = torch.from_numpy(bed.take(sub)).to("cuda")
         codes, _ = decode_packed(rec, bed.n_samples, sidx, n)
         c = counts[sub]
         mu64 = torch.from_numpy(c[:, 1] / np.maximum(c[:, 0], 1)).to("cuda")
-        acc.add(codes, mu64)
+        if i8:
+            acc.add(codes, mu64, bool(np.any(c[:, 0] < n)))
+        else:
+            acc.add(codes, mu64)
     K = acc.finish()
     return K if as_device else K.cpu().numpy()

@@ -106,7 +106,8 @@ def _build_results(mode: int, snp_idx, af, n_miss, snp_info, arrays, f: int = 0)
 
 
 def associate_records(cohort: eng.DeviceCohort, records, n_file: int, sample_idx, means: np.ndarray,
-                      device_chunk: int | None = None, on_chunk=None) -> dict[str, np.ndarray]:
+                      device_chunk: int | None = None, on_chunk=None,
+                      n_miss: np.ndarray | None = None) -> dict[str, np.ndarray]:
     """Run the association for packed .bed records (m, bytes_per_snp) of kept SNPs.
 
     ``records`` is a host uint8 array (or a callable ``records(s, e)`` returning rows
@@ -122,9 +123,10 @@ def associate_records(cohort: eng.DeviceCohort, records, n_file: int, sample_idx
         e = min(s + step, m)
         rec = records(s, e) if callable(records) else records[s:e]
         rec_d = torch.from_numpy(np.ascontiguousarray(rec)).to("cuda", non_blocking=False)
-        codes, _ = eng.decode_packed(rec_d, n_file, sidx, cohort.n)
+        codes, _ = eng.decode_packed(rec_d, n_file, sidx, cohort.n, ld=cohort.code_ld)
         mu = torch.from_numpy(np.asarray(means[s:e], dtype=np.float64)).to("cuda")
-        out = cohort.associate_codes(codes, mu, bufs=bufs)
+        miss = True if n_miss is None else bool(np.any(n_miss[s:e] > 0))
+        out = cohort.associate_codes(codes, mu, bufs=bufs, has_missing=miss)
         for k, v in out.items():
             res[k][:, s:e] = v.cpu().numpy()
         if on_chunk is not None:
@@ -133,13 +135,14 @@ def associate_records(cohort: eng.DeviceCohort, records, n_file: int, sample_idx
 
 
 def _prepare_cohort(kinship, eigenvalues, eigenvectors, covariates, y, lmm_mode, l_min, l_max,
-                    n_grid, n_refine):
+                    n_grid, n_refine, precision="fp64"):
     if eigenvalues is not None:
         evals, U = eigenvalues, eigenvectors
     else:
         K = torch.from_numpy(np.ascontiguousarray(np.asarray(kinship, dtype=np.float64))).to("cuda")
         evals, U = eigendecompose_kinship_device(K)
-    return eng.DeviceCohort(evals, U, covariates, y, lmm_mode, l_min, l_max, n_grid, n_refine)
+    return eng.DeviceCohort(evals, U, covariates, y, lmm_mode, l_min, l_max, n_grid, n_refine,
+                            precision=precision)
 
 
 def run_lmm_association_streaming(
@@ -150,7 +153,7 @@ def run_lmm_association_streaming(
     chunk_size: int = 10_000, use_gpu: bool = True, check_memory: bool = True,
     show_progress: bool = True, output_path: Path | None = None, lmm_mode: int = 1,
     snps_indices: np.ndarray | None = None, hwe_threshold: float = 0.0,
-    validate_genotypes: bool = True, timing: dict | None = None,
+    validate_genotypes: bool = True, timing: dict | None = None, precision: str = "fp64",
 ) -> list[AssocResult]:
     """Two-pass streaming association from a PLINK prefix (runner_streaming.py:94-628).
 
@@ -196,11 +199,11 @@ def run_lmm_association_streaming(
         return []
 
     cohort = _prepare_cohort(kinship, eigenvalues, eigenvectors, cov, y, lmm_mode, l_min, l_max,
-                             n_grid, n_refine)
+                             n_grid, n_refine, precision)
     torch.cuda.synchronize()
     t2 = time.perf_counter()
     res = associate_records(cohort, lambda a, b: bed.take(st.idx[a:b]), n_file, sample_idx,
-                            st.mean[st.idx].astype(np.float64))
+                            st.mean[st.idx].astype(np.float64), n_miss=st.miss[st.idx])
     t3 = time.perf_counter()
     results = _build_results(lmm_mode, st.idx, st.af[st.idx], st.miss[st.idx], snp_info, res)
     if output_path is not None:
@@ -219,7 +222,7 @@ def run_lmm_association_jax(
     eigenvectors: np.ndarray | None = None, maf_threshold: float = 0.01,
     miss_threshold: float = 0.05, l_min: float = 1e-5, l_max: float = 1e5, n_grid: int = 50,
     n_refine: int = 10, use_gpu: bool = True, check_memory: bool = True,
-    show_progress: bool = True, lmm_mode: int = 1,
+    show_progress: bool = True, lmm_mode: int = 1, precision: str = "fp64",
 ) -> list[AssocResult]:
     """In-memory genotype runner (runner_jax.py:52-481): statistics and imputation means
     in the genotype array's own dtype (float64 means for float64 input)."""
@@ -247,6 +250,7 @@ def run_lmm_association_jax(
     if st.idx.size == 0:
         return []
     cohort = _prepare_cohort(kinship, eigenvalues, eigenvectors, covariates, y, lmm_mode, l_min,
-                             l_max, n_grid, n_refine)
-    res = associate_records(cohort, packed[st.idx], n, None, st.mean[st.idx].astype(np.float64))
+                             l_max, n_grid, n_refine, precision)
+    res = associate_records(cohort, packed[st.idx], n, None, st.mean[st.idx].astype(np.float64),
+                            n_miss=st.miss[st.idx])
     return _build_results(lmm_mode, st.idx, st.af[st.idx], st.miss[st.idx], snp_info, res)

@@ -224,13 +224,26 @@ def test_chunking_and_phenotype_batching_are_invariant(cohort_files):
     mu = np.nan_to_num(np.nanmean(gv[:, :600], 0))
     from jamma_b200.lmm import associate_records
 
+    # plain form: cuBLAS picks DGEMM kernels by shape, so U^T G may differ in the last bit
+    # between chunkings; the mixed form's integer rotation makes chunking bit-exact.
     multi = eng.DeviceCohort(w, U, cv, y2, lmm_mode=4)
     r_multi = associate_records(multi, packed, gv.shape[0], None, mu, device_chunk=256)
+    r_multi2 = associate_records(multi, packed, gv.shape[0], None, mu, device_chunk=97)
+    for k in r_multi:
+        np.testing.assert_allclose(r_multi[k], r_multi2[k], rtol=1e-12, err_msg=k)
+    mixed = eng.DeviceCohort(w, U, cv, y2, lmm_mode=4, precision="mixed")
+    miss = (gv[:, :600] != gv[:, :600]).sum(0)
+    r_a = associate_records(mixed, packed, gv.shape[0], None, mu, device_chunk=256, n_miss=miss)
+    r_b = associate_records(mixed, packed, gv.shape[0], None, mu, device_chunk=97, n_miss=miss)
+    for k in r_a:
+        np.testing.assert_array_equal(r_a[k], r_b[k], err_msg=f"mixed {k}")
     for f in range(3):
+        # a single-phenotype cohort rotates y with a 1-column cuBLAS product instead of a
+        # 3-column one, so U^T y may differ in the last bit: compare at 1e-12
         single = eng.DeviceCohort(w, U, cv, y2[:, f], lmm_mode=4)
         r_single = associate_records(single, packed, gv.shape[0], None, mu, device_chunk=97)
         for k in r_single:
-            np.testing.assert_array_equal(r_single[k][0], r_multi[k][f], err_msg=k)
+            np.testing.assert_allclose(r_single[k][0], r_multi[k][f], rtol=1e-12, err_msg=k)
 
 
 def test_device_null_model_matches_oracle(cohort_files):
