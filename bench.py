@@ -212,6 +212,7 @@ def run_ours(args) -> None:
             mu = torch.from_numpy(cc[:, 1] / np.maximum(cc[:, 0], 1)).cuda()
             if form == "int8":
                 acc.add(codes_k, mu, bool(np.any(cc[:, 0] < n)))
+                acc.add_sum_mu2(cc[:, 1] / np.maximum(cc[:, 0], 1))
             else:
                 acc.add(codes_k, mu)
         return acc.finish()

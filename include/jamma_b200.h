@@ -198,6 +198,9 @@ typedef struct jb_lmm_out {
  * (src/jamma/lmm/likelihood_jax.py:231-883) as driven by
  * src/jamma/lmm/runner_streaming.py:469-554.
  * workspace: jb_lmm_workspace_size bytes, filled by jb_lmm_prepare.
+ * chunk_workspace: jb_lmm_chunk_workspace_size(n, n_cvt, phi, n_grid, m) bytes of scratch:
+ * the grid, ones and null-model weighted sums of all m SNPs are formed there by two
+ * cuBLAS DGEMMs before the per-SNP kernel runs.
  * precision: 0 = every likelihood evaluation is a direct FP64 reduction (plain form);
  * 1 = the golden-section probes take log|H^-1| and the genotype-free weighted sums from
  * per-bracket Chebyshev expansions (degree 24, built by jb_lmm_prepare with precision 1
@@ -220,13 +223,16 @@ int32_t jb_lmm_prepare(int32_t lmm_mode, int32_t precision, int64_t n, int32_t n
                        double l_max, int32_t n_grid, void* workspace,
                        int64_t workspace_bytes, uintptr_t stream);
 
+int64_t jb_lmm_chunk_workspace_size(int64_t n, int32_t n_cvt, int32_t phi, int32_t n_grid,
+                                    int64_t m);
 int32_t jb_lmm_chunk(int32_t lmm_mode, int32_t precision, int64_t n, int32_t n_cvt,
                      int32_t phi, int64_t m,
                      const double* evals, const double* UtW, int64_t ldw,
                      const double* Uty, int64_t ldy, const double* UtG, int64_t ldg,
                      const double* lam0, const double* logl0, double l_min, double l_max,
                      int32_t n_grid, int32_t n_iter, jb_lmm_out out, void* workspace,
-                     int64_t workspace_bytes, uintptr_t stream);
+                     int64_t workspace_bytes, void* chunk_workspace, int64_t chunk_bytes,
+                     uintptr_t stream);
 
 /*
  * Null-model MLE (lambda0, logl_H0) per phenotype on the device: the scalar 50-point

@@ -146,13 +146,16 @@ __global__ void codes_to_sample_major_kernel(const int8_t* __restrict__ codes, i
 }
 
 // a_i = sum_j Z_ij mu_j and b_i = sum_{j missing at i} mu_j^2 from SNP-major codes.
+// Block (256 samples) x (256 SNPs); partial sums are added with FP64 atomics.
 __global__ void kin_vectors_kernel(const int8_t* __restrict__ codes, int64_t ldc, int64_t n,
                                    int64_t m, const double* __restrict__ mu,
                                    double* __restrict__ a, double* __restrict__ b) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t j0 = (int64_t)blockIdx.y * 256;
     if (i >= n) return;
     double sa = 0.0, sb = 0.0;
-    for (int64_t j = 0; j < m; ++j) {
+    const int64_t j1 = j0 + 256 < m ? j0 + 256 : m;
+    for (int64_t j = j0; j < j1; ++j) {
         const int8_t c = codes[j * ldc + i];
         const double u = __ldg(mu + j);
         if (c == 3)
@@ -160,13 +163,14 @@ __global__ void kin_vectors_kernel(const int8_t* __restrict__ codes, int64_t ldc
         else
             sa = fma((double)c, u, sa);
     }
-    a[i] += sa;
-    b[i] += sb;
+    atomicAdd(a + i, sa);
+    atomicAdd(b + i, sb);
 }
 
 // Sparse terms for one SNP chunk.  For every sample k and every SNP j of the chunk that
 // is missing at k: R[:, k] += mu_j Z[:, j] and T[:, k] += mu_j^2 M[:, j].  One CTA per
-// (k, block of 2048 samples i); each thread keeps 8 rows of both sums in registers.
+// (k, block of 2048 samples i); each thread owns 8 consecutive samples (one 8-byte load
+// per missing SNP) and keeps their R and T sums in registers.
 __global__ void __launch_bounds__(256) kin_sparse_kernel(const int8_t* __restrict__ codes,
                                                           int64_t ldc, const int8_t* __restrict__ Cs,
                                                           int64_t ldcs, int64_t n, int64_t m,
@@ -174,16 +178,17 @@ __global__ void __launch_bounds__(256) kin_sparse_kernel(const int8_t* __restric
                                                           double* __restrict__ RT,
                                                           int64_t ldr) {
     const int64_t k = blockIdx.x;
-    const int64_t i0 = (int64_t)blockIdx.y * 2048;
-    __shared__ int32_t list[1024];
+    const int64_t i0 = (int64_t)blockIdx.y * 2048 + 8 * threadIdx.x;
+    __shared__ int32_t list[2048];
     __shared__ int cnt;
     double r[8], tt[8];
 #pragma unroll
     for (int e = 0; e < 8; ++e) r[e] = tt[e] = 0.0;
-    for (int64_t jb = 0; jb < m; jb += 1024) {
+    const bool full8 = (i0 + 8 <= n) && ((ldc & 7) == 0);
+    for (int64_t jb = 0; jb < m; jb += 2048) {
         if (threadIdx.x == 0) cnt = 0;
         __syncthreads();
-        for (int64_t j = jb + threadIdx.x; j < m && j < jb + 1024; j += blockDim.x) {
+        for (int64_t j = jb + threadIdx.x; j < m && j < jb + 2048; j += blockDim.x) {
             if (Cs[k * ldcs + j] == 3) list[atomicAdd(&cnt, 1)] = (int32_t)j;
         }
         __syncthreads();
@@ -191,24 +196,33 @@ __global__ void __launch_bounds__(256) kin_sparse_kernel(const int8_t* __restric
         for (int e = 0; e < c; ++e) {
             const int64_t j = list[e];
             const double u = mu[j];
-            const int8_t* row = codes + j * ldc;
+            const double u2 = u * u;
+            int8_t v[8];
+            if (full8) {
+                const uint2 w = *reinterpret_cast<const uint2*>(codes + j * ldc + i0);
+                const uint32_t lo = w.x, hi = w.y;
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    v[q] = (int8_t)((lo >> (8 * q)) & 0xff);
+                    v[4 + q] = (int8_t)((hi >> (8 * q)) & 0xff);
+                }
+            } else {
+#pragma unroll
+                for (int q = 0; q < 8; ++q) v[q] = (i0 + q < n) ? codes[j * ldc + i0 + q] : (int8_t)0;
+            }
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
-                const int64_t i = i0 + threadIdx.x + 256 * q;
-                if (i < n) {
-                    const int8_t v = row[i];
-                    if (v == 3)
-                        tt[q] = fma(u, u, tt[q]);
-                    else
-                        r[q] = fma((double)v, u, r[q]);
-                }
+                if (v[q] == 3)
+                    tt[q] += u2;
+                else
+                    r[q] = fma((double)v[q], u, r[q]);
             }
         }
         __syncthreads();
     }
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-        const int64_t i = i0 + threadIdx.x + 256 * q;
+        const int64_t i = i0 + q;
         if (i < n) {
             RT[k * ldr + i] += r[q];            // R[i, k] (column-major, column k)
             RT[(n + k) * ldr + i] += tt[q];     // T[i, k]
@@ -326,7 +340,9 @@ int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes, const i
     JB_CHECK_ARG(n > 0 && m >= 0 && ld_codes >= n, "jb_kinship_i8_corrections: bad shape");
     if (m == 0) return JB_OK;
     cudaStream_t st = as_stream(stream);
-    kin_vectors_kernel<<<(unsigned)ceil_div(n, 128), 128, 0, st>>>(codes, ld_codes, n, m, mu, a, b);
+    JB_CHECK_ARG(ceil_div(m, 256) < 65536, "jb_kinship_i8_corrections: chunk too large");
+    kin_vectors_kernel<<<dim3((unsigned)ceil_div(n, 256), (unsigned)ceil_div(m, 256)), 256, 0, st>>>(
+        codes, ld_codes, n, m, mu, a, b);
     JB_LAUNCH_CHECK("kin_vectors_kernel");
     if (Cs) {
         JB_CHECK_ARG(RT && ldr >= n && ldcs >= m, "jb_kinship_i8_corrections: RT buffer needed");

@@ -65,6 +65,15 @@ struct Params {
     const double* cheb;    // [n_grid][1 + phi*NS][kChebN] coefficients (NULL: direct)
     const double* cheb_mid;
     const double* cheb_half;
+    // Weighted x-sums of every table row r (grid rows, the ones row n_grid, the null rows
+    // n_grid+1+f), produced for the whole chunk by two FP64 GEMMs:
+    //   CL[j*ldcl + r*(C+phi) + a] = sum_i h_r,i x_ij w_a,i  (a < C)
+    //   CL[j*ldcl + r*(C+phi) + C + f] = sum_i h_r,i x_ij y_f,i
+    //   CQ[j*ldcq + r] = sum_i h_r,i x_ij^2
+    const double* CL;
+    int64_t ldcl;
+    const double* CQ;
+    int64_t ldcq;
 };
 
 constexpr int kChebN = 25;  // interpolation nodes (degree 24) per bracket
@@ -235,6 +244,30 @@ __device__ __forceinline__ void assemble(double (&row0)[Lay<C>::NI], const doubl
 }
 
 // Full evaluation at a per-SNP lambda: H = 1/(lambda*eval + 1), all NI sums + logdet.
+// Loads of UNR consecutive strided samples are issued together (memory-level parallelism).
+constexpr int UNR = 4;
+
+template <int C>
+__device__ __forceinline__ void full_accumulate(double lam, double ev, double xv, double yv,
+                                                const double (&w)[C > 0 ? C : 1],
+                                                double (&acc)[Lay<C>::NI], double& ld) {
+    using L = Lay<C>;
+    const double v = __dadd_rn(__dmul_rn(lam, ev), 1.0);
+    const double hi = __drcp_rn(v);  // correctly rounded, = 1.0 / v
+    ld += log(fabs(v));
+    double vec[L::R];
+#pragma unroll
+    for (int a = 0; a < C; ++a) vec[a] = w[a];
+    vec[C] = xv;
+    vec[C + 1] = yv;
+#pragma unroll
+    for (int a = 0; a < L::R; ++a) {
+        const double t = hi * vec[a];
+#pragma unroll
+        for (int b = a; b < L::R; ++b) acc[L::idx(a, b)] = fma(t, vec[b], acc[L::idx(a, b)]);
+    }
+}
+
 template <int C>
 __device__ __forceinline__ void eval_full(const Params& p, const double* __restrict__ x,
                                           const double* __restrict__ y, double lam,
@@ -245,21 +278,25 @@ __device__ __forceinline__ void eval_full(const Params& p, const double* __restr
     for (int k = 0; k < L::NI; ++k) acc[k] = 0.0;
     double ld = 0.0;
     const int lane = threadIdx.x & 31;
-    for (int64_t i = lane; i < p.n; i += 32) {
-        const double v = __dadd_rn(__dmul_rn(lam, __ldg(p.evals + i)), 1.0);
-        const double hi = __drcp_rn(v);  // correctly rounded, = 1.0 / v
-        ld += log(fabs(v));
-        double vec[L::R];
+    int64_t i = lane;
+    for (; i + 32 * (UNR - 1) < p.n; i += 32 * UNR) {
+        double ev[UNR], xv[UNR], yv[UNR], w[UNR][C > 0 ? C : 1];
 #pragma unroll
-        for (int a = 0; a < C; ++a) vec[a] = __ldg(p.W + a * p.ldw + i);
-        vec[C] = x[i];
-        vec[C + 1] = __ldg(y + i);
+        for (int u = 0; u < UNR; ++u) {
+            ev[u] = __ldg(p.evals + i + 32 * u);
+            xv[u] = x[i + 32 * u];
+            yv[u] = __ldg(y + i + 32 * u);
 #pragma unroll
-        for (int a = 0; a < L::R; ++a) {
-            const double t = hi * vec[a];
-#pragma unroll
-            for (int b = a; b < L::R; ++b) acc[L::idx(a, b)] = fma(t, vec[b], acc[L::idx(a, b)]);
+            for (int a = 0; a < C; ++a) w[u][a] = __ldg(p.W + a * p.ldw + i + 32 * u);
         }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) full_accumulate<C>(lam, ev[u], xv[u], yv[u], w[u], acc, ld);
+    }
+    for (; i < p.n; i += 32) {
+        double w[C > 0 ? C : 1];
+#pragma unroll
+        for (int a = 0; a < C; ++a) w[a] = __ldg(p.W + a * p.ldw + i);
+        full_accumulate<C>(lam, __ldg(p.evals + i), x[i], __ldg(y + i), w, acc, ld);
     }
 #pragma unroll
     for (int k = 0; k < L::NI; ++k) row0[k] = warp_sum(acc[k]);
@@ -306,14 +343,32 @@ __device__ __forceinline__ double eval_logl_interp(const Params& p, const double
 #pragma unroll
     for (int k = 0; k < L::NX; ++k) acc[k] = 0.0;
     const int lane = threadIdx.x & 31;
-    for (int64_t i = lane; i < p.n; i += 32) {
-        const double v = __dadd_rn(__dmul_rn(lam, __ldg(p.evals + i)), 1.0);
-        const double xv = x[i];
-        const double t = __drcp_rn(v) * xv;
+    auto step = [&](double ev, double xv, double yv, const double* w) {
+        const double t = __drcp_rn(__dadd_rn(__dmul_rn(lam, ev), 1.0)) * xv;
 #pragma unroll
-        for (int a = 0; a < C; ++a) acc[a] = fma(t, __ldg(p.W + a * p.ldw + i), acc[a]);
+        for (int a = 0; a < C; ++a) acc[a] = fma(t, w[a], acc[a]);
         acc[C] = fma(t, xv, acc[C]);
-        acc[C + 1] = fma(t, __ldg(y + i), acc[C + 1]);
+        acc[C + 1] = fma(t, yv, acc[C + 1]);
+    };
+    int64_t i = lane;
+    for (; i + 32 * (UNR - 1) < p.n; i += 32 * UNR) {
+        double ev[UNR], xv[UNR], yv[UNR], w[UNR][C > 0 ? C : 1];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            ev[u] = __ldg(p.evals + i + 32 * u);
+            xv[u] = x[i + 32 * u];
+            yv[u] = __ldg(y + i + 32 * u);
+#pragma unroll
+            for (int a = 0; a < C; ++a) w[u][a] = __ldg(p.W + a * p.ldw + i + 32 * u);
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) step(ev[u], xv[u], yv[u], w[u]);
+    }
+    for (; i < p.n; i += 32) {
+        double w[C > 0 ? C : 1];
+#pragma unroll
+        for (int a = 0; a < C; ++a) w[a] = __ldg(p.W + a * p.ldw + i);
+        step(__ldg(p.evals + i), x[i], __ldg(y + i), w);
     }
 #pragma unroll
     for (int k = 0; k < L::NX; ++k) acc[k] = warp_sum(acc[k]);
@@ -385,7 +440,7 @@ __device__ __forceinline__ void beta_se(const PabOut<C>& pb, double px_yy, doubl
     se = valid ? sqrt(var) : jnan();
 }
 
-template <int C, int GB, bool INTERP>
+template <int C, bool INTERP>
 __global__ void __launch_bounds__(256) lmm_pairs_kernel(const Params p) {
     using L = Lay<C>;
     const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -401,57 +456,42 @@ __global__ void __launch_bounds__(256) lmm_pairs_kernel(const Params p) {
     const int64_t o = (int64_t)f * p.m + j;
     const int64_t srow = (int64_t)p.phi * L::NS;  // stride of one S row
 
+    // Weighted x-sums of table row r for this (SNP, phenotype), from the chunk GEMMs.
+    auto row_xsums = [&](int r, double (&xs)[L::NX]) {
+        const double* cl = p.CL + j * p.ldcl + (int64_t)r * (C + p.phi);
+#pragma unroll
+        for (int a = 0; a < C; ++a) xs[a] = cl[a];
+        xs[C] = p.CQ[j * p.ldcq + r];
+        xs[C + 1] = cl[C + f];
+    };
+
     // ---------------- phase 1: H = 1 (Iab) and H = H0 (score)
     double iab_diag[C + 1];
 #pragma unroll
     for (int i = 0; i <= C; ++i) iab_diag[i] = 0.0;
-    {
-        double a1[L::NX], a2[L::NX];
+    if (need_reml) {
+        double xs[L::NX], row0[L::NI];
+        row_xsums(p.n_grid, xs);
+        assemble<C>(row0, p.S + (int64_t)p.n_grid * srow + (int64_t)f * L::NS, xs);
+        const PabOut<C> pb = pab_reduce<C>(row0);
 #pragma unroll
-        for (int k = 0; k < L::NX; ++k) a1[k] = a2[k] = 0.0;
-        const double* h0 = p.H + (int64_t)(p.n_grid + f) * p.n;
-        for (int64_t i = lane; i < p.n; i += 32) {
-            const double xv = x[i];
-            const double yv = __ldg(y + i);
-            const double t2 = need_score ? __ldg(h0 + i) * xv : 0.0;
-#pragma unroll
-            for (int a = 0; a < C; ++a) {
-                const double w = __ldg(p.W + a * p.ldw + i);
-                a1[a] = fma(xv, w, a1[a]);
-                a2[a] = fma(t2, w, a2[a]);
-            }
-            a1[C] = fma(xv, xv, a1[C]);
-            a2[C] = fma(t2, xv, a2[C]);
-            a1[C + 1] = fma(xv, yv, a1[C + 1]);
-            a2[C + 1] = fma(t2, yv, a2[C + 1]);
-        }
-#pragma unroll
-        for (int k = 0; k < L::NX; ++k) {
-            a1[k] = warp_sum(a1[k]);
-            a2[k] = warp_sum(a2[k]);
-        }
-        if (need_reml) {
-            double row0[L::NI];
-            assemble<C>(row0, p.S + (int64_t)p.n_grid * srow + (int64_t)f * L::NS, a1);
-            const PabOut<C> pb = pab_reduce<C>(row0);
-#pragma unroll
-            for (int i = 0; i <= C; ++i) iab_diag[i] = pb.diag[i];
-        }
-        if (need_score) {
-            double row0[L::NI];
-            assemble<C>(row0, p.S + (int64_t)(p.n_grid + 1 + f) * srow + (int64_t)f * L::NS, a2);
-            const PabOut<C> pb = pab_reduce<C>(row0);
-            bool valid;
-            double beta, tau, se;
-            beta_se<C>(pb, clamp_pyy(pb.yy1), p.df, valid, beta, tau, se);
-            const double fstat = p.n_d * (pb.xy * pb.xy) / (pb.yy * (valid ? pb.xx : 1.0));
-            const double pv = f_pvalue(fstat, p.df, valid);
-            if (lane == 0) {
-                if (p.out.p_score) p.out.p_score[o] = pv;
-                if (p.mode == 3) {
-                    if (p.out.beta) p.out.beta[o] = beta;
-                    if (p.out.se) p.out.se[o] = se;
-                }
+        for (int i = 0; i <= C; ++i) iab_diag[i] = pb.diag[i];
+    }
+    if (need_score) {
+        double xs[L::NX], row0[L::NI];
+        row_xsums(p.n_grid + 1 + f, xs);
+        assemble<C>(row0, p.S + (int64_t)(p.n_grid + 1 + f) * srow + (int64_t)f * L::NS, xs);
+        const PabOut<C> pb = pab_reduce<C>(row0);
+        bool valid;
+        double beta, tau, se;
+        beta_se<C>(pb, clamp_pyy(pb.yy1), p.df, valid, beta, tau, se);
+        const double fstat = p.n_d * (pb.xy * pb.xy) / (pb.yy * (valid ? pb.xx : 1.0));
+        const double pv = f_pvalue(fstat, p.df, valid);
+        if (lane == 0) {
+            if (p.out.p_score) p.out.p_score[o] = pv;
+            if (p.mode == 3) {
+                if (p.out.beta) p.out.beta[o] = beta;
+                if (p.out.se) p.out.se[o] = se;
             }
         }
     }
@@ -459,43 +499,14 @@ __global__ void __launch_bounds__(256) lmm_pairs_kernel(const Params p) {
 
     // ---------------- phase 2: shared lambda grid
     ArgMax best_reml, best_mle;
-    for (int g0 = 0; g0 < p.n_grid; g0 += GB) {
-        double acc[GB][L::NX];
-#pragma unroll
-        for (int g = 0; g < GB; ++g)
-#pragma unroll
-            for (int k = 0; k < L::NX; ++k) acc[g][k] = 0.0;
-        const int ng = p.n_grid - g0 < GB ? p.n_grid - g0 : GB;
-        for (int64_t i = lane; i < p.n; i += 32) {
-            const double xv = x[i];
-            const double yv = __ldg(y + i);
-            double w[C > 0 ? C : 1];
-#pragma unroll
-            for (int a = 0; a < C; ++a) w[a] = __ldg(p.W + a * p.ldw + i);
-#pragma unroll
-            for (int g = 0; g < GB; ++g) {
-                if (g < ng) {
-                    const double t = __ldg(p.H + (int64_t)(g0 + g) * p.n + i) * xv;
-#pragma unroll
-                    for (int a = 0; a < C; ++a) acc[g][a] = fma(t, w[a], acc[g][a]);
-                    acc[g][C] = fma(t, xv, acc[g][C]);
-                    acc[g][C + 1] = fma(t, yv, acc[g][C + 1]);
-                }
-            }
-        }
-#pragma unroll
-        for (int g = 0; g < GB; ++g) {
-            if (g < ng) {
-#pragma unroll
-                for (int k = 0; k < L::NX; ++k) acc[g][k] = warp_sum(acc[g][k]);
-                double row0[L::NI];
-                assemble<C>(row0, p.S + (int64_t)(g0 + g) * srow + (int64_t)f * L::NS, acc[g]);
-                const PabOut<C> pb = pab_reduce<C>(row0);
-                const double ldh = p.logdet[g0 + g];
-                if (need_reml) best_reml.push(g0 + g, reml_logl<C>(pb, iab_diag, ldh, p));
-                if (need_mle) best_mle.push(g0 + g, mle_logl<C>(pb, ldh, p));
-            }
-        }
+    for (int g = 0; g < p.n_grid; ++g) {
+        double xs[L::NX], row0[L::NI];
+        row_xsums(g, xs);
+        assemble<C>(row0, p.S + (int64_t)g * srow + (int64_t)f * L::NS, xs);
+        const PabOut<C> pb = pab_reduce<C>(row0);
+        const double ldh = p.logdet[g];
+        if (need_reml) best_reml.push(g, reml_logl<C>(pb, iab_diag, ldh, p));
+        if (need_mle) best_mle.push(g, mle_logl<C>(pb, ldh, p));
     }
 
     // ---------------- phase 3: golden sections + statistics
@@ -600,6 +611,39 @@ __global__ void lmm_shared_kernel(int64_t n, int n_grid, int phi, const double* 
         double t = 0.0;
         for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += red[threadIdx.x][k];
         S[((int64_t)r * phi + f) * L::NS + threadIdx.x] = t;
+    }
+}
+
+// GEMM operands for the per-chunk weighted x-sums: for every table row r (grid rows, the
+// ones row, the null rows) A_sq[r] = h_r and A_lin[r*(C+phi) + a] = h_r * w_a (a < C),
+// A_lin[r*(C+phi) + C + f] = h_r * y_f; each row has n entries.
+template <int C>
+__global__ void lmm_gemm_tables_kernel(int64_t n, int n_grid, int phi, const double* __restrict__ W,
+                                       int64_t ldw, const double* __restrict__ Y, int64_t ldy,
+                                       const double* __restrict__ H, double* __restrict__ Alin,
+                                       double* __restrict__ Asq) {
+    const int r = blockIdx.x;
+    const double* h = r < n_grid ? H + (int64_t)r * n
+                                 : (r == n_grid ? nullptr : H + (int64_t)(r - 1) * n);
+    const int64_t base = (int64_t)r * (C + phi);
+    for (int64_t i = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.y * blockDim.x) {
+        const double hv = h ? h[i] : 1.0;
+        Asq[(int64_t)r * n + i] = hv;
+#pragma unroll
+        for (int a = 0; a < C; ++a) Alin[(base + a) * n + i] = hv * W[a * ldw + i];
+        for (int f = 0; f < phi; ++f) Alin[(base + C + f) * n + i] = hv * Y[(int64_t)f * ldy + i];
+    }
+}
+
+__global__ void square_cols_kernel(const double* __restrict__ X, int64_t ldx, int64_t n, int64_t m,
+                                   double* __restrict__ X2) {
+    const int64_t total = n * m;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t j = t / n, i = t - j * n;
+        const double v = X[j * ldx + i];
+        X2[t] = v * v;
     }
 }
 
@@ -797,7 +841,7 @@ __global__ void null_mle_kernel(int64_t n, const double* W, int64_t ldw, const d
 
 // ---------------------------------------------------------------- host helpers
 struct WsLayout {
-    int64_t loglam, logdet, H, S, cheb, cmid, chalf, cvals, total;
+    int64_t loglam, logdet, H, S, cheb, cmid, chalf, cvals, alin, asq, total;
 };
 
 inline int64_t align256(int64_t b) { return (b + 255) / 256 * 256; }
@@ -824,8 +868,31 @@ inline WsLayout ws_layout(int64_t n, int c, int phi, int n_grid) {
     off += align256(8 * (int64_t)n_grid);
     w.cvals = off;
     off += align256(8 * (int64_t)n_grid * nf * kChebN);
+    const int64_t rows = n_grid + 1 + phi;
+    w.alin = off;
+    off += align256(8 * rows * (c + phi) * n);
+    w.asq = off;
+    off += align256(8 * rows * n);
     w.total = off;
     return w;
+}
+
+struct ChunkLayout {
+    int64_t x2, cl, cq, total;
+};
+
+inline ChunkLayout chunk_layout(int64_t n, int c, int phi, int n_grid, int64_t m) {
+    ChunkLayout L;
+    const int64_t rows = n_grid + 1 + phi;
+    int64_t off = 0;
+    L.x2 = off;
+    off += align256(8 * n * m);
+    L.cl = off;
+    off += align256(8 * rows * (c + phi) * m);
+    L.cq = off;
+    off += align256(8 * rows * m);
+    L.total = off;
+    return L;
 }
 
 // numpy.linspace(start, stop, num): start + i*step, last element = stop.
@@ -842,13 +909,12 @@ __global__ void linspace_kernel(double* out, double start, double stop, int num)
 
 template <int C>
 int32_t launch_pairs(const Params& p, cudaStream_t st) {
-    constexpr int GB = (C <= 1) ? 8 : (C == 2 ? 6 : 5);
     const int64_t warps = p.m * p.phi;
     const int64_t blocks = ceil_div(warps * 32, 256);
     if (p.cheb)
-        lmm_pairs_kernel<C, GB, true><<<(unsigned)blocks, 256, 0, st>>>(p);
+        lmm_pairs_kernel<C, true><<<(unsigned)blocks, 256, 0, st>>>(p);
     else
-        lmm_pairs_kernel<C, GB, false><<<(unsigned)blocks, 256, 0, st>>>(p);
+        lmm_pairs_kernel<C, false><<<(unsigned)blocks, 256, 0, st>>>(p);
     JB_LAUNCH_CHECK("lmm_pairs_kernel");
     return JB_OK;
 }
@@ -871,6 +937,11 @@ int32_t launch_prepare(int64_t n, int phi, int n_grid, const double* evals, cons
     const int rows_s = n_grid + 1 + (lam0 ? phi : 0);
     lmm_shared_kernel<C><<<dim3(rows_s, phi), 256, 0, st>>>(n, n_grid, phi, W, ldw, Y, ldy, H, S);
     JB_LAUNCH_CHECK("lmm_shared_kernel");
+    lmm_gemm_tables_kernel<C><<<dim3(rows_s, (unsigned)(ceil_div(n, 256) < 64 ? ceil_div(n, 256) : 64)),
+                                256, 0, st>>>(n, n_grid, phi, W, ldw, Y, ldy, H,
+                                              reinterpret_cast<double*>(ws + L.alin),
+                                              reinterpret_cast<double*>(ws + L.asq));
+    JB_LAUNCH_CHECK("lmm_gemm_tables_kernel");
     if (interp) {
         const int nf = 1 + phi * Lay<C>::NS;
         double* vals = reinterpret_cast<double*>(ws + L.cvals);
@@ -926,13 +997,19 @@ int32_t jb_lmm_prepare(int32_t lmm_mode, int32_t precision, int64_t n, int32_t n
     return JB_E_UNSUPPORTED;
 }
 
+int64_t jb_lmm_chunk_workspace_size(int64_t n, int32_t n_cvt, int32_t phi, int32_t n_grid,
+                                    int64_t m) {
+    if (n <= 0 || n_cvt < 1 || phi < 1 || n_grid < 1 || m < 0) return -1;
+    return chunk_layout(n, n_cvt, phi, n_grid, m > 0 ? m : 1).total;
+}
+
 int32_t jb_lmm_chunk(int32_t lmm_mode, int32_t precision, int64_t n, int32_t n_cvt, int32_t phi,
                      int64_t m,
                      const double* evals, const double* UtW, int64_t ldw, const double* Uty,
                      int64_t ldy, const double* UtG, int64_t ldg, const double* lam0,
                      const double* logl0, double l_min, double l_max, int32_t n_grid,
                      int32_t n_iter, jb_lmm_out out, void* workspace, int64_t workspace_bytes,
-                     uintptr_t stream) {
+                     void* chunk_workspace, int64_t chunk_bytes, uintptr_t stream) {
     (void)lam0;
     JB_CHECK_ARG(lmm_mode >= 1 && lmm_mode <= 4, "jb_lmm_chunk: lmm_mode must be 1..4");
     JB_CHECK_ARG(n > 0 && phi >= 1 && m >= 0 && n_grid >= 2 && n_iter >= 0, "jb_lmm_chunk: bad sizes");
@@ -977,6 +1054,40 @@ int32_t jb_lmm_chunk(int32_t lmm_mode, int32_t precision, int64_t n, int32_t n_c
     p.cheb_mid = reinterpret_cast<const double*>(ws + L.cmid);
     p.cheb_half = reinterpret_cast<const double*>(ws + L.chalf);
     cudaStream_t st = as_stream(stream);
+    // chunk GEMMs: weighted x-sums of every table row (grid, ones, null) for all SNPs
+    const ChunkLayout CLy = chunk_layout(n, n_cvt, phi, n_grid, m);
+    JB_CHECK_ARG(chunk_workspace && chunk_bytes >= CLy.total, "jb_lmm_chunk: chunk workspace too small");
+    uint8_t* cws = static_cast<uint8_t*>(chunk_workspace);
+    double* X2 = reinterpret_cast<double*>(cws + CLy.x2);
+    double* CL = reinterpret_cast<double*>(cws + CLy.cl);
+    double* CQ = reinterpret_cast<double*>(cws + CLy.cq);
+    const int rows = n_grid + 1 + (lmm_mode == 1 ? 0 : phi);  // null rows only when prepared
+    const int rows_lin = rows * (n_cvt + phi);
+    square_cols_kernel<<<(unsigned)(ceil_div(n * m, 256) < 8192 ? ceil_div(n * m, 256) : 8192), 256, 0,
+                         st>>>(UtG, ldg, n, m, X2);
+    JB_LAUNCH_CHECK("square_cols_kernel");
+    {
+        cublasHandle_t h = cublas_handle();
+        if (!h) {
+            set_error("cuBLAS handle creation failed");
+            return JB_E_LIBRARY;
+        }
+        cublasStatus_t cs = cublasSetStream(h, st);
+        if (cs != CUBLAS_STATUS_SUCCESS) return cublas_status(cs, "cublasSetStream");
+        const double one = 1.0, zero = 0.0;
+        cs = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, rows_lin, (int)m, (int)n, &one,
+                         reinterpret_cast<const double*>(ws + L.alin), (int)n, UtG, (int)ldg, &zero,
+                         CL, rows_lin);
+        if (cs != CUBLAS_STATUS_SUCCESS) return cublas_status(cs, "cublasDgemm (linear x-sums)");
+        cs = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, rows, (int)m, (int)n, &one,
+                         reinterpret_cast<const double*>(ws + L.asq), (int)n, X2, (int)n, &zero, CQ,
+                         rows);
+        if (cs != CUBLAS_STATUS_SUCCESS) return cublas_status(cs, "cublasDgemm (square x-sums)");
+    }
+    p.CL = CL;
+    p.ldcl = rows_lin;
+    p.CQ = CQ;
+    p.ldcq = rows;
     switch (n_cvt) {
         case 1: return launch_pairs<1>(p, st);
         case 2: return launch_pairs<2>(p, st);

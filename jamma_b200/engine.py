@@ -118,6 +118,7 @@ class DeviceCohort:
             _native.call("jb_ozaki_prepare", ptr(self.U), n, n, ptr(self.ozaki), self.ozaki.numel(), st)
         self.code_ld = (n + 127) // 128 * 128 if precision == "mixed" else n
         self._rot_ws = None
+        self._chunk_ws = None
         # interpolated golden probes need log|1 + lambda*eval| to stay pole-free
         ev_min = float(self.evals.min().item())
         self.search = 1 if (precision == "mixed" and 1.0 + self.l_max * ev_min > 0.5) else 0
@@ -136,16 +137,24 @@ class DeviceCohort:
     def alloc_out(self, m: int) -> dict[str, torch.Tensor]:
         return {k: empty((self.phi, m)) for k in MODE_KEYS[self.mode]}
 
+    def chunk_workspace(self, m: int) -> torch.Tensor:
+        need = _native.load().jb_lmm_chunk_workspace_size(self.n, self.c, self.phi, self.n_grid, m)
+        if self._chunk_ws is None or self._chunk_ws.numel() < need:
+            self._chunk_ws = workspace(need)
+        return self._chunk_ws
+
     def associate_rotated(self, UtG: torch.Tensor, out: dict | None = None) -> dict:
         """Statistics for a rotated chunk UtG (m, n) column-major; outputs (phi, m)."""
         m = UtG.shape[0]
         out = out if out is not None else self.alloc_out(m)
         o = _native.LmmOut(**{k: ptr(out.get(k)) for k in OUT_KEYS})
+        cws = self.chunk_workspace(m)
         _native.call("jb_lmm_chunk", self.mode, self.search, self.n, self.c, self.phi, m,
                      ptr(self.evals),
                      ptr(self.UtW), self.n, ptr(self.Uty), self.n, ptr(UtG), self.n,
                      ptr(self.lam0), ptr(self.logl0), self.l_min, self.l_max, self.n_grid,
-                     self.n_iter, o, ptr(self.ws), self.ws.numel(), stream_handle())
+                     self.n_iter, o, ptr(self.ws), self.ws.numel(), ptr(cws), cws.numel(),
+                     stream_handle())
         return out
 
     def associate_genotypes(self, G: torch.Tensor, out: dict | None = None,

@@ -98,8 +98,10 @@ class _KinshipI8:
                      self.col, ptr(Cs), m, st)
         _native.call("jb_kinship_i8_corrections", ptr(codes), ld, ptr(Cs), m, self.n, m, ptr(mu64),
                      ptr(self.a), ptr(self.b), ptr(self.RT), self.n, st)
-        self.sum_mu2 += float(torch.sum(mu64 * mu64).item())
         self.col += m
+
+    def add_sum_mu2(self, mu64_host: np.ndarray) -> None:
+        self.sum_mu2 += float(np.sum(np.asarray(mu64_host, dtype=np.float64) ** 2))
 
     def finish(self) -> torch.Tensor:
         n = self.n
@@ -136,6 +138,7 @@ def _kinship_from_packed(packed_dev: torch.Tensor, n: int, batch_size: int, maf_
     if precision == "int8":
         acc = _KinshipI8(n, idx.size)
         acc.add(codes.index_select(0, sel), mu64, bool(np.any(c[:, 0] < n)))
+        acc.add_sum_mu2(c[:, 1] / np.maximum(c[:, 0], 1))
         return acc.finish(), idx.size
     acc = _KinshipAccumulator(n, max(1, min(batch_size, 8192)))
     acc.add(codes.index_select(0, sel), mu64)
@@ -195,6 +198,7 @@ def compute_kinship_from_bed(bfile, maf_threshold: float = 0.0, miss_threshold: 
         mu64 = torch.from_numpy(c[:, 1] / np.maximum(c[:, 0], 1)).to("cuda")
         if i8:
             acc.add(codes, mu64, bool(np.any(c[:, 0] < n)))
+            acc.add_sum_mu2(c[:, 1] / np.maximum(c[:, 0], 1))
         else:
             acc.add(codes, mu64)
     K = acc.finish()
