@@ -110,6 +110,22 @@ int64_t jb_gram_i8_workspace_size(int64_t n);
 int32_t jb_gram_i8(const int8_t* Zs, int64_t n, int64_t p, int64_t ldz, int32_t* C,
                    int64_t ldc, void* workspace, int64_t workspace_bytes, uintptr_t stream);
 int32_t jb_gram_status(const void* workspace, int32_t* out, uintptr_t stream);
+
+/*
+ * jb_gram_i8_noalloc: the same exact INT8 Gram as jb_gram_i8, for callers that cannot
+ * allocate device memory -- e.g. a host application whose memory pool already owns the
+ * GPU's free HBM, or code that must not trigger the implicit device synchronisation of
+ * cudaMalloc.  It takes no workspace: its scratch (pipeline status word and tile
+ * schedule) lives in a 1 MiB static device array inside this library, which every GPU
+ * that loads the library keeps until the process exits; n <= 65408 fits, larger n is
+ * rejected with JB_E_INVALID and a message.  The first call on a device looks up that
+ * array's device address (cudaGetSymbolAddress), so make it before any stream capture.
+ * Every call reuses the one array (the status word is cleared on each call), so calls
+ * that overlap on the GPU -- on different streams, or from different host threads --
+ * race: serialise them.  No counterpart in the jamma reference.
+ */
+int32_t jb_gram_i8_noalloc(const int8_t* Zs, int64_t n, int64_t p, int64_t ldz, int32_t* C,
+                           int64_t ldc, uintptr_t stream);
 int32_t jb_codes_to_sample_major(const int8_t* codes, int64_t ld_codes, int64_t n,
                                  int64_t m, int8_t* Zs, int64_t ldz, int64_t col0,
                                  int8_t* Cs, int64_t ldcs, uintptr_t stream);

@@ -64,6 +64,7 @@ SIGNATURES: dict[str, tuple] = {
     "jb_gram_i8_workspace_size": (_i64, [_i64]),
     "jb_gram_i8": (_i32, [_p, _i64, _i64, _i64, _p, _i64, _p, _i64, _u]),
     "jb_gram_status": (_i32, [_p, _p, _u]),
+    "jb_gram_i8_noalloc": (_i32, [_p, _i64, _i64, _i64, _p, _i64, _u]),
     "jb_codes_to_sample_major": (_i32, [_p, _i64, _i64, _i64, _p, _i64, _i64, _p, _i64, _u]),
     "jb_kinship_i8_corrections": (_i32, [_p, _i64, _p, _i64, _i64, _i64, _p, _p, _p, _p, _i64, _u]),
     "jb_kinship_i8_finalize": (_i32, [_p, _i64, _i64, _p, _p, _f64, _p, _i64, _i64, _p, _i64, _u]),

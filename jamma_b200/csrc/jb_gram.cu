@@ -269,6 +269,34 @@ GramWs gram_ws(int64_t n) {
     w.total = w.tiles + ((MB * NB * (int64_t)sizeof(Tile) + 255) / 256) * 256;
     return w;
 }
+// Scratch for jb_gram_i8_noalloc: one file-scope device array, 1 MiB, present on every
+// GPU that loads this library until the process exits.  Host code cannot use the symbol
+// itself as a device address; its address on each device is looked up once with
+// cudaGetSymbolAddress while that device is current.
+constexpr int64_t kNoAllocScratchBytes = 1 << 20;
+static __device__ __align__(256) unsigned char g_gram_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {nullptr};
+
+int32_t noalloc_scratch(void** out) {
+    int dev = 0;
+    JB_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) {
+        set_error("jb_gram_i8_noalloc: device ordinal %d out of range", dev);
+        return JB_E_UNSUPPORTED;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_gram_noalloc_scratch);
+        if (e != cudaSuccess) return cuda_status(e, "cudaGetSymbolAddress(gram scratch)");
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return JB_OK;
+}
 }  // namespace
 
 extern "C" {
@@ -308,6 +336,20 @@ int32_t jb_gram_i8(const int8_t* Z, int64_t n, int64_t p, int64_t ldz, int32_t* 
     kern<<<grid, kThreads, GramSmem::TOTAL, st>>>(ta, tb, tiles, n_tiles, num_kb, epi, status);
     JB_LAUNCH_CHECK("i8_gemm_kernel<gram>");
     return JB_OK;
+}
+
+int32_t jb_gram_i8_noalloc(const int8_t* Zs, int64_t n, int64_t p, int64_t ldz, int32_t* C,
+                           int64_t ldc, uintptr_t stream) {
+    JB_CHECK_ARG(n > 0, "jb_gram_i8_noalloc: bad shape");
+    const int64_t need = gram_ws(n).total;
+    JB_CHECK_ARG(need <= kNoAllocScratchBytes,
+                 "jb_gram_i8_noalloc: n = %lld needs %lld bytes of scratch, more than the "
+                 "library's static %lld bytes (n <= 65408); use jb_gram_i8 with a workspace",
+                 (long long)n, (long long)need, (long long)kNoAllocScratchBytes);
+    void* scratch = nullptr;
+    const int32_t rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    return jb_gram_i8(Zs, n, p, ldz, C, ldc, scratch, kNoAllocScratchBytes, stream);
 }
 
 int32_t jb_gram_status(const void* workspace, int32_t* out, uintptr_t stream) {
