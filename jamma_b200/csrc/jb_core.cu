@@ -63,7 +63,8 @@ cusolverDnHandle_t cusolver_handle() {
 // ---------------------------------------------------------------- kernels
 
 // One CTA per SNP: decode the analysed samples, write int8 codes (3 = missing, zero
-// padding up to ld), and reduce {n_obs, sum, n_het, n_hom2}.
+// padding up to ld), and reduce {n_obs, sum, n_het, n_hom2}.  Without a sample subset
+// each thread decodes one packed byte (4 samples) and stores them as one 32-bit word.
 __global__ void decode_bed_kernel(const uint8_t* __restrict__ packed, int64_t bps, int64_t m,
                                   const int32_t* __restrict__ sidx, int64_t n,
                                   int8_t* __restrict__ codes, int64_t ld,
@@ -73,21 +74,45 @@ __global__ void decode_bed_kernel(const uint8_t* __restrict__ packed, int64_t bp
     const uint8_t* rec = packed + j * bps;
     int8_t* out = codes + j * ld;
     int obs = 0, sum = 0, het = 0, hom2 = 0;
-    for (int64_t s = threadIdx.x; s < ld; s += blockDim.x) {
-        int8_t v = 0;
-        if (s < n) {
-            const int64_t fi = sidx ? (int64_t)sidx[s] : s;
-            const int code = (rec[fi >> 2] >> (2 * (fi & 3))) & 3;
-            // count-A1: 00 -> 2, 01 -> missing, 10 -> 1, 11 -> 0
-            v = (int8_t)(code == 0 ? 2 : (code == 1 ? 3 : (code == 2 ? 1 : 0)));
-            if (v != 3) {
-                obs += 1;
-                sum += v;
-                het += (v == 1);
-                hom2 += (v == 2);
+    // count-A1: 00 -> 2, 01 -> missing (3), 10 -> 1, 11 -> 0
+    auto code_of = [](int c) { return c == 0 ? 2 : (c == 1 ? 3 : (c == 2 ? 1 : 0)); };
+    if (!sidx && (ld & 3) == 0) {
+        for (int64_t q = threadIdx.x; q < ld / 4; q += blockDim.x) {
+            const int64_t s0 = 4 * q;
+            uint32_t word = 0;
+            if (s0 < n) {
+                const int byte = rec[q];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    if (s0 + e < n) {
+                        const int v = code_of((byte >> (2 * e)) & 3);
+                        word |= (uint32_t)v << (8 * e);
+                        if (v != 3) {
+                            obs += 1;
+                            sum += v;
+                            het += (v == 1);
+                            hom2 += (v == 2);
+                        }
+                    }
+                }
             }
+            *reinterpret_cast<uint32_t*>(out + s0) = word;
         }
-        out[s] = v;
+    } else {
+        for (int64_t s = threadIdx.x; s < ld; s += blockDim.x) {
+            int8_t v = 0;
+            if (s < n) {
+                const int64_t fi = sidx ? (int64_t)sidx[s] : s;
+                v = (int8_t)code_of((rec[fi >> 2] >> (2 * (fi & 3))) & 3);
+                if (v != 3) {
+                    obs += 1;
+                    sum += v;
+                    het += (v == 1);
+                    hom2 += (v == 2);
+                }
+            }
+            out[s] = v;
+        }
     }
     __shared__ int red[4][32];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;

@@ -79,15 +79,30 @@ __global__ void rot_pack_pairs_kernel(const int8_t* __restrict__ codes, int64_t 
     const int64_t j = blockIdx.x;
     const int64_t rz = (j / 128) * 256 + (j % 128);
     const int64_t rm = rz + 128;
-    for (int64_t k = threadIdx.x; k < ldb; k += blockDim.x) {
-        int8_t z = 0, mk = 0;
-        if (j < m && k < n) {
-            const int8_t c = codes[j * ldc + k];
-            z = (c == 3) ? 0 : c;
-            mk = (c == 3);
+    const bool vec = ((ldc & 3) == 0) && ((ldb & 3) == 0);
+    for (int64_t k = 4 * (int64_t)threadIdx.x; k < ldb; k += 4 * (int64_t)blockDim.x) {
+        uint32_t c4 = 0;
+        if (j < m) {
+            if (vec && k + 4 <= n) {
+                c4 = *reinterpret_cast<const uint32_t*>(codes + j * ldc + k);
+            } else {
+                for (int q = 0; q < 4; ++q)
+                    if (k + q < n) c4 |= (uint32_t)(uint8_t)codes[j * ldc + k + q] << (8 * q);
+            }
         }
-        B[rz * ldb + k] = z;
-        B[rm * ldb + k] = mk;
+        // per byte: code 3 (missing) -> call 0, mask 1; else call = code, mask 0
+        const uint32_t lo = c4 & 0x01010101u, hi = (c4 >> 1) & 0x01010101u;
+        const uint32_t mk = lo & hi;
+        const uint32_t z = c4 & ~(mk * 3u);
+        if (vec) {
+            *reinterpret_cast<uint32_t*>(B + rz * ldb + k) = z;
+            *reinterpret_cast<uint32_t*>(B + rm * ldb + k) = mk;
+        } else {
+            for (int q = 0; q < 4 && k + q < ldb; ++q) {
+                B[rz * ldb + k + q] = (int8_t)((z >> (8 * q)) & 0xff);
+                B[rm * ldb + k + q] = (int8_t)((mk >> (8 * q)) & 0xff);
+            }
+        }
     }
 }
 
@@ -145,15 +160,19 @@ struct RotEpi {
     }
 };
 
-// Tiles over (eigenvector blocks of 32, SNP blocks) in groups of GM x GN.
+// Tiles over (eigenvector blocks of 32, SNP blocks) in groups of GM x GN (GN SNP blocks
+// per group column, groups visited column by column), one thread per tile: tile (mb, nb)
+// sits at its closed-form position in that order.
 __global__ void rot_tiles_kernel(int MB, int NB, Tile* out) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const int GM = 9, GN = 16;
-    int k = 0;
-    for (int gn = 0; gn < NB; gn += GN)
-        for (int gm = 0; gm < MB; gm += GM)
-            for (int mb = gm; mb < MB && mb < gm + GM; ++mb)
-                for (int nb = gn; nb < NB && nb < gn + GN; ++nb) out[k++] = Tile{mb, nb};
+    constexpr int GM = 9, GN = 16;
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (int64_t)MB * NB) return;
+    const int mb = (int)(t / NB), nb = (int)(t % NB);
+    const int gc = nb / GN, gr = mb / GM;
+    const int w = NB - gc * GN < GN ? NB - gc * GN : GN;  // width of this group column
+    const int64_t k = (int64_t)MB * GN * gc + (int64_t)gr * GM * w + (int64_t)(mb - gr * GM) * w +
+                      (nb - gc * GN);
+    out[k] = Tile{mb, nb};
 }
 
 }  // namespace tc
@@ -261,7 +280,7 @@ int32_t jb_rotate_i8(const void* ozaki_ws, int64_t n, const int8_t* codes, int64
     }
     if (rc) return rc;
     JB_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
-    rot_tiles_kernel<<<1, 32, 0, st>>>(MB, NB, tiles);
+    rot_tiles_kernel<<<(unsigned)ceil_div((int64_t)n_tiles, 256), 256, 0, st>>>(MB, NB, tiles);
     JB_LAUNCH_CHECK("rot_tiles_kernel");
     const int grid = n_tiles < num_sms() ? n_tiles : num_sms();
     const int num_kb = (int)ceil_div(n, kBK);
