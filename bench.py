@@ -206,12 +206,12 @@ def run_ours(args) -> None:
         acc = _KinshipI8(n, keep.size) if form == "int8" else _KinshipAccumulator(n, 4096)
         for s in range(0, keep.size, kc):
             sub = keep[s:s + kc]
-            codes_k, _ = eng.decode_packed(kin_rec.index_select(0, torch.from_numpy(sub).cuda()),
-                                           n, None, n)
+            rec_k = kin_rec.index_select(0, torch.from_numpy(sub).cuda())
+            codes_k, _ = eng.decode_packed(rec_k, n, None, n)
             cc = kin_counts[sub]
             mu = torch.from_numpy(cc[:, 1] / np.maximum(cc[:, 0], 1)).cuda()
             if form == "int8":
-                acc.add(codes_k, mu, bool(np.any(cc[:, 0] < n)))
+                acc.add(codes_k, mu, bool(np.any(cc[:, 0] < n)), rec_k)
                 acc.add_sum_mu2(cc[:, 1] / np.maximum(cc[:, 0], 1))
             else:
                 acc.add(codes_k, mu)

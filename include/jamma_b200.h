@@ -59,6 +59,10 @@ int32_t jb_decode_bed(const uint8_t* packed, int64_t bytes_per_snp, int64_t m,
                       const int32_t* sample_idx, int64_t n, int8_t* codes,
                       int64_t ld_codes, int32_t* counts, uintptr_t stream);
 
+/* Re-pack decoded codes (m x ld_codes) into count-A1 .bed records (m x bytes_per_snp). */
+int32_t jb_pack_codes(const int8_t* codes, int64_t ld_codes, int64_t n, int64_t m,
+                      uint8_t* packed, int64_t bytes_per_snp, uintptr_t stream);
+
 /*
  * Mean-impute (no centering) decoded codes into FP64 genotype columns:
  * G[i + j*ldg] = code (0/1/2) or mean[j] where the code is 3 (missing).
@@ -103,7 +107,9 @@ int32_t jb_kinship_finalize(double* K, int64_t n, int64_t ldk, double scale,
  *   its first int32 is a status word (non-zero if a pipeline wait timed out), read with
  *   jb_gram_status (synchronises the stream).
  * jb_kinship_i8_corrections: accumulate a, b (n doubles each) and, when Cs is given
- *   (the chunk has missing calls), R and T into RT (column-major n x 2n, ld ldr).
+ *   (the chunk has missing calls), Q = R + T/2 into RT (column-major n x n, ld ldr;
+ *   T is symmetric, so R + R^T + T = Q + Q^T); the missing-call terms read the chunk's
+ *   packed .bed records (m x bytes_per_snp, all n samples, same SNP order as codes).
  * jb_kinship_i8_finalize: K (n x n, ldk) = symmetric combination above / p_kept.
  */
 int64_t jb_gram_i8_workspace_size(int64_t n);
@@ -129,14 +135,32 @@ int32_t jb_gram_i8_noalloc(const int8_t* Zs, int64_t n, int64_t p, int64_t ldz, 
 int32_t jb_codes_to_sample_major(const int8_t* codes, int64_t ld_codes, int64_t n,
                                  int64_t m, int8_t* Zs, int64_t ldz, int64_t col0,
                                  int8_t* Cs, int64_t ldcs, uintptr_t stream);
-int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes, const int8_t* Cs,
-                                  int64_t ldcs, int64_t n, int64_t m, const double* mu,
-                                  double* a, double* b, double* RT, int64_t ldr,
-                                  uintptr_t stream);
+int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes,
+                                  const uint8_t* packed, int64_t bytes_per_snp,
+                                  const int8_t* Cs, int64_t ldcs, int64_t n, int64_t m,
+                                  const double* mu, double* a, double* b, double* RT,
+                                  int64_t ldr, uintptr_t stream);
 int32_t jb_kinship_i8_finalize(const int32_t* C, int64_t ldc, int64_t n, const double* a,
                                const double* b, double sum_mu2, const double* RT,
                                int64_t ldr, int64_t p_kept, double* K, int64_t ldk,
                                uintptr_t stream);
+
+/*
+ * Leave-one-chromosome-out kinship (compute_loco_kinship_streaming,
+ * src/jamma/kinship/compute.py:693-916): K_loco = (S_full - S_chr) / p_loco.
+ * jb_kinship_i8_finalize_loco: from the full-genome and one chromosome's int32 Grams
+ *   (exact integer difference), correction vectors a, b, Q (Q pair may be NULL when no
+ *   call is missing) and sum_mu2_loco = sum over the kept non-chromosome SNPs of mu^2.
+ * jb_kinship_loco_f64: plain FP64 form from the lower triangles of two centred Grams.
+ */
+int32_t jb_kinship_i8_finalize_loco(const int32_t* C_full, const int32_t* C_chr, int64_t ldc,
+                                    int64_t n, const double* a_full, const double* a_chr,
+                                    const double* b_full, const double* b_chr,
+                                    double sum_mu2_loco, const double* Q_full,
+                                    const double* Q_chr, int64_t ldq, int64_t p_loco,
+                                    double* K, int64_t ldk, uintptr_t stream);
+int32_t jb_kinship_loco_f64(const double* S_full, const double* S_chr, int64_t n, int64_t lds,
+                            int64_t p_loco, double* K, int64_t ldk, uintptr_t stream);
 
 /* ------------------------------------------------------------------ eigen */
 

@@ -44,6 +44,7 @@ SIGNATURES: dict[str, tuple] = {
     "jb_device_arch": (_i32, []),
     "jb_decode_bed": (_i32, [_p, _i64, _i64, _p, _i64, _p, _i64, _p, _u]),
     "jb_impute_f64": (_i32, [_p, _i64, _i64, _i64, _p, _p, _i64, _u]),
+    "jb_pack_codes": (_i32, [_p, _i64, _i64, _i64, _p, _i64, _u]),
     "jb_kinship_f64_workspace_size": (_i64, [_i64, _i64]),
     "jb_kinship_accumulate_f64": (_i32, [_p, _i64, _i64, _i64, _p, _p, _i64, _p, _i64, _u]),
     "jb_kinship_finalize": (_i32, [_p, _i64, _i64, _f64, _u]),
@@ -65,8 +66,12 @@ SIGNATURES: dict[str, tuple] = {
     "jb_gram_i8": (_i32, [_p, _i64, _i64, _i64, _p, _i64, _p, _i64, _u]),
     "jb_gram_status": (_i32, [_p, _p, _u]),
     "jb_gram_i8_noalloc": (_i32, [_p, _i64, _i64, _i64, _p, _i64, _u]),
+    "jb_kinship_i8_finalize_loco": (
+        _i32, [_p, _p, _i64, _i64, _p, _p, _p, _p, _f64, _p, _p, _i64, _i64, _p, _i64, _u]),
+    "jb_kinship_loco_f64": (_i32, [_p, _p, _i64, _i64, _i64, _p, _i64, _u]),
     "jb_codes_to_sample_major": (_i32, [_p, _i64, _i64, _i64, _p, _i64, _i64, _p, _i64, _u]),
-    "jb_kinship_i8_corrections": (_i32, [_p, _i64, _p, _i64, _i64, _i64, _p, _p, _p, _p, _i64, _u]),
+    "jb_kinship_i8_corrections": (
+        _i32, [_p, _i64, _p, _i64, _p, _i64, _i64, _i64, _p, _p, _p, _p, _i64, _u]),
     "jb_kinship_i8_finalize": (_i32, [_p, _i64, _i64, _p, _p, _f64, _p, _i64, _i64, _p, _i64, _u]),
     "jb_ozaki_workspace_size": (_i64, [_i64]),
     "jb_ozaki_prepare": (_i32, [_p, _i64, _i64, _p, _i64, _u]),

@@ -136,6 +136,28 @@ __global__ void decode_bed_kernel(const uint8_t* __restrict__ packed, int64_t bp
     }
 }
 
+// Inverse of the decode: int8 codes (0/1/2, 3 = missing) -> count-A1 2-bit records,
+// samples past n padded with "0 copies" (11).
+__global__ void pack_codes_kernel(const int8_t* __restrict__ codes, int64_t ldc, int64_t n,
+                                  int64_t m, uint8_t* __restrict__ packed, int64_t bps) {
+    const int64_t j = blockIdx.x;
+    if (j >= m) return;
+    for (int64_t q = threadIdx.x; q < bps; q += blockDim.x) {
+        uint32_t byte = 0;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const int64_t s = 4 * q + e;
+            uint32_t bits = 3u;
+            if (s < n) {
+                const int8_t v = codes[j * ldc + s];
+                bits = v == 2 ? 0u : (v == 3 ? 1u : (v == 1 ? 2u : 3u));
+            }
+            byte |= bits << (2 * e);
+        }
+        packed[j * bps + q] = (uint8_t)byte;
+    }
+}
+
 __global__ void impute_f64_kernel(const int8_t* __restrict__ codes, int64_t ldc, int64_t n,
                                   int64_t m, const double* __restrict__ mean,
                                   double* __restrict__ G, int64_t ldg) {
@@ -225,6 +247,18 @@ int32_t jb_decode_bed(const uint8_t* packed, int64_t bytes_per_snp, int64_t m,
                                                                  sample_idx, n, codes,
                                                                  ld_codes, counts);
     JB_LAUNCH_CHECK("decode_bed_kernel");
+    return JB_OK;
+}
+
+int32_t jb_pack_codes(const int8_t* codes, int64_t ld_codes, int64_t n, int64_t m,
+                      uint8_t* packed, int64_t bytes_per_snp, uintptr_t stream) {
+    JB_CHECK_ARG(n >= 0 && m >= 0 && ld_codes >= n && 4 * bytes_per_snp >= n,
+                 "jb_pack_codes: bad shape");
+    if (m == 0) return JB_OK;
+    JB_CHECK_ARG(m < (1ll << 31), "jb_pack_codes: too many SNPs");
+    pack_codes_kernel<<<(unsigned)m, 128, 0, as_stream(stream)>>>(codes, ld_codes, n, m, packed,
+                                                                 bytes_per_snp);
+    JB_LAUNCH_CHECK("pack_codes_kernel");
     return JB_OK;
 }
 

@@ -10,8 +10,9 @@
 //   p K = Z Z^T - a 1^T - 1 a^T + (sum mu^2) 1 1^T - b 1^T - 1 b^T + R + R^T + T
 //   a = Z mu,  b = M mu^2,  R = Z diag(mu) M^T,  T = M diag(mu^2) M^T
 //
-// The dense Z Z^T runs on tcgen05 (kind::i8); the vectors and the sparse R, T terms are
-// FP64 on the CUDA cores.
+// T is symmetric, so R + R^T + T = Q + Q^T with Q = R + T/2: one n x n buffer holds both
+// sparse terms.  The dense Z Z^T runs on tcgen05 (kind::i8); the vectors and Q are FP64
+// on the CUDA cores.
 #include "jb_common.cuh"
 #include "jb_gemm_i8.cuh"
 
@@ -168,23 +169,24 @@ __global__ void kin_vectors_kernel(const int8_t* __restrict__ codes, int64_t ldc
 }
 
 // Sparse terms for one SNP chunk.  For every sample k and every SNP j of the chunk that
-// is missing at k: R[:, k] += mu_j Z[:, j] and T[:, k] += mu_j^2 M[:, j].  One CTA per
-// (k, block of 2048 samples i); each thread owns 8 consecutive samples (one 8-byte load
-// per missing SNP) and keeps their R and T sums in registers.
-__global__ void __launch_bounds__(256) kin_sparse_kernel(const int8_t* __restrict__ codes,
-                                                          int64_t ldc, const int8_t* __restrict__ Cs,
+// is missing at k: Q[:, k] += mu_j Z[:, j] + (mu_j^2 / 2) M[:, j]  (Q = R + T/2).  The
+// SNP columns are read from the 2-bit packed .bed records (4x less traffic than int8
+// codes).  One CTA per (k, block of 4096 samples i); each thread owns 16 consecutive
+// samples (one 32-bit packed load per missing SNP) and keeps their sums in registers.
+__global__ void __launch_bounds__(256) kin_sparse_kernel(const uint8_t* __restrict__ packed,
+                                                          int64_t bps, const int8_t* __restrict__ Cs,
                                                           int64_t ldcs, int64_t n, int64_t m,
                                                           const double* __restrict__ mu,
-                                                          double* __restrict__ RT,
-                                                          int64_t ldr) {
+                                                          double* __restrict__ Q, int64_t ldq) {
     const int64_t k = blockIdx.x;
-    const int64_t i0 = (int64_t)blockIdx.y * 2048 + 8 * threadIdx.x;
+    const int64_t i0 = (int64_t)blockIdx.y * 4096 + 16 * threadIdx.x;
     __shared__ int32_t list[2048];
     __shared__ int cnt;
-    double r[8], tt[8];
+    double r[16], tt[16];
 #pragma unroll
-    for (int e = 0; e < 8; ++e) r[e] = tt[e] = 0.0;
-    const bool full8 = (i0 + 8 <= n) && ((ldc & 7) == 0);
+    for (int e = 0; e < 16; ++e) r[e] = tt[e] = 0.0;
+    const int64_t b0 = i0 >> 2;  // first packed byte of this thread's 16 samples
+    const bool full = (i0 + 16 <= n) && ((bps & 3) == 0);
     for (int64_t jb = 0; jb < m; jb += 2048) {
         if (threadIdx.x == 0) cnt = 0;
         __syncthreads();
@@ -193,44 +195,41 @@ __global__ void __launch_bounds__(256) kin_sparse_kernel(const int8_t* __restric
         }
         __syncthreads();
         const int c = cnt;
-        for (int e = 0; e < c; ++e) {
-            const int64_t j = list[e];
-            const double u = mu[j];
-            const double u2 = u * u;
-            int8_t v[8];
-            if (full8) {
-                const uint2 w = *reinterpret_cast<const uint2*>(codes + j * ldc + i0);
-                const uint32_t lo = w.x, hi = w.y;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    v[q] = (int8_t)((lo >> (8 * q)) & 0xff);
-                    v[4 + q] = (int8_t)((hi >> (8 * q)) & 0xff);
+        if (i0 < n) {
+            for (int e = 0; e < c; ++e) {
+                const int64_t j = list[e];
+                const double u = mu[j];
+                const double u2h = 0.5 * u * u;
+                const uint8_t* rec = packed + j * bps;
+                uint32_t w;
+                if (full) {
+                    w = *reinterpret_cast<const uint32_t*>(rec + b0);
+                } else {
+                    w = 0xffffffffu;  // padding decodes as 0 copies
+                    for (int q = 0; q < 4; ++q)
+                        if (b0 + q < bps) w = (w & ~(0xffu << (8 * q))) | ((uint32_t)rec[b0 + q] << (8 * q));
                 }
-            } else {
 #pragma unroll
-                for (int q = 0; q < 8; ++q) v[q] = (i0 + q < n) ? codes[j * ldc + i0 + q] : (int8_t)0;
-            }
-#pragma unroll
-            for (int q = 0; q < 8; ++q) {
-                if (v[q] == 3)
-                    tt[q] += u2;
-                else
-                    r[q] = fma((double)v[q], u, r[q]);
+                for (int q = 0; q < 16; ++q) {
+                    // count-A1 codes: 00 -> 2, 01 -> missing, 10 -> 1, 11 -> 0
+                    const uint32_t code = (w >> (2 * q)) & 3u;
+                    if (code == 1u)
+                        tt[q] += u2h;
+                    else
+                        r[q] += (code == 0u) ? 2.0 * u : (code == 2u ? u : 0.0);
+                }
             }
         }
         __syncthreads();
     }
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < 16; ++q) {
         const int64_t i = i0 + q;
-        if (i < n) {
-            RT[k * ldr + i] += r[q];            // R[i, k] (column-major, column k)
-            RT[(n + k) * ldr + i] += tt[q];     // T[i, k]
-        }
+        if (i < n) Q[k * ldq + i] += r[q] + tt[q];  // Q[i, k] (column-major, column k)
     }
 }
 
-// K = (C - a_i - a_j + s - b_i - b_j + R_ij + R_ji + T_ij) / p, symmetric, column-major.
+// K = (C - a_i - a_j + s - b_i - b_j + Q_ij + Q_ji) / p, symmetric, column-major.
 __global__ void kin_finalize_i8_kernel(const int32_t* __restrict__ C, int64_t ldc, int64_t n,
                                        const double* __restrict__ a, const double* __restrict__ b,
                                        double s, const double* __restrict__ RT, int64_t ldr,
@@ -240,10 +239,49 @@ __global__ void kin_finalize_i8_kernel(const int32_t* __restrict__ C, int64_t ld
          i += (int64_t)gridDim.x * blockDim.x) {
         // the int32 Gram holds the upper triangle (row i <= column j) at C[j*ldc + i]
         double v = (double)C[j * ldc + i] - a[i] - a[j] + s - b[i] - b[j];
-        if (RT) v += RT[j * ldr + i] + RT[i * ldr + j] + RT[(n + j) * ldr + i];
+        if (RT) v += RT[j * ldr + i] + RT[i * ldr + j];
         v *= inv_p;
         K[j * ldk + i] = v;
         K[i * ldk + j] = v;
+    }
+}
+
+// Leave-one-chromosome-out: every term of p K is a sum over SNPs, so the kinship without
+// chromosome c is the full-genome combination minus chromosome c's, over p - p_c SNPs.
+// The int32 Grams subtract exactly.
+__global__ void kin_finalize_loco_kernel(const int32_t* __restrict__ Cf, const int32_t* __restrict__ Cc,
+                                         int64_t ldc, int64_t n, const double* __restrict__ af,
+                                         const double* __restrict__ ac, const double* __restrict__ bf,
+                                         const double* __restrict__ bc, double s,
+                                         const double* __restrict__ Qf,
+                                         const double* __restrict__ Qc, int64_t ldq, double inv_p,
+                                         double* __restrict__ K, int64_t ldk) {
+    const int64_t j = blockIdx.y;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= j && i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int32_t g = Cf[j * ldc + i] - Cc[j * ldc + i];
+        const double ai = af[i] - ac[i], aj = af[j] - ac[j];
+        const double bi = bf[i] - bc[i], bj = bf[j] - bc[j];
+        double v = (double)g - ai - aj + s - bi - bj;
+        if (Qf) v += (Qf[j * ldq + i] + Qf[i * ldq + j]) - (Qc[j * ldq + i] + Qc[i * ldq + j]);
+        v *= inv_p;
+        K[j * ldk + i] = v;
+        K[i * ldk + j] = v;
+    }
+}
+
+// Plain FP64 form: K = (S_full - S_c) * scale from lower triangles, written symmetric.
+__global__ void kin_sub_scale_kernel(const double* __restrict__ Sf, const double* __restrict__ Sc,
+                                     int64_t n, int64_t lds, double scale, double* __restrict__ K,
+                                     int64_t ldk) {
+    const int64_t j = blockIdx.y;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        if (i >= j) {
+            const double v = (Sf[j * lds + i] - Sc[j * lds + i]) * scale;
+            K[j * ldk + i] = v;
+            K[i * ldk + j] = v;
+        }
     }
 }
 
@@ -338,6 +376,34 @@ int32_t jb_gram_i8(const int8_t* Z, int64_t n, int64_t p, int64_t ldz, int32_t* 
     return JB_OK;
 }
 
+int32_t jb_kinship_i8_finalize_loco(const int32_t* C_full, const int32_t* C_chr, int64_t ldc,
+                                    int64_t n, const double* a_full, const double* a_chr,
+                                    const double* b_full, const double* b_chr, double sum_mu2_loco,
+                                    const double* Q_full, const double* Q_chr, int64_t ldq,
+                                    int64_t p_loco, double* K, int64_t ldk, uintptr_t stream) {
+    JB_CHECK_ARG(n > 0 && ldc >= n && ldk >= n && p_loco > 0, "jb_kinship_i8_finalize_loco: bad shape");
+    JB_CHECK_ARG((Q_full == nullptr) == (Q_chr == nullptr) && (!Q_full || ldq >= n),
+                 "jb_kinship_i8_finalize_loco: Q_full and Q_chr go together");
+    JB_CHECK_ARG(n < 65536 * 4, "jb_kinship_i8_finalize_loco: n too large");
+    dim3 grid((unsigned)(ceil_div(n, 256) < 64 ? ceil_div(n, 256) : 64), (unsigned)n, 1);
+    kin_finalize_loco_kernel<<<grid, 256, 0, as_stream(stream)>>>(
+        C_full, C_chr, ldc, n, a_full, a_chr, b_full, b_chr, sum_mu2_loco, Q_full, Q_chr, ldq,
+        1.0 / (double)p_loco, K, ldk);
+    JB_LAUNCH_CHECK("kin_finalize_loco_kernel");
+    return JB_OK;
+}
+
+int32_t jb_kinship_loco_f64(const double* S_full, const double* S_chr, int64_t n, int64_t lds,
+                            int64_t p_loco, double* K, int64_t ldk, uintptr_t stream) {
+    JB_CHECK_ARG(n > 0 && lds >= n && ldk >= n && p_loco > 0, "jb_kinship_loco_f64: bad shape");
+    JB_CHECK_ARG(n < 65536 * 4, "jb_kinship_loco_f64: n too large");
+    dim3 grid((unsigned)(ceil_div(n, 256) < 64 ? ceil_div(n, 256) : 64), (unsigned)n, 1);
+    kin_sub_scale_kernel<<<grid, 256, 0, as_stream(stream)>>>(S_full, S_chr, n, lds,
+                                                             1.0 / (double)p_loco, K, ldk);
+    JB_LAUNCH_CHECK("kin_sub_scale_kernel");
+    return JB_OK;
+}
+
 int32_t jb_gram_i8_noalloc(const int8_t* Zs, int64_t n, int64_t p, int64_t ldz, int32_t* C,
                            int64_t ldc, uintptr_t stream) {
     JB_CHECK_ARG(n > 0, "jb_gram_i8_noalloc: bad shape");
@@ -376,9 +442,10 @@ int32_t jb_codes_to_sample_major(const int8_t* codes, int64_t ld_codes, int64_t 
     return JB_OK;
 }
 
-int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes, const int8_t* Cs,
-                                  int64_t ldcs, int64_t n, int64_t m, const double* mu, double* a,
-                                  double* b, double* RT, int64_t ldr, uintptr_t stream) {
+int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes, const uint8_t* packed,
+                                  int64_t bytes_per_snp, const int8_t* Cs, int64_t ldcs, int64_t n,
+                                  int64_t m, const double* mu, double* a, double* b, double* RT,
+                                  int64_t ldr, uintptr_t stream) {
     JB_CHECK_ARG(n > 0 && m >= 0 && ld_codes >= n, "jb_kinship_i8_corrections: bad shape");
     if (m == 0) return JB_OK;
     cudaStream_t st = as_stream(stream);
@@ -387,10 +454,10 @@ int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes, const i
         codes, ld_codes, n, m, mu, a, b);
     JB_LAUNCH_CHECK("kin_vectors_kernel");
     if (Cs) {
-        JB_CHECK_ARG(RT && ldr >= n && ldcs >= m, "jb_kinship_i8_corrections: RT buffer needed");
-        JB_CHECK_ARG(ceil_div(n, 2048) < 65536, "jb_kinship_i8_corrections: n too large");
-        dim3 grid((unsigned)n, (unsigned)ceil_div(n, 2048), 1);
-        kin_sparse_kernel<<<grid, 256, 0, st>>>(codes, ld_codes, Cs, ldcs, n, m, mu, RT, ldr);
+        JB_CHECK_ARG(RT && ldr >= n && ldcs >= m && packed && 4 * bytes_per_snp >= n,
+                     "jb_kinship_i8_corrections: Q buffer and packed records needed");
+        dim3 grid((unsigned)n, (unsigned)ceil_div(n, 4096), 1);
+        kin_sparse_kernel<<<grid, 256, 0, st>>>(packed, bytes_per_snp, Cs, ldcs, n, m, mu, RT, ldr);
         JB_LAUNCH_CHECK("kin_sparse_kernel");
     }
     return JB_OK;

@@ -49,8 +49,6 @@ def gwas(bfile, *, kinship_file=None, covariate_file=None, lmm_mode: int = 1, ma
         raise ValueError("kinship_file and loco are mutually exclusive")
     if (eigenvalue_file is None) != (eigenvector_file is None):
         raise ValueError("eigenvalue_file and eigenvector_file must be provided together")
-    if loco:
-        raise NotImplementedError("LOCO association is not available in this build")
     t0 = time.perf_counter()
     bfile = Path(bfile)
     meta = get_plink_metadata(bfile)
@@ -61,8 +59,15 @@ def gwas(bfile, *, kinship_file=None, covariate_file=None, lmm_mode: int = 1, ma
     snps_idx = None
     if snps_file is not None:
         snps_idx = np.array(sorted(pos[s] for s in _read_snp_list(snps_file) if s in pos), dtype=np.int64)
+    cov = None
+    if covariate_file is not None:
+        cov, _ = read_covariate_file(covariate_file)
+        if cov.shape[0] != n:
+            raise ValueError(f"Covariate file has {cov.shape[0]} rows but .fam has {n} samples")
     evals = evecs = K = None
-    if eigenvalue_file is not None:
+    if loco:
+        pass
+    elif eigenvalue_file is not None:
         evals = np.loadtxt(eigenvalue_file, dtype=np.float64)
         evecs = np.loadtxt(eigenvector_file, dtype=np.float64)
     elif kinship_file is not None:
@@ -74,13 +79,22 @@ def gwas(bfile, *, kinship_file=None, covariate_file=None, lmm_mode: int = 1, ma
         if save_kinship:
             write_kinship_matrix(K, Path(output_dir) / f"{output_prefix}.cXX.txt")
     t_k = time.perf_counter()
-    cov = None
-    if covariate_file is not None:
-        cov, _ = read_covariate_file(covariate_file)
-        if cov.shape[0] != n:
-            raise ValueError(f"Covariate file has {cov.shape[0]} rows but .fam has {n} samples")
     out = Path(output_dir) / f"{output_prefix}.assoc.txt"
     timing: dict = {}
+    if loco:
+        from jamma_b200.loco import run_lmm_loco
+
+        ks = None
+        if ksnps_file is not None:
+            ks = np.array(sorted(pos[s] for s in _read_snp_list(ksnps_file) if s in pos), dtype=np.int64)
+        res = run_lmm_loco(bfile, y, covariates=cov, maf_threshold=maf, miss_threshold=miss,
+                           lmm_mode=lmm_mode, output_path=out, save_kinship=save_kinship,
+                           kinship_output_dir=Path(output_dir), kinship_output_prefix=output_prefix,
+                           snps_indices=snps_idx, ksnps_indices=ks)
+        t_end = time.perf_counter()
+        n_valid = int(np.sum(~np.isnan(y) & (y != -9.0)))
+        return GWASResult(res, n_valid, meta["n_snps"],
+                          {"kinship_s": 0.0, "lmm_s": t_end - t0, "total_s": t_end - t0})
     res = run_lmm_association_streaming(
         bfile, y, kinship=K, covariates=cov, eigenvalues=evals, eigenvectors=evecs,
         maf_threshold=maf, miss_threshold=miss, output_path=out, lmm_mode=lmm_mode,

@@ -86,37 +86,50 @@ class _KinshipI8:
         self.sum_mu2 = 0.0
         self.col = 0
 
-    def add(self, codes: torch.Tensor, mu64: torch.Tensor, has_missing: bool) -> None:
+    def add(self, codes: torch.Tensor, mu64: torch.Tensor, has_missing: bool,
+            packed: torch.Tensor | None = None) -> None:
+        """Add a chunk of decoded codes (m, ld); ``packed`` are the same SNPs' .bed records
+        (needed when ``has_missing``)."""
         m, ld = codes.shape
         st = stream_handle()
         Cs = None
         if has_missing:
             if self.RT is None:
-                self.RT = torch.zeros((2 * self.n, self.n), dtype=torch.float64, device="cuda")
+                self.RT = torch.zeros((self.n, self.n), dtype=torch.float64, device="cuda")
             Cs = torch.empty((self.n, m), dtype=torch.int8, device="cuda")
         _native.call("jb_codes_to_sample_major", ptr(codes), ld, self.n, m, ptr(self.Zs), self.ldz,
                      self.col, ptr(Cs), m, st)
-        _native.call("jb_kinship_i8_corrections", ptr(codes), ld, ptr(Cs), m, self.n, m, ptr(mu64),
-                     ptr(self.a), ptr(self.b), ptr(self.RT), self.n, st)
+        if has_missing and packed is None:
+            packed = torch.empty((m, (self.n + 3) // 4), dtype=torch.uint8, device="cuda")
+            _native.call("jb_pack_codes", ptr(codes), ld, self.n, m, ptr(packed), packed.shape[1], st)
+        bps = 0 if packed is None else packed.shape[1]
+        _native.call("jb_kinship_i8_corrections", ptr(codes), ld, ptr(packed), bps, ptr(Cs), m,
+                     self.n, m, ptr(mu64), ptr(self.a), ptr(self.b), ptr(self.RT), self.n, st)
         self.col += m
 
     def add_sum_mu2(self, mu64_host: np.ndarray) -> None:
         self.sum_mu2 += float(np.sum(np.asarray(mu64_host, dtype=np.float64) ** 2))
 
-    def finish(self) -> torch.Tensor:
+    def gram(self) -> torch.Tensor:
+        """Exact int32 Gram of the accumulated calls (upper triangle, column-major)."""
         n = self.n
         st = stream_handle()
         C = torch.empty((n, n), dtype=torch.int32, device="cuda")
         ws = workspace(_native.load().jb_gram_i8_workspace_size(n))
         _native.call("jb_gram_i8", ptr(self.Zs), n, self.p, self.ldz, ptr(C), n, ptr(ws), ws.numel(), st)
-        K = torch.empty((n, n), dtype=torch.float64, device="cuda")
-        _native.call("jb_kinship_i8_finalize", ptr(C), n, n, ptr(self.a), ptr(self.b), self.sum_mu2,
-                     ptr(self.RT), n, self.p, ptr(K), n, st)
         status = np.zeros(1, dtype=np.int32)
         _native.call("jb_gram_status", ptr(ws), status.ctypes.data, st)
         if status[0] != 0:
             raise RuntimeError(f"INT8 Gram pipeline reported status {int(status[0])}")
-        self.C = C
+        self.Zs = None  # the operand is no longer needed
+        return C
+
+    def finish(self) -> torch.Tensor:
+        n = self.n
+        C = self.gram()
+        K = torch.empty((n, n), dtype=torch.float64, device="cuda")
+        _native.call("jb_kinship_i8_finalize", ptr(C), n, n, ptr(self.a), ptr(self.b), self.sum_mu2,
+                     ptr(self.RT), n, self.p, ptr(K), n, stream_handle())
         return K
 
 
@@ -137,7 +150,8 @@ def _kinship_from_packed(packed_dev: torch.Tensor, n: int, batch_size: int, maf_
     sel = torch.from_numpy(idx).to("cuda")
     if precision == "int8":
         acc = _KinshipI8(n, idx.size)
-        acc.add(codes.index_select(0, sel), mu64, bool(np.any(c[:, 0] < n)))
+        acc.add(codes.index_select(0, sel), mu64, bool(np.any(c[:, 0] < n)),
+                packed_dev.index_select(0, sel))
         acc.add_sum_mu2(c[:, 1] / np.maximum(c[:, 0], 1))
         return acc.finish(), idx.size
     acc = _KinshipAccumulator(n, max(1, min(batch_size, 8192)))
@@ -197,7 +211,7 @@ def compute_kinship_from_bed(bfile, maf_threshold: float = 0.0, miss_threshold: 
         c = counts[sub]
         mu64 = torch.from_numpy(c[:, 1] / np.maximum(c[:, 0], 1)).to("cuda")
         if i8:
-            acc.add(codes, mu64, bool(np.any(c[:, 0] < n)))
+            acc.add(codes, mu64, bool(np.any(c[:, 0] < n)), None if sidx is not None else rec)
             acc.add_sum_mu2(c[:, 1] / np.maximum(c[:, 0], 1))
         else:
             acc.add(codes, mu64)

@@ -72,3 +72,36 @@ def stream_pass1_means(g32: np.ndarray):
     before storing into float32, so the mean is ``float32(sum / n_obs)``.
     """
     return snp_stats(np.asarray(g32, dtype=np.float32))
+
+
+def loco_kinships(g: np.ndarray, chroms, maf_threshold: float = 0.0, miss_threshold: float = 1.0):
+    """Leave-one-chromosome-out kinships, in sorted chromosome-name order.
+
+    Restates ``compute_loco_kinship_streaming`` (``src/jamma/kinship/compute.py:693-916``):
+    float32 pass-1 statistics over all samples pick the SNPs (MAF / missing / monomorphic),
+    float64 ``impute_and_center`` per SNP, S_full = sum of all kept SNPs' Xc Xc^T and
+    S_c per chromosome, K_loco_c = (S_full - S_c) / (p - p_c).  Yields (chr, K_loco_c).
+    """
+    chroms = np.asarray(chroms).astype(str)
+    n, _ = g.shape
+    mean, miss, var = snp_stats(np.asarray(g, dtype=np.float32))
+    mask, _ = filter_mask(mean, miss, var, n, maf_threshold, miss_threshold)
+    idx = np.where(mask)[0]
+    if idx.size == 0:
+        raise ValueError("No SNPs passed filtering")
+    x = np.asarray(g[:, idx], dtype=np.float64)
+    with np.testing.suppress_warnings() as sup:
+        sup.filter(RuntimeWarning)
+        mu = np.nan_to_num(np.nanmean(x, axis=0, keepdims=True), nan=0.0)
+    xc = np.where(np.isnan(x), mu, x) - mu
+    s_full = xc @ xc.T
+    kept_chr = chroms[idx]
+    for c in sorted(set(chroms.tolist())):
+        sel = kept_chr == c
+        if not np.any(sel):
+            continue
+        p_loco = idx.size - int(sel.sum())
+        if p_loco == 0:
+            raise ValueError(f"all filtered SNPs are on chromosome {c}")
+        s_c = xc[:, sel] @ xc[:, sel].T
+        yield c, (s_full - s_c) / p_loco

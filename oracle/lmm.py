@@ -427,3 +427,48 @@ def lmm_association(g, phenotypes, kinship=None, covariates=None, eigenvalues=No
     keys = parts[0].keys() if parts else []
     res.stats = {k: np.concatenate([p[k] for p in parts]) for k in keys}
     return res
+
+
+def loco_association(g, phenotypes, chroms, covariates=None, lmm_mode=1, maf_threshold=0.01,
+                     miss_threshold=0.05, chunk=2000):
+    """``run_lmm_loco`` (``src/jamma/lmm/loco.py:54-252``): per chromosome (sorted names)
+    the LOCO kinship (filtered with the association's MAF / missing thresholds over all
+    samples) is restricted to the analysed samples and eigendecomposed; that chromosome's
+    SNPs are tested with float64 statistics and imputation means over the analysed
+    samples (``_run_lmm_for_chromosome``, 255-593).  Returns a list of
+    (chr, snp_indices, af, n_miss, stats) in output order.
+    """
+    from oracle.kinship import filter_mask, loco_kinships, snp_stats
+
+    chroms = np.asarray(chroms).astype(str)
+    y = np.asarray(phenotypes, dtype=np.float64)
+    valid = ~np.isnan(y) & (y != -9.0)
+    if covariates is not None:
+        valid &= np.all(~np.isnan(covariates), axis=1)
+    yv = y[valid]
+    W = np.ones((yv.size, 1)) if covariates is None else np.asarray(covariates, np.float64)[valid]
+    n = yv.size
+    out = []
+    for c, K in loco_kinships(g, chroms, maf_threshold, miss_threshold):
+        evals, U = eigh_threshold(K[np.ix_(valid, valid)])
+        cols = np.where(chroms == c)[0]
+        gc = np.asarray(g[np.ix_(valid, cols)], dtype=np.float64)
+        mean, miss, var = snp_stats(gc)
+        mask, af = filter_mask(mean, miss, var, n, maf_threshold, miss_threshold)
+        loc = np.where(mask)[0]
+        if loc.size == 0:
+            continue
+        UT = np.ascontiguousarray(U.T)
+        UtW, Uty = UT @ W, UT @ yv
+        lam0 = l0 = None
+        if lmm_mode in (2, 3, 4):
+            lam0, l0 = null_model_mle(evals, UtW, Uty)
+        parts = []
+        for s in range(0, loc.size, chunk):
+            sub = loc[s:s + chunk]
+            gs = gc[:, sub]
+            gs = np.where(np.isnan(gs), mean[sub][None, :], gs)
+            parts.append(lmm_chunk(lmm_mode, evals, UtW, Uty, UT @ gs, l0, lam0))
+        stats = {k: np.concatenate([p[k] for p in parts]) for k in parts[0]}
+        out.append((c, cols[loc], af[loc], miss[loc].astype(int), stats))
+    return out
