@@ -167,6 +167,49 @@ def _cpu_baseline(args, cohort, evals_h, U_h, UtW_h, Uty_h, lam0, l0) -> dict:
             "sample": f"{m} SNPs at n={args.n} (rotation on host BLAS + NumPy search, -lmm {args.mode})"}
 
 
+def run_serving(args, seed: int = 7) -> dict:
+    """A Poisson stream of GWAS jobs through the continuous-batching server.
+
+    Scaled-down version of the serving configuration (200 jobs, n up to 40 000) so the
+    default bench stays within minutes: ``args.serve_jobs`` jobs, n ~ log-uniform in
+    [2 000, 8 000], SNPs ~ log-uniform in [10 000, 40 000], 1-4 phenotypes, lmm mode
+    drawn from {1, 2, 3, 4}, 30 % of jobs reusing a resident cohort's eigenvectors.
+    """
+    import torch
+
+    from jamma_b200 import synth
+    from jamma_b200.serve import GwasJob, GwasServer
+
+    rng = np.random.default_rng(seed)
+    cohorts = {}
+    jobs = []
+    t = 0.0
+    for i in range(args.serve_jobs):
+        if cohorts and rng.random() < 0.3:
+            cid = list(cohorts)[rng.integers(len(cohorts))]
+        else:
+            cid = f"c{i}"
+            n = int(np.exp(rng.uniform(np.log(2000), np.log(8000))))
+            p = int(np.exp(rng.uniform(np.log(10000), np.log(40000))))
+            cohorts[cid] = (n, synth.packed_records_device(n, p, 0.01, seed=5000 + i).cpu().numpy())
+        n, packed = cohorts[cid]
+        phi = int(rng.integers(1, 5))
+        y = rng.normal(size=(n, phi))
+        cov = np.column_stack([np.ones(n), rng.normal(size=n)]) if rng.random() < 0.5 else None
+        t += rng.exponential(args.serve_gap)
+        jobs.append((t, GwasJob(f"j{i}", cid, packed, n, y if phi > 1 else y[:, 0], cov,
+                                int(rng.integers(1, 5)))))
+    srv = GwasServer(hbm_budget_bytes=int(args.serve_budget_gb * (1 << 30)), max_active=4,
+                     chunk=4096)
+    torch.cuda.synchronize()
+    srv.run(jobs)
+    out = srv.latency_summary()
+    out.update(workload=f"{args.serve_jobs} jobs, Poisson gaps {args.serve_gap}s, n 2k-8k, "
+                        f"SNPs 10k-40k, 1-4 phenotypes, modes 1-4, 30% cohort reuse",
+               hbm_budget_gb=args.serve_budget_gb, max_active=4)
+    return out
+
+
 def run_ours(args) -> None:
     import torch
     import torch.distributed as dist
@@ -347,6 +390,10 @@ def run_ours(args) -> None:
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         e2e_ms = float(tt.item())
 
+    serving = None
+    if rank == 0 and not args.no_serving:
+        serving = run_serving(args)
+
     if rank == 0:
         peaks = _peaks()
         # dominant kernel of the mixed form: the INT8 tcgen05 rotation, 4 digit planes x
@@ -387,6 +434,7 @@ def run_ours(args) -> None:
                     "h2d_bytes_per_step": m * bps + m * 8,
                     "d2h_bytes_per_step": len(outs) * m * 8},
             "clocks": clocks,
+            "serving": serving,
             "hbm_peak_gbs": peaks.get("hbm_gbs", HBM_PEAK_FALLBACK),
         }
         print(json.dumps(line), flush=True)
@@ -416,6 +464,10 @@ def main():
     ap.add_argument("--cpu-snps", type=int, default=64)
     ap.add_argument("--ref-snps", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-serving", action="store_true")
+    ap.add_argument("--serve-jobs", type=int, default=24)
+    ap.add_argument("--serve-gap", type=float, default=0.2)
+    ap.add_argument("--serve-budget-gb", type=float, default=60.0)
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

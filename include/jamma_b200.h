@@ -110,6 +110,8 @@ int32_t jb_kinship_finalize(double* K, int64_t n, int64_t ldk, double scale,
  *   (the chunk has missing calls), Q = R + T/2 into RT (column-major n x n, ld ldr;
  *   T is symmetric, so R + R^T + T = Q + Q^T); the missing-call terms read the chunk's
  *   packed .bed records (m x bytes_per_snp, all n samples, same SNP order as codes).
+ *   partial: jb_kinship_i8_partial_size(n, m) bytes of scratch for the ordered
+ *   (deterministic) two-stage reduction of a and b.
  * jb_kinship_i8_finalize: K (n x n, ldk) = symmetric combination above / p_kept.
  */
 int64_t jb_gram_i8_workspace_size(int64_t n);
@@ -135,11 +137,13 @@ int32_t jb_gram_i8_noalloc(const int8_t* Zs, int64_t n, int64_t p, int64_t ldz, 
 int32_t jb_codes_to_sample_major(const int8_t* codes, int64_t ld_codes, int64_t n,
                                  int64_t m, int8_t* Zs, int64_t ldz, int64_t col0,
                                  int8_t* Cs, int64_t ldcs, uintptr_t stream);
+int64_t jb_kinship_i8_partial_size(int64_t n, int64_t m);
 int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes,
                                   const uint8_t* packed, int64_t bytes_per_snp,
                                   const int8_t* Cs, int64_t ldcs, int64_t n, int64_t m,
                                   const double* mu, double* a, double* b, double* RT,
-                                  int64_t ldr, uintptr_t stream);
+                                  int64_t ldr, void* partial, int64_t partial_bytes,
+                                  uintptr_t stream);
 int32_t jb_kinship_i8_finalize(const int32_t* C, int64_t ldc, int64_t n, const double* a,
                                const double* b, double sum_mu2, const double* RT,
                                int64_t ldr, int64_t p_kept, double* K, int64_t ldk,

@@ -146,16 +146,17 @@ __global__ void codes_to_sample_major_kernel(const int8_t* __restrict__ codes, i
     }
 }
 
-// a_i = sum_j Z_ij mu_j and b_i = sum_{j missing at i} mu_j^2 from SNP-major codes.
-// Block (256 samples) x (256 SNPs); partial sums are added with FP64 atomics.
-__global__ void kin_vectors_kernel(const int8_t* __restrict__ codes, int64_t ldc, int64_t n,
-                                   int64_t m, const double* __restrict__ mu,
-                                   double* __restrict__ a, double* __restrict__ b) {
+// a_i = sum_j Z_ij mu_j and b_i = sum_{j missing at i} mu_j^2 from SNP-major codes, in
+// two deterministic stages: block (256 samples) x (256 SNPs) partial sums, then an
+// ordered sum over the SNP blocks (no atomics, so results are bit-reproducible).
+__global__ void kin_vectors_partial_kernel(const int8_t* __restrict__ codes, int64_t ldc,
+                                           int64_t n, int64_t m, const double* __restrict__ mu,
+                                           double* __restrict__ pa, double* __restrict__ pb) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const int64_t j0 = (int64_t)blockIdx.y * 256;
+    const int64_t jb = blockIdx.y;
     if (i >= n) return;
     double sa = 0.0, sb = 0.0;
-    const int64_t j1 = j0 + 256 < m ? j0 + 256 : m;
+    const int64_t j0 = jb * 256, j1 = j0 + 256 < m ? j0 + 256 : m;
     for (int64_t j = j0; j < j1; ++j) {
         const int8_t c = codes[j * ldc + i];
         const double u = __ldg(mu + j);
@@ -164,29 +165,64 @@ __global__ void kin_vectors_kernel(const int8_t* __restrict__ codes, int64_t ldc
         else
             sa = fma((double)c, u, sa);
     }
-    atomicAdd(a + i, sa);
-    atomicAdd(b + i, sb);
+    pa[jb * n + i] = sa;
+    pb[jb * n + i] = sb;
+}
+
+__global__ void kin_vectors_reduce_kernel(int64_t n, int64_t nblk, const double* __restrict__ pa,
+                                          const double* __restrict__ pb, double* __restrict__ a,
+                                          double* __restrict__ b) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    double sa = 0.0, sb = 0.0;
+    for (int64_t k = 0; k < nblk; ++k) {
+        sa += pa[k * n + i];
+        sb += pb[k * n + i];
+    }
+    a[i] += sa;
+    b[i] += sb;
 }
 
 // Sparse terms for one SNP chunk.  For every sample k and every SNP j of the chunk that
 // is missing at k: Q[:, k] += mu_j Z[:, j] + (mu_j^2 / 2) M[:, j]  (Q = R + T/2).  The
 // SNP columns are read from the 2-bit packed .bed records (4x less traffic than int8
-// codes).  One CTA per (k, block of 4096 samples i); each thread owns 16 consecutive
-// samples (one 32-bit packed load per missing SNP) and keeps their sums in registers.
+// codes).  One CTA per (k, block of 2048 samples i); each thread owns 8 consecutive
+// samples (one 16-bit packed load per missing SNP, four loads in flight) and keeps their
+// sums in registers.
+__device__ __forceinline__ void kin_sparse_accum(uint32_t w, double u, double (&r)[8],
+                                                 double (&tt)[8]) {
+    const double u2h = 0.5 * u * u, u2 = 2.0 * u;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        // count-A1 codes: 00 -> 2, 01 -> missing, 10 -> 1, 11 -> 0
+        const uint32_t code = (w >> (2 * q)) & 3u;
+        r[q] += code == 0u ? u2 : (code == 2u ? u : 0.0);
+        tt[q] += code == 1u ? u2h : 0.0;
+    }
+}
+
 __global__ void __launch_bounds__(256) kin_sparse_kernel(const uint8_t* __restrict__ packed,
                                                           int64_t bps, const int8_t* __restrict__ Cs,
                                                           int64_t ldcs, int64_t n, int64_t m,
                                                           const double* __restrict__ mu,
                                                           double* __restrict__ Q, int64_t ldq) {
     const int64_t k = blockIdx.x;
-    const int64_t i0 = (int64_t)blockIdx.y * 4096 + 16 * threadIdx.x;
+    const int64_t i0 = (int64_t)blockIdx.y * 2048 + 8 * threadIdx.x;
     __shared__ int32_t list[2048];
     __shared__ int cnt;
-    double r[16], tt[16];
+    double r[8], tt[8];
 #pragma unroll
-    for (int e = 0; e < 16; ++e) r[e] = tt[e] = 0.0;
-    const int64_t b0 = i0 >> 2;  // first packed byte of this thread's 16 samples
-    const bool full = (i0 + 16 <= n) && ((bps & 3) == 0);
+    for (int e = 0; e < 8; ++e) r[e] = tt[e] = 0.0;
+    const int64_t b0 = i0 >> 2;  // first packed byte of this thread's 8 samples
+    const bool full = (i0 + 8 <= n) && ((bps & 1) == 0);
+    auto load = [&](int64_t j) -> uint32_t {
+        const uint8_t* rec = packed + j * bps;
+        if (full) return *reinterpret_cast<const uint16_t*>(rec + b0);
+        uint32_t w = 0xffffu;  // padding decodes as 0 copies
+        for (int q = 0; q < 2; ++q)
+            if (b0 + q < bps) w = (w & ~(0xffu << (8 * q))) | ((uint32_t)rec[b0 + q] << (8 * q));
+        return w;
+    };
     for (int64_t jb = 0; jb < m; jb += 2048) {
         if (threadIdx.x == 0) cnt = 0;
         __syncthreads();
@@ -196,34 +232,25 @@ __global__ void __launch_bounds__(256) kin_sparse_kernel(const uint8_t* __restri
         __syncthreads();
         const int c = cnt;
         if (i0 < n) {
-            for (int e = 0; e < c; ++e) {
+            int e = 0;
+            for (; e + 4 <= c; e += 4) {
+                const int64_t j0 = list[e], j1 = list[e + 1], j2 = list[e + 2], j3 = list[e + 3];
+                const uint32_t w0 = load(j0), w1 = load(j1), w2 = load(j2), w3 = load(j3);
+                const double u0 = mu[j0], u1 = mu[j1], u2 = mu[j2], u3 = mu[j3];
+                kin_sparse_accum(w0, u0, r, tt);
+                kin_sparse_accum(w1, u1, r, tt);
+                kin_sparse_accum(w2, u2, r, tt);
+                kin_sparse_accum(w3, u3, r, tt);
+            }
+            for (; e < c; ++e) {
                 const int64_t j = list[e];
-                const double u = mu[j];
-                const double u2h = 0.5 * u * u;
-                const uint8_t* rec = packed + j * bps;
-                uint32_t w;
-                if (full) {
-                    w = *reinterpret_cast<const uint32_t*>(rec + b0);
-                } else {
-                    w = 0xffffffffu;  // padding decodes as 0 copies
-                    for (int q = 0; q < 4; ++q)
-                        if (b0 + q < bps) w = (w & ~(0xffu << (8 * q))) | ((uint32_t)rec[b0 + q] << (8 * q));
-                }
-#pragma unroll
-                for (int q = 0; q < 16; ++q) {
-                    // count-A1 codes: 00 -> 2, 01 -> missing, 10 -> 1, 11 -> 0
-                    const uint32_t code = (w >> (2 * q)) & 3u;
-                    if (code == 1u)
-                        tt[q] += u2h;
-                    else
-                        r[q] += (code == 0u) ? 2.0 * u : (code == 2u ? u : 0.0);
-                }
+                kin_sparse_accum(load(j), mu[j], r, tt);
             }
         }
         __syncthreads();
     }
 #pragma unroll
-    for (int q = 0; q < 16; ++q) {
+    for (int q = 0; q < 8; ++q) {
         const int64_t i = i0 + q;
         if (i < n) Q[k * ldq + i] += r[q] + tt[q];  // Q[i, k] (column-major, column k)
     }
@@ -442,21 +469,34 @@ int32_t jb_codes_to_sample_major(const int8_t* codes, int64_t ld_codes, int64_t 
     return JB_OK;
 }
 
+int64_t jb_kinship_i8_partial_size(int64_t n, int64_t m) {
+    if (n <= 0 || m < 0) return -1;
+    return 2 * ceil_div(m > 0 ? m : 1, 256) * n * 8;
+}
+
 int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes, const uint8_t* packed,
                                   int64_t bytes_per_snp, const int8_t* Cs, int64_t ldcs, int64_t n,
                                   int64_t m, const double* mu, double* a, double* b, double* RT,
-                                  int64_t ldr, uintptr_t stream) {
+                                  int64_t ldr, void* partial, int64_t partial_bytes,
+                                  uintptr_t stream) {
     JB_CHECK_ARG(n > 0 && m >= 0 && ld_codes >= n, "jb_kinship_i8_corrections: bad shape");
     if (m == 0) return JB_OK;
     cudaStream_t st = as_stream(stream);
     JB_CHECK_ARG(ceil_div(m, 256) < 65536, "jb_kinship_i8_corrections: chunk too large");
-    kin_vectors_kernel<<<dim3((unsigned)ceil_div(n, 256), (unsigned)ceil_div(m, 256)), 256, 0, st>>>(
-        codes, ld_codes, n, m, mu, a, b);
-    JB_LAUNCH_CHECK("kin_vectors_kernel");
+    JB_CHECK_ARG(partial && partial_bytes >= jb_kinship_i8_partial_size(n, m),
+                 "jb_kinship_i8_corrections: partial-sum buffer too small");
+    const int64_t nblk = ceil_div(m, 256);
+    double* pa = static_cast<double*>(partial);
+    double* pb = pa + nblk * n;
+    kin_vectors_partial_kernel<<<dim3((unsigned)ceil_div(n, 256), (unsigned)nblk), 256, 0, st>>>(
+        codes, ld_codes, n, m, mu, pa, pb);
+    JB_LAUNCH_CHECK("kin_vectors_partial_kernel");
+    kin_vectors_reduce_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, st>>>(n, nblk, pa, pb, a, b);
+    JB_LAUNCH_CHECK("kin_vectors_reduce_kernel");
     if (Cs) {
         JB_CHECK_ARG(RT && ldr >= n && ldcs >= m && packed && 4 * bytes_per_snp >= n,
                      "jb_kinship_i8_corrections: Q buffer and packed records needed");
-        dim3 grid((unsigned)n, (unsigned)ceil_div(n, 4096), 1);
+        dim3 grid((unsigned)n, (unsigned)ceil_div(n, 2048), 1);
         kin_sparse_kernel<<<grid, 256, 0, st>>>(packed, bytes_per_snp, Cs, ldcs, n, m, mu, RT, ldr);
         JB_LAUNCH_CHECK("kin_sparse_kernel");
     }

@@ -58,6 +58,14 @@ def rotate(U: torch.Tensor, B: torch.Tensor, out: torch.Tensor | None = None) ->
     return out
 
 
+def ozaki_split(U: torch.Tensor) -> torch.Tensor:
+    """INT8 digit planes of column-major eigenvectors U (n, n) for the mixed rotation."""
+    n = U.shape[0]
+    oz = workspace(_native.load().jb_ozaki_workspace_size(n))
+    _native.call("jb_ozaki_prepare", ptr(U), n, n, ptr(oz), oz.numel(), stream_handle())
+    return oz
+
+
 class DeviceCohort:
     """One cohort's resident state for association testing.
 
@@ -71,7 +79,8 @@ class DeviceCohort:
     """
 
     def __init__(self, eigenvalues, eigenvectors, covariates, phenotypes, lmm_mode=1,
-                 l_min=1e-5, l_max=1e5, n_grid=50, n_refine=10, precision: str = "fp64"):
+                 l_min=1e-5, l_max=1e5, n_grid=50, n_refine=10, precision: str = "fp64",
+                 ozaki: torch.Tensor | None = None):
         require_cuda()
         if precision not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
@@ -114,8 +123,10 @@ class DeviceCohort:
                          ptr(self.logl0), st)
         self.ozaki = None
         if precision == "mixed":
-            self.ozaki = workspace(_native.load().jb_ozaki_workspace_size(n))
-            _native.call("jb_ozaki_prepare", ptr(self.U), n, n, ptr(self.ozaki), self.ozaki.numel(), st)
+            if ozaki is not None:  # digit planes shared with other users of the same cohort
+                self.ozaki = ozaki
+            else:
+                self.ozaki = ozaki_split(self.U)
         self.code_ld = (n + 127) // 128 * 128 if precision == "mixed" else n
         self._rot_ws = None
         self._chunk_ws = None

@@ -103,8 +103,10 @@ class _KinshipI8:
             packed = torch.empty((m, (self.n + 3) // 4), dtype=torch.uint8, device="cuda")
             _native.call("jb_pack_codes", ptr(codes), ld, self.n, m, ptr(packed), packed.shape[1], st)
         bps = 0 if packed is None else packed.shape[1]
+        part = workspace(_native.load().jb_kinship_i8_partial_size(self.n, m))
         _native.call("jb_kinship_i8_corrections", ptr(codes), ld, ptr(packed), bps, ptr(Cs), m,
-                     self.n, m, ptr(mu64), ptr(self.a), ptr(self.b), ptr(self.RT), self.n, st)
+                     self.n, m, ptr(mu64), ptr(self.a), ptr(self.b), ptr(self.RT), self.n, ptr(part),
+                     part.numel(), st)
         self.col += m
 
     def add_sum_mu2(self, mu64_host: np.ndarray) -> None:

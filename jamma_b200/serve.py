@@ -1,0 +1,238 @@
+"""Continuous-batching GWAS job server on one GPU.
+
+Jobs of different sample and SNP counts arrive over time.  A job is admitted when its
+device memory fits the HBM budget beside what is already resident; admitted jobs run
+concurrently, each on its own CUDA stream, advancing one SNP chunk at a time, so their
+kernels overlap on the device and a job that arrives while others run starts as soon as
+memory frees up.  Cohorts (eigenvalues, eigenvectors and their INT8 digit planes) stay
+resident and are shared: a job on a known cohort skips kinship and eigendecomposition.
+Packed genotype records stream from pinned host memory with asynchronous copies on the
+job's stream.  Every job's arithmetic is the library's ordinary association path with
+per-job buffers and a fixed chunk width, so its results do not depend on what else runs.
+"""
+
+from __future__ import annotations
+
+import time
+from collections import OrderedDict, deque
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from jamma_b200 import _native
+from jamma_b200 import engine as eng
+from jamma_b200.device import empty, ptr, require_cuda, stream_handle
+from jamma_b200.kinship import _KinshipI8, filter_mask, snp_stats_from_counts
+
+
+@dataclass
+class GwasJob:
+    """One association request.
+
+    ``packed``: (p, ceil(n/4)) count-A1 .bed records of the cohort's SNPs (host);
+    ``phenotypes``: (n,) or (n, phi), no missing values (the serving path expects
+    pre-filtered samples); ``cohort_id``: jobs naming a resident cohort reuse its
+    eigendecomposition, otherwise the kinship is built from ``packed`` on the device.
+    """
+
+    job_id: str
+    cohort_id: str
+    packed: np.ndarray
+    n_samples: int
+    phenotypes: np.ndarray
+    covariates: np.ndarray | None = None
+    lmm_mode: int = 1
+    maf_threshold: float = 0.01
+    miss_threshold: float = 0.05
+    arrival: float = 0.0
+    done: float = 0.0
+    results: dict = field(default_factory=dict)
+    snp_indices: np.ndarray | None = None
+
+
+class _Resident:
+    def __init__(self, evals: torch.Tensor, U: torch.Tensor, ozaki: torch.Tensor | None):
+        self.evals, self.U, self.ozaki = evals, U, ozaki
+        n = U.shape[0]
+        self.bytes = 8 * n * n + 8 * n + (ozaki.numel() if ozaki is not None else 0)
+        self.refs = 0
+
+
+class _Active:
+    def __init__(self, job: GwasJob, stream: torch.cuda.Stream):
+        self.job, self.stream = job, stream
+        self.chunk_starts: list[int] = []
+        self.next = 0
+        self.inflight: list = []  # (event, host buffers, start, end)
+        self.bytes = 0
+
+
+def job_device_bytes(n: int, phi: int, n_cvt: int, chunk: int, resident: bool) -> int:
+    """Device bytes a job holds while it runs (cohort state counted when not resident)."""
+    lib = _native.load()
+    b = lib.jb_lmm_workspace_size(n, n_cvt, phi, 50) + lib.jb_lmm_chunk_workspace_size(
+        n, n_cvt, phi, 50, chunk)
+    b += lib.jb_rotate_i8_workspace_size(n, chunk) + chunk * n * 8 + chunk * ((n + 127) // 128 * 128)
+    b += 9 * phi * chunk * 8 + 2 * n * (n_cvt + phi) * 8
+    if not resident:
+        b += 8 * n * n * 2 + lib.jb_ozaki_workspace_size(n) + n * 8  # K / U, digits, evals
+    return int(b)
+
+
+class GwasServer:
+    def __init__(self, hbm_budget_bytes: int, max_active: int = 4, chunk: int = 4096,
+                 precision: str = "mixed"):
+        require_cuda()
+        self.budget = int(hbm_budget_bytes)
+        self.max_active = max_active
+        self.chunk = chunk
+        self.precision = precision
+        self.cohorts: OrderedDict[str, _Resident] = OrderedDict()
+        self.queue: deque[GwasJob] = deque()
+        self.active: list[_Active] = []
+        self.finished: list[GwasJob] = []
+        self.used = 0
+        self.snps_done = 0
+        self.t0 = None
+
+    # ------------------------------------------------------------ admission
+    def submit(self, job: GwasJob, now: float | None = None) -> None:
+        job.arrival = time.perf_counter() if now is None else now
+        self.queue.append(job)
+
+    def _resident_bytes(self) -> int:
+        return sum(r.bytes for r in self.cohorts.values())
+
+    def _evict_for(self, need: int) -> None:
+        for cid in list(self.cohorts):
+            if self.used + self._resident_bytes() + need <= self.budget:
+                return
+            if self.cohorts[cid].refs == 0:
+                del self.cohorts[cid]
+
+    def _try_admit(self) -> None:
+        while self.queue and len(self.active) < self.max_active:
+            job = self.queue[0]
+            phi = 1 if np.ndim(job.phenotypes) == 1 else job.phenotypes.shape[1]
+            c = 1 if job.covariates is None else job.covariates.shape[1]
+            need = job_device_bytes(job.n_samples, phi, c, self.chunk, job.cohort_id in self.cohorts)
+            self._evict_for(need)
+            if self.used + self._resident_bytes() + need > self.budget:
+                if not self.active:
+                    raise MemoryError(f"job {job.job_id} needs {need} bytes, over the HBM budget")
+                return
+            self.queue.popleft()
+            self._start(job, need)
+
+    def _start(self, job: GwasJob, need: int) -> None:
+        stream = torch.cuda.Stream()
+        act = _Active(job, stream)
+        act.bytes = need
+        self.used += need
+        n = job.n_samples
+        with torch.cuda.stream(stream):
+            packed = torch.from_numpy(job.packed).pin_memory().to("cuda", non_blocking=True)
+            codes, counts = eng.decode_packed(packed, n, None, n)
+            cnt = counts.cpu().numpy()  # pass 1: per-SNP statistics
+            mean, miss, poly = snp_stats_from_counts(cnt, n, np.float32)
+            keep, af = filter_mask(mean, miss, poly, n, job.maf_threshold, job.miss_threshold)
+            idx = np.where(keep)[0]
+            res = self.cohorts.get(job.cohort_id)
+            if res is None:  # new cohort: INT8 kinship + FP64 eigendecomposition on the device
+                acc = _KinshipI8(n, int(poly.sum()))
+                kidx = np.where(poly)[0]
+                sel = torch.from_numpy(kidx).cuda()
+                cc = cnt[kidx]
+                acc.add(codes.index_select(0, sel), torch.from_numpy(cc[:, 1] / np.maximum(cc[:, 0], 1)).cuda(),
+                        bool(np.any(cc[:, 0] < n)), packed.index_select(0, sel))
+                acc.add_sum_mu2(cc[:, 1] / np.maximum(cc[:, 0], 1))
+                K = acc.finish()
+                evals, U = eng.eigh_device(K)
+                oz = eng.ozaki_split(U) if self.precision == "mixed" else None
+                res = _Resident(evals, U, oz)
+                self.cohorts[job.cohort_id] = res
+            res.refs += 1
+            self.cohorts.move_to_end(job.cohort_id)
+            act.cohort = eng.DeviceCohort(res.evals, res.U, job.covariates, job.phenotypes,
+                                          job.lmm_mode, precision=self.precision, ozaki=res.ozaki)
+            act.packed_host = torch.from_numpy(np.ascontiguousarray(job.packed[idx])).pin_memory()
+            act.means = torch.from_numpy(mean[idx].astype(np.float64)).pin_memory()
+            act.n_miss = miss[idx]
+        job.snp_indices = idx
+        job.results = {k: np.empty((act.cohort.phi, idx.size)) for k in eng.MODE_KEYS[job.lmm_mode]}
+        job.af, job.n_miss = af[idx], miss[idx]
+        act.chunk_starts = list(range(0, idx.size, self.chunk))
+        act.bufs = {"UtG": empty((self.chunk, n))}
+        self.active.append(act)
+
+    # ------------------------------------------------------------ execution
+    def _launch_chunk(self, act: _Active) -> None:
+        s = act.chunk_starts[act.next]
+        e = min(s + self.chunk, act.job.snp_indices.size)
+        act.next += 1
+        n = act.job.n_samples
+        with torch.cuda.stream(act.stream):
+            rec = act.packed_host[s:e].to("cuda", non_blocking=True)
+            mu = act.means[s:e].to("cuda", non_blocking=True)
+            codes, _ = eng.decode_packed(rec, n, None, n, ld=act.cohort.code_ld)
+            out = act.cohort.associate_codes(codes, mu, bufs=act.bufs,
+                                             has_missing=bool(np.any(act.n_miss[s:e] > 0)))
+            host = {k: torch.empty(v.shape, dtype=torch.float64).pin_memory() for k, v in out.items()}
+            for k, v in out.items():
+                host[k].copy_(v, non_blocking=True)
+            ev = torch.cuda.Event()
+            ev.record(act.stream)
+        act.inflight.append((ev, host, s, e, rec, mu, codes, out))
+
+    def _poll(self, act: _Active) -> bool:
+        """Collect finished chunks; returns True when the job is complete."""
+        keep = []
+        for item in act.inflight:
+            ev, host, s, e = item[:4]
+            if ev.query():
+                for k, v in host.items():
+                    act.job.results[k][:, s:e] = v.numpy()
+                self.snps_done += (e - s) * act.cohort.phi
+            else:
+                keep.append(item)
+        act.inflight = keep
+        return act.next >= len(act.chunk_starts) and not act.inflight
+
+    def step(self) -> None:
+        self._try_admit()
+        for act in list(self.active):
+            if act.next < len(act.chunk_starts) and len(act.inflight) < 2:
+                self._launch_chunk(act)
+            if self._poll(act):
+                act.job.done = time.perf_counter()
+                self.finished.append(act.job)
+                self.cohorts[act.job.cohort_id].refs -= 1
+                self.used -= act.bytes
+                self.active.remove(act)
+
+    def run(self, arrivals: list[tuple[float, GwasJob]] | None = None) -> list[GwasJob]:
+        """Drive the loop until every submitted (and, if given, scheduled) job is done.
+
+        ``arrivals``: (offset seconds, job) pairs submitted when the wall clock reaches
+        start + offset -- a job stream arriving while others run.
+        """
+        pending = deque(sorted(arrivals or [], key=lambda a: a[0]))
+        self.t0 = time.perf_counter()
+        while pending or self.queue or self.active:
+            now = time.perf_counter()
+            while pending and now - self.t0 >= pending[0][0]:
+                self.submit(pending.popleft()[1], now)
+            if not self.active and not self.queue and pending:
+                time.sleep(min(0.001, max(0.0, pending[0][0] - (now - self.t0))))
+                continue
+            self.step()
+        torch.cuda.synchronize()
+        return self.finished
+
+    def latency_summary(self) -> dict:
+        lat = np.array([j.done - j.arrival for j in self.finished])
+        span = max(j.done for j in self.finished) - min(j.arrival for j in self.finished)
+        return {"jobs": len(self.finished), "p50_s": float(np.percentile(lat, 50)),
+                "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()),
+                "snps_per_s": self.snps_done / span if span > 0 else None}
