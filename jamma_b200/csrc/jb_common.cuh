@@ -28,6 +28,20 @@ cusolverDnHandle_t cusolver_handle();
 
 inline cudaStream_t as_stream(uintptr_t s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// cuBLAS picks its kernels (and so its rounding) by the workspace it can use.  With the
+// library's default pool that depends on how many streams are active, so a DGEMM run
+// beside other jobs may round differently from the same DGEMM run alone.  Calls whose
+// results must not depend on concurrent work bind a caller-owned workspace of this fixed
+// size (one per concurrently used buffer set, so no two streams share it).
+constexpr int64_t kCublasWorkspaceBytes = int64_t(32) << 20;
+
+// Set the stream, then the workspace (cublasSetStream resets the workspace to the pool).
+inline cublasStatus_t bind_cublas(cublasHandle_t h, cudaStream_t st, void* ws, int64_t bytes) {
+    cublasStatus_t s = cublasSetStream(h, st);
+    if (s != CUBLAS_STATUS_SUCCESS) return s;
+    return cublasSetWorkspace(h, ws, (size_t)bytes);
+}
+
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
 }  // namespace jb

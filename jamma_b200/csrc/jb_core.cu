@@ -292,8 +292,9 @@ int32_t jb_kinship_accumulate_f64(const int8_t* codes, int64_t ld_codes, int64_t
         set_error("cuBLAS handle creation failed");
         return JB_E_LIBRARY;
     }
-    cublasStatus_t s = cublasSetStream(h, as_stream(stream));
-    if (s != CUBLAS_STATUS_SUCCESS) return cublas_status(s, "cublasSetStream");
+    // no workspace: the kernel choice must not depend on other streams' work
+    cublasStatus_t s = bind_cublas(h, as_stream(stream), nullptr, 0);
+    if (s != CUBLAS_STATUS_SUCCESS) return cublas_status(s, "cublasSetStream/Workspace");
     const double one = 1.0;
     s = cublasDsyrk(h, CUBLAS_FILL_MODE_LOWER, CUBLAS_OP_N, (int)n, (int)m, &one, X, (int)n, &one,
                     K, (int)ldk);
@@ -384,8 +385,10 @@ int32_t jb_rotate_f64(const double* U, int64_t n, int64_t ldu, const double* B, 
         set_error("cuBLAS handle creation failed");
         return JB_E_LIBRARY;
     }
-    cublasStatus_t s = cublasSetStream(h, as_stream(stream));
-    if (s != CUBLAS_STATUS_SUCCESS) return cublas_status(s, "cublasSetStream");
+    // no workspace: the kernel choice (and rounding) of U^T B must not depend on other
+    // streams' work -- U^T W and U^T y feed every SNP's search
+    cublasStatus_t s = bind_cublas(h, as_stream(stream), nullptr, 0);
+    if (s != CUBLAS_STATUS_SUCCESS) return cublas_status(s, "cublasSetStream/Workspace");
     const double one = 1.0, zero = 0.0;
     s = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, (int)n, (int)m, (int)n, &one, U, (int)ldu, B,
                     (int)ldb, &zero, C, (int)ldc);

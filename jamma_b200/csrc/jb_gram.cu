@@ -209,7 +209,8 @@ __global__ void __launch_bounds__(256) kin_sparse_kernel(const uint8_t* __restri
     const int64_t k = blockIdx.x;
     const int64_t i0 = (int64_t)blockIdx.y * 2048 + 8 * threadIdx.x;
     __shared__ int32_t list[2048];
-    __shared__ int cnt;
+    __shared__ int wcnt[8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double r[8], tt[8];
 #pragma unroll
     for (int e = 0; e < 8; ++e) r[e] = tt[e] = 0.0;
@@ -224,13 +225,26 @@ __global__ void __launch_bounds__(256) kin_sparse_kernel(const uint8_t* __restri
         return w;
     };
     for (int64_t jb = 0; jb < m; jb += 2048) {
-        if (threadIdx.x == 0) cnt = 0;
-        __syncthreads();
-        for (int64_t j = jb + threadIdx.x; j < m && j < jb + 2048; j += blockDim.x) {
-            if (Cs[k * ldcs + j] == 3) list[atomicAdd(&cnt, 1)] = (int32_t)j;
+        // Missing SNPs of sample k in this block, listed in increasing SNP order (ballot +
+        // warp prefix), so the FP64 accumulation order -- and the kinship -- is the same
+        // on every run.
+        int c = 0;
+        for (int64_t r0 = jb; r0 < m && r0 < jb + 2048; r0 += 256) {
+            const int64_t j = r0 + threadIdx.x;
+            const bool miss = j < m && j < jb + 2048 && Cs[k * ldcs + j] == 3;
+            const unsigned bal = __ballot_sync(0xffffffffu, miss);
+            if (lane == 0) wcnt[warp] = __popc(bal);
+            __syncthreads();
+            int off = c, tot = 0;
+#pragma unroll
+            for (int w = 0; w < 8; ++w) {
+                off += w < warp ? wcnt[w] : 0;
+                tot += wcnt[w];
+            }
+            if (miss) list[off + __popc(bal & ((1u << lane) - 1u))] = (int32_t)j;
+            c += tot;
+            __syncthreads();
         }
-        __syncthreads();
-        const int c = cnt;
         if (i0 < n) {
             int e = 0;
             for (; e + 4 <= c; e += 4) {

@@ -70,13 +70,23 @@ struct Params {
     //   CL[j*ldcl + r*(C+phi) + a] = sum_i h_r,i x_ij w_a,i  (a < C)
     //   CL[j*ldcl + r*(C+phi) + C + f] = sum_i h_r,i x_ij y_f,i
     //   CQ[j*ldcq + r] = sum_i h_r,i x_ij^2
+    // In the mixed form the rows are the ones row (r = 0) and the kChebG Chebyshev
+    // coefficients (r = 1 + k) of the x-dependent sums over the whole log-lambda domain
+    // [log 1e-5, log 1e5] (series_xsums), so no probe streams x.
     const double* CL;
     int64_t ldcl;
     const double* CQ;
     int64_t ldcq;
+    const double* lam0;  // null-model lambda per phenotype (modes 2-4)
+    double gmid, ginv;   // domain centre and 1 / half-width of the global series
 };
 
 constexpr int kChebN = 25;  // interpolation nodes (degree 24) per bracket
+// Global series of the x-dependent sums: each term 1/(lambda e_i + 1) is analytic in
+// t = log lambda in the strip |Im t| < pi, so over the 23-wide domain a degree-127
+// Chebyshev series converges to ~1e-15 of the sum's scale (Bernstein ellipse rho ~ 1.31).
+constexpr int kChebG = 128;
+constexpr double kDomainLo = 1e-5, kDomainHi = 1e5;
 
 __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -328,50 +338,57 @@ __device__ __forceinline__ double cheb_eval(const double* __restrict__ c, double
     return fma(t, b1, c[0] - b2);
 }
 
-// Mixed-form evaluation inside the golden bracket of grid index `best`: the length-n
-// reduction is restricted to the c+2 genotype-dependent sums; log|H^-1| and the x-free
-// sums (smooth in log lambda, analytic in a strip of half-width pi) come from degree-24
-// Chebyshev expansions over the bracket, built from exact FP64 values at the nodes.
+// Mixed form: the c+2 x-dependent sums at log-lambda `s` from the SNP's global Chebyshev
+// coefficients (chunk GEMM rows 1..kChebG), by Clenshaw's recurrence.  Every lane
+// computes the same values (broadcast loads), so the warp stays uniform.
+template <int C>
+__device__ __forceinline__ void series_xsums(const Params& p, int64_t j, int f, double s,
+                                             double (&xs)[Lay<C>::NX]) {
+    using L = Lay<C>;
+    const int64_t cp = C + p.phi;
+    const double* __restrict__ cl = p.CL + j * p.ldcl;
+    const double* __restrict__ cq = p.CQ + j * p.ldcq;
+    const double tt = (s - p.gmid) * p.ginv;
+    const double t2 = 2.0 * tt;
+    double b1[L::NX], b2[L::NX];
+#pragma unroll
+    for (int q = 0; q < L::NX; ++q) b1[q] = b2[q] = 0.0;
+#pragma unroll 4
+    for (int k = kChebG - 1; k >= 1; --k) {
+        const double* rl = cl + (1 + k) * cp;
+        double c[L::NX];
+#pragma unroll
+        for (int a = 0; a < C; ++a) c[a] = __ldg(rl + a);
+        c[C] = __ldg(cq + 1 + k);
+        c[C + 1] = __ldg(rl + C + f);
+#pragma unroll
+        for (int q = 0; q < L::NX; ++q) {
+            const double b0 = fma(t2, b1[q], c[q] - b2[q]);
+            b2[q] = b1[q];
+            b1[q] = b0;
+        }
+    }
+    const double* rl = cl + cp;
+    double c[L::NX];
+#pragma unroll
+    for (int a = 0; a < C; ++a) c[a] = __ldg(rl + a);
+    c[C] = __ldg(cq + 1);
+    c[C + 1] = __ldg(rl + C + f);
+#pragma unroll
+    for (int q = 0; q < L::NX; ++q) xs[q] = fma(tt, b1[q], c[q] - b2[q]);
+}
+
+// Mixed-form evaluation inside the golden bracket of grid index `best`: the x-dependent
+// sums come from the SNP's global series; log|H^-1| and the x-free sums (smooth in log
+// lambda, analytic in a strip of half-width pi) from degree-24 Chebyshev expansions over
+// the bracket, built from exact FP64 values at the nodes.
 template <int C, bool REML>
-__device__ __forceinline__ double eval_logl_interp(const Params& p, const double* __restrict__ x,
-                                                   const double* __restrict__ y, double log_lam,
+__device__ __forceinline__ double eval_logl_interp(const Params& p, int64_t j, double log_lam,
                                                    int best, int f,
                                                    const double (&iab_diag)[C + 1]) {
     using L = Lay<C>;
-    const double lam = exp(log_lam);
-    double acc[L::NX];
-#pragma unroll
-    for (int k = 0; k < L::NX; ++k) acc[k] = 0.0;
-    const int lane = threadIdx.x & 31;
-    auto step = [&](double ev, double xv, double yv, const double* w) {
-        const double t = __drcp_rn(__dadd_rn(__dmul_rn(lam, ev), 1.0)) * xv;
-#pragma unroll
-        for (int a = 0; a < C; ++a) acc[a] = fma(t, w[a], acc[a]);
-        acc[C] = fma(t, xv, acc[C]);
-        acc[C + 1] = fma(t, yv, acc[C + 1]);
-    };
-    int64_t i = lane;
-    for (; i + 32 * (UNR - 1) < p.n; i += 32 * UNR) {
-        double ev[UNR], xv[UNR], yv[UNR], w[UNR][C > 0 ? C : 1];
-#pragma unroll
-        for (int u = 0; u < UNR; ++u) {
-            ev[u] = __ldg(p.evals + i + 32 * u);
-            xv[u] = x[i + 32 * u];
-            yv[u] = __ldg(y + i + 32 * u);
-#pragma unroll
-            for (int a = 0; a < C; ++a) w[u][a] = __ldg(p.W + a * p.ldw + i + 32 * u);
-        }
-#pragma unroll
-        for (int u = 0; u < UNR; ++u) step(ev[u], xv[u], yv[u], w[u]);
-    }
-    for (; i < p.n; i += 32) {
-        double w[C > 0 ? C : 1];
-#pragma unroll
-        for (int a = 0; a < C; ++a) w[a] = __ldg(p.W + a * p.ldw + i);
-        step(__ldg(p.evals + i), x[i], __ldg(y + i), w);
-    }
-#pragma unroll
-    for (int k = 0; k < L::NX; ++k) acc[k] = warp_sum(acc[k]);
+    double xs[L::NX];
+    series_xsums<C>(p, j, f, log_lam, xs);
     const int nf = 1 + p.phi * L::NS;
     const double* cb = p.cheb + (int64_t)best * nf * kChebN;
     const double tt = (log_lam - p.cheb_mid[best]) / p.cheb_half[best];
@@ -380,20 +397,20 @@ __device__ __forceinline__ double eval_logl_interp(const Params& p, const double
 #pragma unroll
     for (int k = 0; k < L::NS; ++k) shared[k] = cheb_eval(cb + (1 + f * L::NS + k) * kChebN, tt);
     double row0[L::NI];
-    assemble<C>(row0, shared, acc);
+    assemble<C>(row0, shared, xs);
     const PabOut<C> pb = pab_reduce<C>(row0);
     return REML ? reml_logl<C>(pb, iab_diag, logdet, p) : mle_logl<C>(pb, logdet, p);
 }
 
 // Grid bracket + golden section (_golden_section_refine, likelihood_jax.py:419-488).
 template <int C, bool REML, bool INTERP>
-__device__ void golden(const Params& p, const double* x, const double* y, int best, int f,
-                       const double (&iab_diag)[C + 1], double& lam_out, double& logl_out,
+__device__ void golden(const Params& p, int64_t j, const double* x, const double* y, int best,
+                       int f, const double (&iab_diag)[C + 1], double& lam_out, double& logl_out,
                        PabOut<C>& pb_out) {
     const int lo = best - 1 > 0 ? best - 1 : 0;
     const int hi = best + 1 < p.n_grid - 1 ? best + 1 : p.n_grid - 1;
     auto probe = [&](double s) {
-        return INTERP ? eval_logl_interp<C, REML>(p, x, y, s, best, f, iab_diag)
+        return INTERP ? eval_logl_interp<C, REML>(p, j, s, best, f, iab_diag)
                       : eval_logl<C, REML>(p, x, y, s, iab_diag, nullptr);
     };
     double a = p.loglam[lo], b = p.loglam[hi];
@@ -425,6 +442,27 @@ struct ArgMax {
         if (idx < 0) { idx = i; v = x; return; }
         if (isnan(v)) return;
         if (isnan(x) || x > v) { idx = i; v = x; }
+    }
+    // Merge with a partial result over other indices (any order): the lowest-index NaN
+    // if there is one, else the maximum with the lowest index among ties -- the same
+    // pick as pushing every index in increasing order.
+    __device__ void merge(int i, double x) {
+        if (i < 0) return;
+        if (idx < 0) { idx = i; v = x; return; }
+        const bool na = isnan(v), nb = isnan(x);
+        if (na || nb) {
+            if (na && nb ? i < idx : nb) { idx = i; v = x; }
+            return;
+        }
+        if (x > v || (x == v && i < idx)) { idx = i; v = x; }
+    }
+    __device__ void warp_reduce() {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+            const double ov = __shfl_xor_sync(0xffffffffu, v, o);
+            merge(oi, ov);
+        }
     }
 };
 
@@ -471,7 +509,7 @@ __global__ void __launch_bounds__(256) lmm_pairs_kernel(const Params p) {
     for (int i = 0; i <= C; ++i) iab_diag[i] = 0.0;
     if (need_reml) {
         double xs[L::NX], row0[L::NI];
-        row_xsums(p.n_grid, xs);
+        row_xsums(INTERP ? 0 : p.n_grid, xs);
         assemble<C>(row0, p.S + (int64_t)p.n_grid * srow + (int64_t)f * L::NS, xs);
         const PabOut<C> pb = pab_reduce<C>(row0);
 #pragma unroll
@@ -479,7 +517,10 @@ __global__ void __launch_bounds__(256) lmm_pairs_kernel(const Params p) {
     }
     if (need_score) {
         double xs[L::NX], row0[L::NI];
-        row_xsums(p.n_grid + 1 + f, xs);
+        if (INTERP)
+            series_xsums<C>(p, j, f, log(p.lam0[f]), xs);
+        else
+            row_xsums(p.n_grid + 1 + f, xs);
         assemble<C>(row0, p.S + (int64_t)(p.n_grid + 1 + f) * srow + (int64_t)f * L::NS, xs);
         const PabOut<C> pb = pab_reduce<C>(row0);
         bool valid;
@@ -499,21 +540,29 @@ __global__ void __launch_bounds__(256) lmm_pairs_kernel(const Params p) {
 
     // ---------------- phase 2: shared lambda grid
     ArgMax best_reml, best_mle;
-    for (int g = 0; g < p.n_grid; ++g) {
+    // mixed form: lanes take grid points lane, lane+32, ... from the series, then merge
+    for (int g = INTERP ? lane : 0; g < p.n_grid; g += INTERP ? 32 : 1) {
         double xs[L::NX], row0[L::NI];
-        row_xsums(g, xs);
+        if (INTERP)
+            series_xsums<C>(p, j, f, p.loglam[g], xs);
+        else
+            row_xsums(g, xs);
         assemble<C>(row0, p.S + (int64_t)g * srow + (int64_t)f * L::NS, xs);
         const PabOut<C> pb = pab_reduce<C>(row0);
         const double ldh = p.logdet[g];
         if (need_reml) best_reml.push(g, reml_logl<C>(pb, iab_diag, ldh, p));
         if (need_mle) best_mle.push(g, mle_logl<C>(pb, ldh, p));
     }
+    if (INTERP) {
+        best_reml.warp_reduce();
+        best_mle.warp_reduce();
+    }
 
     // ---------------- phase 3: golden sections + statistics
     if (need_mle) {
         double lam, logl;
         PabOut<C> pb;
-        golden<C, false, INTERP>(p, x, y, best_mle.idx, f, iab_diag, lam, logl, pb);
+        golden<C, false, INTERP>(p, j, x, y, best_mle.idx, f, iab_diag, lam, logl, pb);
         if (lane == 0) {
             if (p.out.lambda_mle) p.out.lambda_mle[o] = lam;
             if (p.out.logl_mle) p.out.logl_mle[o] = logl;
@@ -524,7 +573,7 @@ __global__ void __launch_bounds__(256) lmm_pairs_kernel(const Params p) {
     if (need_reml) {
         double lam, logl;
         PabOut<C> pb;
-        golden<C, true, INTERP>(p, x, y, best_reml.idx, f, iab_diag, lam, logl, pb);
+        golden<C, true, INTERP>(p, j, x, y, best_reml.idx, f, iab_diag, lam, logl, pb);
         bool valid;
         double beta, tau, se;
         const double px_yy = clamp_pyy(pb.yy1);
@@ -644,6 +693,48 @@ __global__ void square_cols_kernel(const double* __restrict__ X, int64_t ldx, in
         const int64_t j = t / n, i = t - j * n;
         const double v = X[j * ldx + i];
         X2[t] = v * v;
+    }
+}
+
+// Mixed form, global series over t = log lambda in [lo, hi]: node j of kChebG at
+// t_j = mid + half * cos(pi (j + 1/2) / kChebG); hn[j * n + i] = 1 / (exp(t_j) e_i + 1).
+__global__ void lmm_series_nodes_kernel(int64_t n, double mid, double half,
+                                        const double* __restrict__ evals, double* __restrict__ hn) {
+    const int j = blockIdx.y;
+    const double lam = exp(mid + half * cos(M_PI * (j + 0.5) / kChebG));
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x)
+        hn[(int64_t)j * n + i] = __drcp_rn(__dadd_rn(__dmul_rn(lam, evals[i]), 1.0));
+}
+
+// Chebyshev transform of the node values, column-major kChebG x kChebG:
+// ccos[k + j * kChebG] = (2 / kChebG) cos(pi k (j + 1/2) / kChebG), row k = 0 halved, so
+// coefficient k of any per-sample weight is sum_j ccos[k, j] * value_j.
+__global__ void lmm_series_dct_kernel(double* __restrict__ ccos) {
+    const int j = blockIdx.x, k = threadIdx.x;
+    const double c = (2.0 / kChebG) * cos(M_PI * k * (j + 0.5) / kChebG);
+    ccos[k + (int64_t)j * kChebG] = k == 0 ? 0.5 * c : c;
+}
+
+// GEMM operands of the mixed form: row 0 is the ones row (h = 1), row 1 + k holds the
+// Chebyshev coefficient k of h_i(t) (already in Asq rows 1..kChebG from the transform
+// GEMM); A_lin[r*(C+phi) + a] = Asq[r] * w_a, A_lin[r*(C+phi) + C + f] = Asq[r] * y_f.
+template <int C>
+__global__ void lmm_series_tables_kernel(int64_t n, int phi, const double* __restrict__ W,
+                                         int64_t ldw, const double* __restrict__ Y, int64_t ldy,
+                                         double* __restrict__ Alin, double* __restrict__ Asq) {
+    const int r = blockIdx.x;
+    const int64_t base = (int64_t)r * (C + phi);
+    for (int64_t i = blockIdx.y * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.y * blockDim.x) {
+        double hv = 1.0;
+        if (r == 0)
+            Asq[i] = 1.0;
+        else
+            hv = Asq[(int64_t)r * n + i];
+#pragma unroll
+        for (int a = 0; a < C; ++a) Alin[(base + a) * n + i] = hv * W[a * ldw + i];
+        for (int f = 0; f < phi; ++f) Alin[(base + C + f) * n + i] = hv * Y[(int64_t)f * ldy + i];
     }
 }
 
@@ -841,12 +932,19 @@ __global__ void null_mle_kernel(int64_t n, const double* W, int64_t ldw, const d
 
 // ---------------------------------------------------------------- host helpers
 struct WsLayout {
-    int64_t loglam, logdet, H, S, cheb, cmid, chalf, cvals, alin, asq, total;
+    int64_t loglam, logdet, H, S, cheb, cmid, chalf, cvals, alin, asq, hn, ccos, blas, total;
 };
 
 inline int64_t align256(int64_t b) { return (b + 255) / 256 * 256; }
 
 inline int ns_of(int c) { return (c + 2) * (c + 1) / 2; }
+
+// Table rows of the chunk GEMMs: grid rows + ones row + null rows (FP64 form) or the ones
+// row + kChebG series coefficients (mixed form); sized for whichever is larger.
+inline int64_t table_rows(int phi, int n_grid) {
+    const int64_t direct = (int64_t)n_grid + 1 + phi, series = 1 + kChebG;
+    return direct > series ? direct : series;
+}
 
 inline WsLayout ws_layout(int64_t n, int c, int phi, int n_grid) {
     WsLayout w;
@@ -868,22 +966,28 @@ inline WsLayout ws_layout(int64_t n, int c, int phi, int n_grid) {
     off += align256(8 * (int64_t)n_grid);
     w.cvals = off;
     off += align256(8 * (int64_t)n_grid * nf * kChebN);
-    const int64_t rows = n_grid + 1 + phi;
+    const int64_t rows = table_rows(phi, n_grid);
     w.alin = off;
     off += align256(8 * rows * (c + phi) * n);
     w.asq = off;
     off += align256(8 * rows * n);
+    w.hn = off;
+    off += align256(8 * (int64_t)kChebG * n);
+    w.ccos = off;
+    off += align256(8 * (int64_t)kChebG * kChebG);
+    w.blas = off;
+    off += kCublasWorkspaceBytes;
     w.total = off;
     return w;
 }
 
 struct ChunkLayout {
-    int64_t x2, cl, cq, total;
+    int64_t x2, cl, cq, blas, total;
 };
 
 inline ChunkLayout chunk_layout(int64_t n, int c, int phi, int n_grid, int64_t m) {
     ChunkLayout L;
-    const int64_t rows = n_grid + 1 + phi;
+    const int64_t rows = table_rows(phi, n_grid);
     int64_t off = 0;
     L.x2 = off;
     off += align256(8 * n * m);
@@ -891,6 +995,8 @@ inline ChunkLayout chunk_layout(int64_t n, int c, int phi, int n_grid, int64_t m
     off += align256(8 * rows * (c + phi) * m);
     L.cq = off;
     off += align256(8 * rows * m);
+    L.blas = off;  // cuBLAS workspace of this chunk's DGEMMs (fixed size: same kernels alone or
+    off += kCublasWorkspaceBytes;  // beside other streams' work, so results do not depend on it)
     L.total = off;
     return L;
 }
@@ -937,11 +1043,39 @@ int32_t launch_prepare(int64_t n, int phi, int n_grid, const double* evals, cons
     const int rows_s = n_grid + 1 + (lam0 ? phi : 0);
     lmm_shared_kernel<C><<<dim3(rows_s, phi), 256, 0, st>>>(n, n_grid, phi, W, ldw, Y, ldy, H, S);
     JB_LAUNCH_CHECK("lmm_shared_kernel");
-    lmm_gemm_tables_kernel<C><<<dim3(rows_s, (unsigned)(ceil_div(n, 256) < 64 ? ceil_div(n, 256) : 64)),
-                                256, 0, st>>>(n, n_grid, phi, W, ldw, Y, ldy, H,
-                                              reinterpret_cast<double*>(ws + L.alin),
-                                              reinterpret_cast<double*>(ws + L.asq));
-    JB_LAUNCH_CHECK("lmm_gemm_tables_kernel");
+    const unsigned ny = (unsigned)(ceil_div(n, 256) < 64 ? ceil_div(n, 256) : 64);
+    double* Alin = reinterpret_cast<double*>(ws + L.alin);
+    double* Asq = reinterpret_cast<double*>(ws + L.asq);
+    if (!interp) {
+        lmm_gemm_tables_kernel<C><<<dim3(rows_s, ny), 256, 0, st>>>(n, n_grid, phi, W, ldw, Y, ldy,
+                                                                   H, Alin, Asq);
+        JB_LAUNCH_CHECK("lmm_gemm_tables_kernel");
+    } else {
+        // global series tables: node values -> coefficients (one DGEMM) -> A_lin / A_sq
+        const double lo = std::log(kDomainLo), hi = std::log(kDomainHi);
+        double* hn = reinterpret_cast<double*>(ws + L.hn);
+        double* ccos = reinterpret_cast<double*>(ws + L.ccos);
+        lmm_series_nodes_kernel<<<dim3(ny, kChebG), 256, 0, st>>>(n, 0.5 * (lo + hi), 0.5 * (hi - lo),
+                                                                   evals, hn);
+        JB_LAUNCH_CHECK("lmm_series_nodes_kernel");
+        lmm_series_dct_kernel<<<kChebG, kChebG, 0, st>>>(ccos);
+        JB_LAUNCH_CHECK("lmm_series_dct_kernel");
+        cublasHandle_t h = cublas_handle();
+        if (!h) {
+            set_error("cuBLAS handle creation failed");
+            return JB_E_LIBRARY;
+        }
+        cublasStatus_t cs = bind_cublas(h, st, ws + L.blas, kCublasWorkspaceBytes);
+        if (cs != CUBLAS_STATUS_SUCCESS) return cublas_status(cs, "cublasSetStream/Workspace");
+        const double one = 1.0, zero = 0.0;
+        // (n x K, column-major, ld n) = hn (n x K) * ccos^T: coefficient rows 1..K of Asq
+        cs = cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_T, (int)n, kChebG, kChebG, &one, hn, (int)n,
+                         ccos, kChebG, &zero, Asq + n, (int)n);
+        if (cs != CUBLAS_STATUS_SUCCESS) return cublas_status(cs, "cublasDgemm (series transform)");
+        lmm_series_tables_kernel<C><<<dim3(1 + kChebG, ny), 256, 0, st>>>(n, phi, W, ldw, Y, ldy,
+                                                                         Alin, Asq);
+        JB_LAUNCH_CHECK("lmm_series_tables_kernel");
+    }
     if (interp) {
         const int nf = 1 + phi * Lay<C>::NS;
         double* vals = reinterpret_cast<double*>(ws + L.cvals);
@@ -985,6 +1119,8 @@ int32_t jb_lmm_prepare(int32_t lmm_mode, int32_t precision, int64_t n, int32_t n
     JB_CHECK_ARG(workspace_bytes >= jb_lmm_workspace_size(n, n_cvt, phi, n_grid),
                  "jb_lmm_prepare: workspace too small");
     JB_CHECK_ARG(phi <= 65535, "jb_lmm_prepare: too many phenotypes");
+    JB_CHECK_ARG(precision == 0 || (l_min >= kDomainLo * (1 - 1e-12) && l_max <= kDomainHi * (1 + 1e-12)),
+                 "jb_lmm_prepare: the mixed form needs 1e-5 <= l_min < l_max <= 1e5");
     cudaStream_t st = as_stream(stream);
     uint8_t* ws = static_cast<uint8_t*>(workspace);
     const double* l0 = lmm_mode == 1 ? nullptr : lam0;
@@ -1010,7 +1146,6 @@ int32_t jb_lmm_chunk(int32_t lmm_mode, int32_t precision, int64_t n, int32_t n_c
                      const double* logl0, double l_min, double l_max, int32_t n_grid,
                      int32_t n_iter, jb_lmm_out out, void* workspace, int64_t workspace_bytes,
                      void* chunk_workspace, int64_t chunk_bytes, uintptr_t stream) {
-    (void)lam0;
     JB_CHECK_ARG(lmm_mode >= 1 && lmm_mode <= 4, "jb_lmm_chunk: lmm_mode must be 1..4");
     JB_CHECK_ARG(n > 0 && phi >= 1 && m >= 0 && n_grid >= 2 && n_iter >= 0, "jb_lmm_chunk: bad sizes");
     JB_CHECK_ARG(n_cvt >= 1 && n_cvt <= kMaxCvt, "jb_lmm_chunk: n_cvt must be in 1..%d", kMaxCvt);
@@ -1053,6 +1188,16 @@ int32_t jb_lmm_chunk(int32_t lmm_mode, int32_t precision, int64_t n, int32_t n_c
     p.cheb = precision == 1 ? reinterpret_cast<const double*>(ws + L.cheb) : nullptr;
     p.cheb_mid = reinterpret_cast<const double*>(ws + L.cmid);
     p.cheb_half = reinterpret_cast<const double*>(ws + L.chalf);
+    p.lam0 = lam0;
+    JB_CHECK_ARG(precision == 0 || lmm_mode == 1 || lam0 != nullptr,
+                 "jb_lmm_chunk: the mixed form needs lam0 in modes 2-4");
+    JB_CHECK_ARG(precision == 0 || (l_min >= kDomainLo * (1 - 1e-12) && l_max <= kDomainHi * (1 + 1e-12)),
+                 "jb_lmm_chunk: the mixed form needs 1e-5 <= l_min < l_max <= 1e5");
+    {
+        const double lo = std::log(kDomainLo), hi = std::log(kDomainHi);
+        p.gmid = 0.5 * (lo + hi);
+        p.ginv = 1.0 / (0.5 * (hi - lo));
+    }
     cudaStream_t st = as_stream(stream);
     // chunk GEMMs: weighted x-sums of every table row (grid, ones, null) for all SNPs
     const ChunkLayout CLy = chunk_layout(n, n_cvt, phi, n_grid, m);
@@ -1061,7 +1206,8 @@ int32_t jb_lmm_chunk(int32_t lmm_mode, int32_t precision, int64_t n, int32_t n_c
     double* X2 = reinterpret_cast<double*>(cws + CLy.x2);
     double* CL = reinterpret_cast<double*>(cws + CLy.cl);
     double* CQ = reinterpret_cast<double*>(cws + CLy.cq);
-    const int rows = n_grid + 1 + (lmm_mode == 1 ? 0 : phi);  // null rows only when prepared
+    // FP64 form: grid rows, ones row, null rows (only when prepared); mixed: ones + series
+    const int rows = precision == 1 ? 1 + kChebG : n_grid + 1 + (lmm_mode == 1 ? 0 : phi);
     const int rows_lin = rows * (n_cvt + phi);
     square_cols_kernel<<<(unsigned)(ceil_div(n * m, 256) < 8192 ? ceil_div(n * m, 256) : 8192), 256, 0,
                          st>>>(UtG, ldg, n, m, X2);
@@ -1072,8 +1218,8 @@ int32_t jb_lmm_chunk(int32_t lmm_mode, int32_t precision, int64_t n, int32_t n_c
             set_error("cuBLAS handle creation failed");
             return JB_E_LIBRARY;
         }
-        cublasStatus_t cs = cublasSetStream(h, st);
-        if (cs != CUBLAS_STATUS_SUCCESS) return cublas_status(cs, "cublasSetStream");
+        cublasStatus_t cs = bind_cublas(h, st, cws + CLy.blas, kCublasWorkspaceBytes);
+        if (cs != CUBLAS_STATUS_SUCCESS) return cublas_status(cs, "cublasSetStream/Workspace");
         const double one = 1.0, zero = 0.0;
         cs = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, rows_lin, (int)m, (int)n, &one,
                          reinterpret_cast<const double*>(ws + L.alin), (int)n, UtG, (int)ldg, &zero,

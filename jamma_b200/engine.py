@@ -33,6 +33,8 @@ MAX_CVT = 4
 # The null model always runs with jamma's defaults: compute_null_model_mle is called
 # without the user's lambda range (src/jamma/lmm/prepare.py:143).
 NULL_L_MIN, NULL_L_MAX, NULL_N_GRID, NULL_N_ITER = 1e-5, 1e5, 50, 20
+# log-lambda domain of the mixed form's series tables (jb_lmm_prepare precision 1)
+SERIES_L_MIN, SERIES_L_MAX = 1e-5, 1e5
 
 
 def eigh_device(K: torch.Tensor, threshold: float = 1e-10) -> tuple[torch.Tensor, torch.Tensor]:
@@ -130,9 +132,12 @@ class DeviceCohort:
         self.code_ld = (n + 127) // 128 * 128 if precision == "mixed" else n
         self._rot_ws = None
         self._chunk_ws = None
-        # interpolated golden probes need log|1 + lambda*eval| to stay pole-free
+        # The interpolated search expands 1/(lambda*eval + 1) in log lambda over the fixed
+        # domain [1e-5, 1e5]: it needs the user's range inside that domain and no pole of
+        # the weights near it; otherwise every probe is evaluated directly in FP64.
         ev_min = float(self.evals.min().item())
-        self.search = 1 if (precision == "mixed" and 1.0 + self.l_max * ev_min > 0.5) else 0
+        self.search = 1 if (precision == "mixed" and 1.0 + SERIES_L_MAX * ev_min > 0.5
+                            and self.l_min >= SERIES_L_MIN and self.l_max <= SERIES_L_MAX) else 0
         self.ws = workspace(_native.load().jb_lmm_workspace_size(n, c, phi, self.n_grid))
         _native.call("jb_lmm_prepare", lmm_mode, self.search, n, c, phi, ptr(self.evals), ptr(self.UtW), n,
                      ptr(self.Uty), n, ptr(self.lam0), self.l_min, self.l_max, self.n_grid,

@@ -92,3 +92,14 @@ def test_int8_kinship_with_sample_subset_and_missing(tmp_path):
     k = compute_kinship_from_bed(tmp_path / "s", chunk_size=128, sample_idx=sel, precision="int8")
     ref = OK.centered_kinship(g[sel].astype(np.float32))
     assert np.abs(k - ref).max() <= 1e-10 * np.abs(ref).max()
+
+
+def test_int8_kinship_is_bit_reproducible(tmp_path):
+    """The sparse missing-call correction sums in SNP order, so repeated runs agree bitwise."""
+    from jamma_b200 import compute_kinship_from_bed
+
+    g = synth.genotypes(300, 2600, 0.05, seed=41)
+    OP.write_plink(tmp_path / "r", g)
+    k1 = compute_kinship_from_bed(tmp_path / "r", chunk_size=2600, precision="int8")
+    k2 = compute_kinship_from_bed(tmp_path / "r", chunk_size=2600, precision="int8")
+    np.testing.assert_array_equal(k1, k2)
