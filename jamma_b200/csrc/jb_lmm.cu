@@ -378,41 +378,238 @@ __device__ __forceinline__ void series_xsums(const Params& p, int64_t j, int f, 
     for (int q = 0; q < L::NX; ++q) xs[q] = fma(tt, b1[q], c[q] - b2[q]);
 }
 
-// Mixed-form evaluation inside the golden bracket of grid index `best`: the x-dependent
-// sums come from the SNP's global series; log|H^-1| and the x-free sums (smooth in log
-// lambda, analytic in a strip of half-width pi) from degree-24 Chebyshev expansions over
-// the bracket, built from exact FP64 values at the nodes.
-template <int C, bool REML>
-__device__ __forceinline__ double eval_logl_interp(const Params& p, int64_t j, double log_lam,
-                                                   int best, int f,
-                                                   const double (&iab_diag)[C + 1]) {
+// ---------------------------------------------------------------- warp-cooperative series
+// Chebyshev values for a series summed across the warp: lane l gets T_l(x) (l = 0..31)
+// and every lane T_32(x), by the doubling identity T_{a+b} = 2 T_a T_b - T_{a-b} (round r
+// fills lanes 2^r+1 .. 2^(r+1) from lanes already known).
+__device__ __forceinline__ void lane_cheb(double x, double& tl, double& t32) {
+    const int lane = threadIdx.x & 31;
+    tl = lane == 0 ? 1.0 : x;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+        const int a = 1 << r;
+        const bool act = lane > a && lane <= 2 * a;
+        const double ta = __shfl_sync(0xffffffffu, tl, a);
+        const double tb = __shfl_sync(0xffffffffu, tl, act ? lane - a : 0);
+        const double tc = __shfl_sync(0xffffffffu, tl, act ? 2 * a - lane : 0);
+        if (act) tl = fma(2.0 * ta, tb, -tc);
+    }
+    const double t16 = __shfl_sync(0xffffffffu, tl, 16);
+    t32 = fma(2.0 * t16, t16, -1.0);
+}
+
+// T_k(x) for the kChebG = 128 coefficients a lane owns: k = lane + 32 i, i = 0..3.
+struct LaneT {
+    double t[4];
+};
+__device__ __forceinline__ LaneT lane_cheb_global(double x) {
+    const int lane = threadIdx.x & 31;
+    double tl, t32;
+    lane_cheb(x, tl, t32);
+    const double tm = __shfl_sync(0xffffffffu, tl, (32 - lane) & 31);  // T_{32-l}
+    LaneT r;
+    r.t[0] = tl;
+    r.t[1] = fma(2.0 * t32, tl, -(lane == 0 ? t32 : tm));  // T_{l+32}
+    r.t[2] = fma(2.0 * t32, r.t[1], -r.t[0]);             // T_{l+64}
+    r.t[3] = fma(2.0 * t32, r.t[2], -r.t[1]);             // T_{l+96}
+    return r;
+}
+
+// Per-(SNP, phenotype) coefficients of the global x-sum series, spread over the warp
+// (lane l holds k = l + 32 i of every series), loaded once per SNP.
+template <int C>
+struct GlobalCoef {
+    double c[Lay<C>::NX][4];
+};
+template <int C>
+__device__ __forceinline__ GlobalCoef<C> load_global_coef(const Params& p, int64_t j, int f) {
+    const int lane = threadIdx.x & 31;
+    const int64_t cp = C + p.phi;
+    GlobalCoef<C> g;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int64_t r = 1 + lane + 32 * i;
+        const double* rl = p.CL + j * p.ldcl + r * cp;
+#pragma unroll
+        for (int a = 0; a < C; ++a) g.c[a][i] = __ldg(rl + a);
+        g.c[C][i] = __ldg(p.CQ + j * p.ldcq + r);
+        g.c[C + 1][i] = __ldg(rl + C + f);
+    }
+    return g;
+}
+
+// The c+2 x-dependent sums at log-lambda s; identical bits in every lane.
+template <int C>
+__device__ __forceinline__ void coop_xsums(const Params& p, const GlobalCoef<C>& g, double s,
+                                           double (&xs)[Lay<C>::NX]) {
+    const LaneT T = lane_cheb_global((s - p.gmid) * p.ginv);
+#pragma unroll
+    for (int q = 0; q < Lay<C>::NX; ++q) {
+        double v = g.c[q][0] * T.t[0];
+        v = fma(g.c[q][1], T.t[1], v);
+        v = fma(g.c[q][2], T.t[2], v);
+        v = fma(g.c[q][3], T.t[3], v);
+        xs[q] = warp_sum(v);
+    }
+}
+
+// Per-bracket expansions of log|H^-1| and the x-free sums of phenotype f (degree 24 over
+// the golden bracket of grid index `best`): lane j < kChebN holds coefficient j.
+template <int C>
+struct BracketCoef {
+    double c[1 + Lay<C>::NS];
+    double mid, inv_half;
+};
+template <int C>
+__device__ __forceinline__ BracketCoef<C> load_bracket_coef(const Params& p, int best, int f) {
     using L = Lay<C>;
-    double xs[L::NX];
-    series_xsums<C>(p, j, f, log_lam, xs);
+    const int lane = threadIdx.x & 31;
     const int nf = 1 + p.phi * L::NS;
     const double* cb = p.cheb + (int64_t)best * nf * kChebN;
-    const double tt = (log_lam - p.cheb_mid[best]) / p.cheb_half[best];
-    const double logdet = cheb_eval(cb, tt);
-    double shared[L::NS];
+    BracketCoef<C> b;
+    b.c[0] = lane < kChebN ? __ldg(cb + lane) : 0.0;
 #pragma unroll
-    for (int k = 0; k < L::NS; ++k) shared[k] = cheb_eval(cb + (1 + f * L::NS + k) * kChebN, tt);
+    for (int k = 0; k < L::NS; ++k)
+        b.c[1 + k] = lane < kChebN ? __ldg(cb + (1 + f * L::NS + k) * kChebN + lane) : 0.0;
+    b.mid = p.cheb_mid[best];
+    b.inv_half = 1.0 / p.cheb_half[best];
+    return b;
+}
+
+// log|H^-1| and the x-free sums at log-lambda s inside the bracket; identical bits in
+// every lane.
+template <int C>
+__device__ __forceinline__ void coop_shared(const BracketCoef<C>& b, double s, double& logdet,
+                                            double (&shared)[Lay<C>::NS]) {
+    double tl, t32;
+    lane_cheb((s - b.mid) * b.inv_half, tl, t32);
+    logdet = warp_sum(b.c[0] * tl);
+#pragma unroll
+    for (int k = 0; k < Lay<C>::NS; ++k) shared[k] = warp_sum(b.c[1 + k] * tl);
+}
+
+// Mixed-form log-likelihood at log-lambda s: no length-n pass (series for the x-dependent
+// sums, bracket expansions for the rest).
+template <int C, bool REML>
+__device__ __forceinline__ double coop_logl(const Params& p, const GlobalCoef<C>& g,
+                                            const BracketCoef<C>& b, double s,
+                                            const double (&iab_diag)[C + 1]) {
+    using L = Lay<C>;
+    double xs[L::NX], shared[L::NS], logdet;
+    coop_xsums<C>(p, g, s, xs);
+    coop_shared<C>(b, s, logdet, shared);
     double row0[L::NI];
     assemble<C>(row0, shared, xs);
     const PabOut<C> pb = pab_reduce<C>(row0);
     return REML ? reml_logl<C>(pb, iab_diag, logdet, p) : mle_logl<C>(pb, logdet, p);
 }
 
+// Golden-section refinement (_golden_section_refine, likelihood_jax.py:419-488) on the
+// mixed-form likelihood; returns the optimum's log-lambda (a + b) / 2 and the bracket's
+// expansions for the final evaluation.
+template <int C, bool REML>
+__device__ double golden_coop(const Params& p, const GlobalCoef<C>& g, int best, int f,
+                              const double (&iab_diag)[C + 1], BracketCoef<C>& bc) {
+    const int lo = best - 1 > 0 ? best - 1 : 0;
+    const int hi = best + 1 < p.n_grid - 1 ? best + 1 : p.n_grid - 1;
+    bc = load_bracket_coef<C>(p, best, f);
+    auto probe = [&](double s) { return coop_logl<C, REML>(p, g, bc, s, iab_diag); };
+    double a = p.loglam[lo], b = p.loglam[hi];
+    double c = __dsub_rn(b, __dmul_rn(kPhi, __dsub_rn(b, a)));
+    double d = __dadd_rn(a, __dmul_rn(kPhi, __dsub_rn(b, a)));
+    double fc = probe(c);
+    double fd = probe(d);
+    for (int it = 0; it < p.n_iter; ++it) {
+        const bool keep_left = fc > fd;
+        const double na = keep_left ? a : c;
+        const double nb = keep_left ? d : b;
+        const double nc = __dsub_rn(nb, __dmul_rn(kPhi, __dsub_rn(nb, na)));
+        const double nd = __dadd_rn(na, __dmul_rn(kPhi, __dsub_rn(nb, na)));
+        const double nl = probe(keep_left ? nc : nd);
+        const double nfc = keep_left ? nl : fd;
+        const double nfd = keep_left ? fc : nl;
+        a = na; b = nb; c = nc; d = nd; fc = nfc; fd = nfd;
+    }
+    return __dmul_rn(__dadd_rn(a, b), 0.5);
+}
+
+// Direct FP64 x-dependent sums at two lambdas in one pass over the rotated genotype
+// (the final MLE and REML evaluations share the read of x).
+template <int C>
+__device__ __forceinline__ void direct_xsums2(const Params& p, const double* __restrict__ x,
+                                              const double* __restrict__ y, double lam0,
+                                              double lam1, bool two,
+                                              double (&xs0)[Lay<C>::NX],
+                                              double (&xs1)[Lay<C>::NX]) {
+    using L = Lay<C>;
+    double a0[L::NX], a1[L::NX];
+#pragma unroll
+    for (int k = 0; k < L::NX; ++k) a0[k] = a1[k] = 0.0;
+    const int lane = threadIdx.x & 31;
+    auto step = [&](double ev, double xv, double yv, const double* w) {
+        const double t0 = __drcp_rn(__dadd_rn(__dmul_rn(lam0, ev), 1.0)) * xv;
+#pragma unroll
+        for (int a = 0; a < C; ++a) a0[a] = fma(t0, w[a], a0[a]);
+        a0[C] = fma(t0, xv, a0[C]);
+        a0[C + 1] = fma(t0, yv, a0[C + 1]);
+        if (two) {
+            const double t1 = __drcp_rn(__dadd_rn(__dmul_rn(lam1, ev), 1.0)) * xv;
+#pragma unroll
+            for (int a = 0; a < C; ++a) a1[a] = fma(t1, w[a], a1[a]);
+            a1[C] = fma(t1, xv, a1[C]);
+            a1[C + 1] = fma(t1, yv, a1[C + 1]);
+        }
+    };
+    int64_t i = lane;
+    for (; i + 32 * (UNR - 1) < p.n; i += 32 * UNR) {
+        double ev[UNR], xv[UNR], yv[UNR], w[UNR][C > 0 ? C : 1];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            ev[u] = __ldg(p.evals + i + 32 * u);
+            xv[u] = x[i + 32 * u];
+            yv[u] = __ldg(y + i + 32 * u);
+#pragma unroll
+            for (int a = 0; a < C; ++a) w[u][a] = __ldg(p.W + a * p.ldw + i + 32 * u);
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) step(ev[u], xv[u], yv[u], w[u]);
+    }
+    for (; i < p.n; i += 32) {
+        double w[C > 0 ? C : 1];
+#pragma unroll
+        for (int a = 0; a < C; ++a) w[a] = __ldg(p.W + a * p.ldw + i);
+        step(__ldg(p.evals + i), x[i], __ldg(y + i), w);
+    }
+#pragma unroll
+    for (int k = 0; k < L::NX; ++k) {
+        xs0[k] = warp_sum(a0[k]);
+        xs1[k] = two ? warp_sum(a1[k]) : 0.0;
+    }
+}
+
+// Final mixed-form evaluation at the optimum: direct x-dependent sums, x-free sums and
+// log|H^-1| from the bracket's expansions (exact FP64 node values, ~1e-16 relative).
+template <int C, bool REML>
+__device__ __forceinline__ double final_logl(const Params& p, const double (&xs)[Lay<C>::NX],
+                                             const BracketCoef<C>& bc, double s,
+                                             const double (&iab_diag)[C + 1], PabOut<C>& pb) {
+    using L = Lay<C>;
+    double shared[L::NS], logdet;
+    coop_shared<C>(bc, s, logdet, shared);
+    double row0[L::NI];
+    assemble<C>(row0, shared, xs);
+    pb = pab_reduce<C>(row0);
+    return REML ? reml_logl<C>(pb, iab_diag, logdet, p) : mle_logl<C>(pb, logdet, p);
+}
+
 // Grid bracket + golden section (_golden_section_refine, likelihood_jax.py:419-488).
-template <int C, bool REML, bool INTERP>
-__device__ void golden(const Params& p, int64_t j, const double* x, const double* y, int best,
-                       int f, const double (&iab_diag)[C + 1], double& lam_out, double& logl_out,
+template <int C, bool REML>
+__device__ void golden(const Params& p, const double* x, const double* y, int best,
+                       const double (&iab_diag)[C + 1], double& lam_out, double& logl_out,
                        PabOut<C>& pb_out) {
     const int lo = best - 1 > 0 ? best - 1 : 0;
     const int hi = best + 1 < p.n_grid - 1 ? best + 1 : p.n_grid - 1;
-    auto probe = [&](double s) {
-        return INTERP ? eval_logl_interp<C, REML>(p, j, s, best, f, iab_diag)
-                      : eval_logl<C, REML>(p, x, y, s, iab_diag, nullptr);
-    };
+    auto probe = [&](double s) { return eval_logl<C, REML>(p, x, y, s, iab_diag, nullptr); };
     double a = p.loglam[lo], b = p.loglam[hi];
     double c = __dsub_rn(b, __dmul_rn(kPhi, __dsub_rn(b, a)));
     double d = __dadd_rn(a, __dmul_rn(kPhi, __dsub_rn(b, a)));
@@ -503,6 +700,10 @@ __global__ void __launch_bounds__(256) lmm_pairs_kernel(const Params p) {
         xs[C + 1] = cl[C + f];
     };
 
+    // mixed form: this SNP's global series coefficients, spread over the warp
+    GlobalCoef<C> gc;
+    if (INTERP) gc = load_global_coef<C>(p, j, f);
+
     // ---------------- phase 1: H = 1 (Iab) and H = H0 (score)
     double iab_diag[C + 1];
 #pragma unroll
@@ -518,7 +719,7 @@ __global__ void __launch_bounds__(256) lmm_pairs_kernel(const Params p) {
     if (need_score) {
         double xs[L::NX], row0[L::NI];
         if (INTERP)
-            series_xsums<C>(p, j, f, log(p.lam0[f]), xs);
+            coop_xsums<C>(p, gc, log(p.lam0[f]), xs);
         else
             row_xsums(p.n_grid + 1 + f, xs);
         assemble<C>(row0, p.S + (int64_t)(p.n_grid + 1 + f) * srow + (int64_t)f * L::NS, xs);
@@ -559,30 +760,52 @@ __global__ void __launch_bounds__(256) lmm_pairs_kernel(const Params p) {
     }
 
     // ---------------- phase 3: golden sections + statistics
-    if (need_mle) {
-        double lam, logl;
-        PabOut<C> pb;
-        golden<C, false, INTERP>(p, j, x, y, best_mle.idx, f, iab_diag, lam, logl, pb);
-        if (lane == 0) {
-            if (p.out.lambda_mle) p.out.lambda_mle[o] = lam;
-            if (p.out.logl_mle) p.out.logl_mle[o] = logl;
-            const double stat = jmax(2.0 * (logl - p.logl0[f]), 0.0);
-            if (p.out.p_lrt) p.out.p_lrt[o] = chi2_1_sf(stat);
+    double lam_m = 0.0, logl_m = 0.0, lam_r = 0.0, logl_r = 0.0;
+    PabOut<C> pb_r;
+    if (INTERP) {
+        // both searches first, then one direct pass over x for the two final evaluations
+        BracketCoef<C> bm, br;
+        double s_m = 0.0, s_r = 0.0;
+        if (need_mle) s_m = golden_coop<C, false>(p, gc, best_mle.idx, f, iab_diag, bm);
+        if (need_reml) s_r = golden_coop<C, true>(p, gc, best_reml.idx, f, iab_diag, br);
+        lam_m = exp(s_m);
+        lam_r = exp(s_r);
+        double xm[L::NX], xr[L::NX];
+        if (need_mle && need_reml) {
+            direct_xsums2<C>(p, x, y, lam_m, lam_r, true, xm, xr);
+        } else if (need_mle) {
+            direct_xsums2<C>(p, x, y, lam_m, lam_m, false, xm, xr);
+        } else {
+            direct_xsums2<C>(p, x, y, lam_r, lam_r, false, xr, xm);
         }
+        if (need_mle) {
+            PabOut<C> pb;
+            logl_m = final_logl<C, false>(p, xm, bm, s_m, iab_diag, pb);
+        }
+        if (need_reml) logl_r = final_logl<C, true>(p, xr, br, s_r, iab_diag, pb_r);
+    } else {
+        if (need_mle) {
+            PabOut<C> pb;
+            golden<C, false>(p, x, y, best_mle.idx, iab_diag, lam_m, logl_m, pb);
+        }
+        if (need_reml) golden<C, true>(p, x, y, best_reml.idx, iab_diag, lam_r, logl_r, pb_r);
+    }
+    if (need_mle && lane == 0) {
+        if (p.out.lambda_mle) p.out.lambda_mle[o] = lam_m;
+        if (p.out.logl_mle) p.out.logl_mle[o] = logl_m;
+        const double stat = jmax(2.0 * (logl_m - p.logl0[f]), 0.0);
+        if (p.out.p_lrt) p.out.p_lrt[o] = chi2_1_sf(stat);
     }
     if (need_reml) {
-        double lam, logl;
-        PabOut<C> pb;
-        golden<C, true, INTERP>(p, j, x, y, best_reml.idx, f, iab_diag, lam, logl, pb);
         bool valid;
         double beta, tau, se;
-        const double px_yy = clamp_pyy(pb.yy1);
-        beta_se<C>(pb, px_yy, p.df, valid, beta, tau, se);
-        const double fstat = (pb.yy - px_yy) * tau;
+        const double px_yy = clamp_pyy(pb_r.yy1);
+        beta_se<C>(pb_r, px_yy, p.df, valid, beta, tau, se);
+        const double fstat = (pb_r.yy - px_yy) * tau;
         const double pv = f_pvalue(fstat, p.df, valid);
         if (lane == 0) {
-            if (p.out.lambda_remle) p.out.lambda_remle[o] = lam;
-            if (p.out.logl_h1) p.out.logl_h1[o] = logl;
+            if (p.out.lambda_remle) p.out.lambda_remle[o] = lam_r;
+            if (p.out.logl_h1) p.out.logl_h1[o] = logl_r;
             if (p.out.beta) p.out.beta[o] = beta;
             if (p.out.se) p.out.se[o] = se;
             if (p.out.p_wald) p.out.p_wald[o] = pv;
