@@ -160,6 +160,27 @@ def _config(args, per_step_snps) -> dict:
             "parallelism": f"replicas{_dist()[0]}"}
 
 
+def _accuracy(got: dict, ref: dict) -> dict:
+    """Errors of one form's statistics against another's on the same SNPs: max / median
+    relative error per field; for p-values also the fraction within 1e-6 relative, the
+    max |log10 p| difference and the number of significance calls that differ at 5e-8."""
+    out = {}
+    for k in sorted(got):
+        a, b = np.asarray(got[k]).ravel(), np.asarray(ref[k]).ravel()
+        ok = np.isfinite(a) & np.isfinite(b)
+        rel = np.abs(a[ok] - b[ok]) / np.maximum(np.abs(b[ok]), 1e-300)
+        e = {"max_rel": float(rel.max()) if rel.size else None,
+             "median_rel": float(np.median(rel)) if rel.size else None,
+             "nonfinite_mismatch": int(np.sum(np.isfinite(a) != np.isfinite(b)))}
+        if k.startswith("p_"):
+            e["frac_rel_lt_1e-6"] = float(np.mean(rel < 1e-6)) if rel.size else None
+            e["max_abs_dlog10"] = float(np.max(np.abs(np.log10(a[ok]) - np.log10(b[ok])))) \
+                if rel.size else None
+            e["calls_differ_5e-8"] = int(np.sum((a[ok] < 5e-8) != (b[ok] < 5e-8)))
+        out[k] = e
+    return out
+
+
 def _cpu_baseline(args, cohort, evals_h, U_h, UtW_h, Uty_h, lam0, l0) -> dict:
     """Oracle timed on the host over a bounded sample of the same workload."""
     from threadpoolctl import threadpool_info
@@ -377,6 +398,23 @@ def run_ours(args) -> None:
     ms64, kern64, _, _ = run_form("fp64", fp64_steps)
     value64 = fp64_steps * m * world / (ms64 / 1e3)
 
+    # ---------------- accuracy: mixed form vs the plain FP64 form on the same chunk (untimed)
+    def one_chunk(precision: str, s: int) -> dict:
+        c = cohort_mixed if precision == "mixed" else cohort
+        o = c.alloc_out(m)
+        _native.call("jb_decode_bed", ptr(rec[s * m:(s + 1) * m]), bps, m, None, n, ptr(codes), ld,
+                     ptr(counts), stream_handle())
+        if precision == "mixed":
+            c.rotate_codes_i8(codes, means[s], has_missing, out=UtG)
+        else:
+            _native.call("jb_impute_f64", ptr(codes), ld, n, m, ptr(means[s]), ptr(G), n,
+                         stream_handle())
+            eng.rotate(c.U, G, out=UtG)
+        c.associate_rotated(UtG, o)
+        return {k: v.cpu().numpy() for k, v in o.items()}
+
+    accuracy = _accuracy(one_chunk("mixed", args.warmup), one_chunk("fp64", args.warmup))
+
     # ---------------- end to end through the public chunk API with host buffers (mixed form)
     rec_h = rec[:m].cpu().pin_memory()
     mean_h = means[0].cpu()
@@ -443,6 +481,7 @@ def run_ours(args) -> None:
                          "bound": "tensor", "achieved": achieved, "peak": i8_peak,
                          "unit": "TOP/s", "frac": achieved / i8_peak, "traffic": None,
                          "peak_source": args.int8_peak_source},
+            "accuracy_mixed_vs_fp64_form": {"snps": m, "fields": accuracy},
             "search_kernel": {"kernel": "lmm_pairs_kernel (FP64 search + statistics)",
                               "ms_per_step": kern_ms["lmm"]},
             "cpu_baseline": cpu,

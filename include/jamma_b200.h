@@ -243,14 +243,19 @@ typedef struct jb_lmm_out {
  * src/jamma/lmm/runner_streaming.py:469-554.
  * workspace: jb_lmm_workspace_size bytes, filled by jb_lmm_prepare.
  * chunk_workspace: jb_lmm_chunk_workspace_size(n, n_cvt, phi, n_grid, m) bytes of scratch:
- * the grid, ones and null-model weighted sums of all m SNPs are formed there by two
- * cuBLAS DGEMMs before the per-SNP kernel runs.
- * precision: 0 = every likelihood evaluation is a direct FP64 reduction (plain form);
- * 1 = the golden-section probes take log|H^-1| and the genotype-free weighted sums from
- * per-bracket Chebyshev expansions (degree 24, built by jb_lmm_prepare with precision 1
- * from exact FP64 node values) and reduce only the c+2 genotype-dependent sums over n;
- * grid points, the final evaluation and all statistics stay direct FP64.  Use 1 only
- * when 1 + l_max * min(eval) > 0.5 (no pole of log|1 + lambda eval| near the range).
+ * the weighted genotype sums of all m SNPs are formed there by cuBLAS DGEMMs (or, with
+ * precision 2, partly by jb_lmm_chunk_series_i8) before the per-SNP kernel runs.
+ * precision: 0 = every likelihood evaluation is a direct FP64 reduction over n (plain
+ * form; grid, ones and null rows by DGEMM);
+ * 1 = mixed form: the c+2 genotype-dependent sums are a degree-127 Chebyshev series in
+ * log lambda over [1e-5, 1e5] whose coefficients come from the chunk DGEMMs; log|H^-1|
+ * and the genotype-free sums come from per-bracket degree-24 expansions of exact FP64
+ * node values (both built by jb_lmm_prepare with precision 1); grid points and golden
+ * probes read these series, the final evaluation at each optimum reduces the genotype
+ * sums directly in FP64.  Needs 1e-5 <= l_min < l_max <= 1e5 and
+ * 1 + 1e5 * min(eval) > 0.5 (no pole of 1/(lambda eval + 1) near the domain);
+ * 2 = as 1, with the linear series sums already placed in chunk_workspace by
+ * jb_lmm_chunk_series_i8 for the same chunk (only the squared sums use a DGEMM).
  */
 int64_t jb_lmm_workspace_size(int64_t n, int32_t n_cvt, int32_t phi, int32_t n_grid);
 
@@ -277,6 +282,36 @@ int32_t jb_lmm_chunk(int32_t lmm_mode, int32_t precision, int64_t n, int32_t n_c
                      int32_t n_grid, int32_t n_iter, jb_lmm_out out, void* workspace,
                      int64_t workspace_bytes, void* chunk_workspace, int64_t chunk_bytes,
                      uintptr_t stream);
+
+/*
+ * Mixed form, genotype-side linear sums (no reference counterpart: an evaluation order
+ * of the sums in likelihood_jax.py:148-186).  The weighted sums sum_i h_i(lambda) x_i v_i
+ * of the rotated genotype x = U^T g are linear in g, so with the series tables A_lin of a
+ * workspace prepared by jb_lmm_prepare(precision 1) the basis V = U A_lin^T is formed once
+ * (one DGEMM) and split into INT8 digit planes like the eigenvectors
+ * (jb_ozaki_prepare); every chunk then obtains the linear sums from the int8 calls on the
+ * tcgen05 rotation core.  U: column-major eigenvectors (ldu >= n).
+ * series_ws: jb_lmm_series_workspace_size(n, n_cvt, phi) bytes, kept per cohort and
+ * phenotype set (it depends on W and y).
+ */
+int64_t jb_lmm_series_workspace_size(int64_t n, int32_t n_cvt, int32_t phi);
+int32_t jb_lmm_series_prepare(int64_t n, int32_t n_cvt, int32_t phi, int32_t n_grid,
+                              const void* workspace, int64_t workspace_bytes, const double* U,
+                              int64_t ldu, void* series_ws, int64_t series_bytes,
+                              uintptr_t stream);
+
+/*
+ * Per chunk, after jb_rotate_i8 ran on the same codes with rot_ws on the same stream
+ * (its packed [calls | masks] operand and tile list are reused; errors go to the same
+ * status word, read by jb_rotate_status): write the chunk's linear series sums into
+ * chunk_workspace, then call jb_lmm_chunk with precision 2.  codes / mean / has_missing
+ * as for jb_rotate_i8.
+ */
+int32_t jb_lmm_chunk_series_i8(int64_t n, int32_t n_cvt, int32_t phi, int32_t n_grid, int64_t m,
+                               const void* series_ws, int64_t series_bytes, const int8_t* codes,
+                               int64_t ld_codes, const double* mean, int32_t has_missing,
+                               void* rot_ws, int64_t rot_bytes, void* chunk_workspace,
+                               int64_t chunk_bytes, uintptr_t stream);
 
 /*
  * Null-model MLE (lambda0, logl_H0) per phenotype on the device: the scalar 50-point

@@ -17,6 +17,7 @@
 // src/jamma/lmm/likelihood_jax.py (148-339 likelihoods, 419-598 search, 601-798
 // statistics) exactly; only the summation order of the length-n reductions differs.
 #include "jb_common.cuh"
+#include "jb_rotate_i8.cuh"
 
 #include <cmath>
 
@@ -1224,6 +1225,27 @@ inline ChunkLayout chunk_layout(int64_t n, int c, int phi, int n_grid, int64_t m
     return L;
 }
 
+// Mixed form, genotype-side linear x-sums: the chunk GEMM  CL = A_lin x~  with x~ = U^T g
+// equals  (U A_lin^T)^T g, so the basis  V = U A_lin^T  (n x rows_lin, column q = basis of
+// CL row q) is formed once per cohort and split into INT8 digit planes; every chunk then
+// gets CL from the decoded calls on the INT8 rotation core (V has rows_lin ~ 1 % of U's n
+// columns), instead of an FP64 DGEMM over the rotated chunk.
+struct SeriesLayout {
+    int64_t rows_lin, basis, ozaki, total;
+};
+
+inline SeriesLayout series_layout(int64_t n, int c, int phi) {
+    SeriesLayout L;
+    L.rows_lin = (int64_t)(1 + kChebG) * (c + phi);
+    int64_t off = 0;
+    L.basis = off;
+    off += align256(8 * n * L.rows_lin);
+    L.ozaki = off;
+    off += align256(tc::ozaki_layout(L.rows_lin, n).total);
+    L.total = off;
+    return L;
+}
+
 // numpy.linspace(start, stop, num): start + i*step, last element = stop.
 __global__ void linspace_kernel(double* out, double start, double stop, int num) {
     const int i = threadIdx.x + blockIdx.x * blockDim.x;
@@ -1362,6 +1384,75 @@ int64_t jb_lmm_chunk_workspace_size(int64_t n, int32_t n_cvt, int32_t phi, int32
     return chunk_layout(n, n_cvt, phi, n_grid, m > 0 ? m : 1).total;
 }
 
+int64_t jb_lmm_series_workspace_size(int64_t n, int32_t n_cvt, int32_t phi) {
+    if (n <= 0 || n_cvt < 1 || n_cvt > kMaxCvt || phi < 1) return -1;
+    return series_layout(n, n_cvt, phi).total;
+}
+
+int32_t jb_lmm_series_prepare(int64_t n, int32_t n_cvt, int32_t phi, int32_t n_grid,
+                              const void* workspace, int64_t workspace_bytes, const double* U,
+                              int64_t ldu, void* series_ws, int64_t series_bytes,
+                              uintptr_t stream) {
+    JB_CHECK_ARG(n > 0 && n_cvt >= 1 && n_cvt <= kMaxCvt && phi >= 1 && n_grid >= 2,
+                 "jb_lmm_series_prepare: bad sizes");
+    JB_CHECK_ARG(U && ldu >= n, "jb_lmm_series_prepare: bad eigenvector matrix");
+    JB_CHECK_ARG(workspace && workspace_bytes >= jb_lmm_workspace_size(n, n_cvt, phi, n_grid),
+                 "jb_lmm_series_prepare: workspace too small");
+    const SeriesLayout SL = series_layout(n, n_cvt, phi);
+    JB_CHECK_ARG(series_ws && series_bytes >= SL.total, "jb_lmm_series_prepare: series workspace too small");
+    JB_CHECK_ARG(SL.rows_lin <= 65535, "jb_lmm_series_prepare: too many phenotypes");
+    const WsLayout L = ws_layout(n, n_cvt, phi, n_grid);
+    uint8_t* ws = const_cast<uint8_t*>(static_cast<const uint8_t*>(workspace));
+    uint8_t* sws = static_cast<uint8_t*>(series_ws);
+    cudaStream_t st = as_stream(stream);
+    cublasHandle_t h = cublas_handle();
+    if (!h) {
+        set_error("cuBLAS handle creation failed");
+        return JB_E_LIBRARY;
+    }
+    cublasStatus_t cs = bind_cublas(h, st, ws + L.blas, kCublasWorkspaceBytes);
+    if (cs != CUBLAS_STATUS_SUCCESS) return cublas_status(cs, "cublasSetStream/Workspace");
+    const double one = 1.0, zero = 0.0;
+    double* V = reinterpret_cast<double*>(sws + SL.basis);
+    // V (n x rows_lin) = U (n x n) * A_lin^T, A_lin stored as rows of n (column-major n x rows_lin)
+    cs = cublasDgemm(h, CUBLAS_OP_N, CUBLAS_OP_N, (int)n, (int)SL.rows_lin, (int)n, &one, U, (int)ldu,
+                     reinterpret_cast<const double*>(ws + L.alin), (int)n, &zero, V, (int)n);
+    if (cs != CUBLAS_STATUS_SUCCESS) return cublas_status(cs, "cublasDgemm (series basis)");
+    return tc::ozaki_split(V, n, SL.rows_lin, n, sws + SL.ozaki, st);
+}
+
+int32_t jb_lmm_chunk_series_i8(int64_t n, int32_t n_cvt, int32_t phi, int32_t n_grid, int64_t m,
+                               const void* series_ws, int64_t series_bytes, const int8_t* codes,
+                               int64_t ld_codes, const double* mean, int32_t has_missing,
+                               void* rot_ws, int64_t rot_bytes, void* chunk_workspace,
+                               int64_t chunk_bytes, uintptr_t stream) {
+    JB_CHECK_ARG(n > 0 && n_cvt >= 1 && n_cvt <= kMaxCvt && phi >= 1 && n_grid >= 2 && m >= 0,
+                 "jb_lmm_chunk_series_i8: bad sizes");
+    if (m == 0) return JB_OK;
+    const SeriesLayout SL = series_layout(n, n_cvt, phi);
+    JB_CHECK_ARG(series_ws && series_bytes >= SL.total, "jb_lmm_chunk_series_i8: series workspace too small");
+    const tc::RotChunkLayout RL = tc::rot_chunk_layout(n, m);
+    JB_CHECK_ARG(rot_ws && rot_bytes >= RL.total, "jb_lmm_chunk_series_i8: rotation workspace too small");
+    JB_CHECK_ARG(ceil_div(SL.rows_lin, 32) <= ceil_div(n, 32),
+                 "jb_lmm_chunk_series_i8: more series rows than samples");
+    JB_CHECK_ARG(codes && ld_codes >= n && (!has_missing || mean), "jb_lmm_chunk_series_i8: bad genotype input");
+    const ChunkLayout CLy = chunk_layout(n, n_cvt, phi, n_grid, m);
+    JB_CHECK_ARG(chunk_workspace && chunk_bytes >= CLy.total, "jb_lmm_chunk_series_i8: chunk workspace too small");
+    uint8_t* rws = static_cast<uint8_t*>(rot_ws);
+    double* CL = reinterpret_cast<double*>(static_cast<uint8_t*>(chunk_workspace) + CLy.cl);
+    const uint8_t* ows = static_cast<const uint8_t*>(series_ws) + SL.ozaki;
+    tc::Tile* tiles = reinterpret_cast<tc::Tile*>(rws + RL.tiles);
+    int* status = reinterpret_cast<int*>(rws + RL.status);
+    cudaStream_t st = as_stream(stream);
+    if (has_missing) {  // the [calls | masks] pairs packed by jb_rotate_i8 for these codes
+        const int64_t NB = ceil_div(m, 128);
+        return tc::rotate_i8_gemm(ows, SL.rows_lin, n, reinterpret_cast<const int8_t*>(rws + RL.b_off),
+                                  NB * 256, RL.ldb, true, m, mean, CL, SL.rows_lin, tiles, status, st);
+    }
+    return tc::rotate_i8_gemm(ows, SL.rows_lin, n, codes, m, ld_codes, false, m, nullptr, CL,
+                              SL.rows_lin, tiles, status, st);
+}
+
 int32_t jb_lmm_chunk(int32_t lmm_mode, int32_t precision, int64_t n, int32_t n_cvt, int32_t phi,
                      int64_t m,
                      const double* evals, const double* UtW, int64_t ldw, const double* Uty,
@@ -1407,8 +1498,8 @@ int32_t jb_lmm_chunk(int32_t lmm_mode, int32_t precision, int64_t n, int32_t n_c
     p.c_reml = 0.5 * df * (std::log(df) - std::log(2 * M_PI) - 1.0);
     p.c_mle = 0.5 * (double)n * (std::log((double)n) - std::log(2 * M_PI) - 1.0);
     p.out = out;
-    JB_CHECK_ARG(precision == 0 || precision == 1, "jb_lmm_chunk: precision must be 0 or 1");
-    p.cheb = precision == 1 ? reinterpret_cast<const double*>(ws + L.cheb) : nullptr;
+    JB_CHECK_ARG(precision >= 0 && precision <= 2, "jb_lmm_chunk: precision must be 0, 1 or 2");
+    p.cheb = precision >= 1 ? reinterpret_cast<const double*>(ws + L.cheb) : nullptr;
     p.cheb_mid = reinterpret_cast<const double*>(ws + L.cmid);
     p.cheb_half = reinterpret_cast<const double*>(ws + L.chalf);
     p.lam0 = lam0;
@@ -1430,7 +1521,7 @@ int32_t jb_lmm_chunk(int32_t lmm_mode, int32_t precision, int64_t n, int32_t n_c
     double* CL = reinterpret_cast<double*>(cws + CLy.cl);
     double* CQ = reinterpret_cast<double*>(cws + CLy.cq);
     // FP64 form: grid rows, ones row, null rows (only when prepared); mixed: ones + series
-    const int rows = precision == 1 ? 1 + kChebG : n_grid + 1 + (lmm_mode == 1 ? 0 : phi);
+    const int rows = precision >= 1 ? 1 + kChebG : n_grid + 1 + (lmm_mode == 1 ? 0 : phi);
     const int rows_lin = rows * (n_cvt + phi);
     square_cols_kernel<<<(unsigned)(ceil_div(n * m, 256) < 8192 ? ceil_div(n * m, 256) : 8192), 256, 0,
                          st>>>(UtG, ldg, n, m, X2);
@@ -1444,10 +1535,12 @@ int32_t jb_lmm_chunk(int32_t lmm_mode, int32_t precision, int64_t n, int32_t n_c
         cublasStatus_t cs = bind_cublas(h, st, cws + CLy.blas, kCublasWorkspaceBytes);
         if (cs != CUBLAS_STATUS_SUCCESS) return cublas_status(cs, "cublasSetStream/Workspace");
         const double one = 1.0, zero = 0.0;
-        cs = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, rows_lin, (int)m, (int)n, &one,
-                         reinterpret_cast<const double*>(ws + L.alin), (int)n, UtG, (int)ldg, &zero,
-                         CL, rows_lin);
-        if (cs != CUBLAS_STATUS_SUCCESS) return cublas_status(cs, "cublasDgemm (linear x-sums)");
+        if (precision != 2) {  // precision 2: CL already formed by jb_lmm_chunk_series_i8
+            cs = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, rows_lin, (int)m, (int)n, &one,
+                             reinterpret_cast<const double*>(ws + L.alin), (int)n, UtG, (int)ldg,
+                             &zero, CL, rows_lin);
+            if (cs != CUBLAS_STATUS_SUCCESS) return cublas_status(cs, "cublasDgemm (linear x-sums)");
+        }
         cs = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, rows, (int)m, (int)n, &one,
                          reinterpret_cast<const double*>(ws + L.asq), (int)n, X2, (int)n, &zero, CQ,
                          rows);

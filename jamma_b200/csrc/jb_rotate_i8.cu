@@ -18,6 +18,7 @@
 // exchange their FP64 digit contributions through shared memory.
 #include "jb_common.cuh"
 #include "jb_gemm_i8.cuh"
+#include "jb_rotate_i8.cuh"
 
 namespace jb {
 namespace tc {
@@ -181,25 +182,20 @@ __global__ void rot_tiles_kernel(int MB, int NB, Tile* out) {
 using namespace jb;
 using namespace jb::tc;
 
-namespace {
+namespace jb {
+namespace tc {
 using RotSmem = GemmSmem<kRotBN, kRotStages, kRotEpiSmem>;
 
-struct OzakiLayout {
-    int64_t lda, rows, a_off, s_off, total;
-};
-OzakiLayout ozaki_layout(int64_t n) {
+OzakiLayout ozaki_layout(int64_t n_out, int64_t n_k) {
     OzakiLayout L;
-    L.lda = (n + 127) / 128 * 128;
-    L.rows = ceil_div(n, 32) * 128;
+    L.lda = (n_k + 127) / 128 * 128;
+    L.rows = ceil_div(n_out, 32) * 128;
     L.a_off = 0;
     L.s_off = ((L.rows * L.lda + 255) / 256) * 256;
-    L.total = L.s_off + ((n * 8 + 255) / 256) * 256;
+    L.total = L.s_off + ((n_out * 8 + 255) / 256) * 256;
     return L;
 }
 
-struct RotChunkLayout {
-    int64_t status, tiles, b_off, ldb, total;
-};
 RotChunkLayout rot_chunk_layout(int64_t n, int64_t m) {
     RotChunkLayout L;
     L.ldb = (n + 127) / 128 * 128;
@@ -210,32 +206,73 @@ RotChunkLayout rot_chunk_layout(int64_t n, int64_t m) {
     L.total = L.b_off + NB * 256 * L.ldb;
     return L;
 }
-}  // namespace
+
+int32_t ozaki_split(const double* V, int64_t n_k, int64_t n_out, int64_t ldv, uint8_t* ws,
+                    cudaStream_t st) {
+    const OzakiLayout L = ozaki_layout(n_out, n_k);
+    double* smax = reinterpret_cast<double*>(ws + L.s_off);
+    int8_t* A = reinterpret_cast<int8_t*>(ws + L.a_off);
+    // rows of column blocks past n_out and K padding stay zero
+    JB_CUDA(cudaMemsetAsync(A, 0, (size_t)(L.rows * L.lda), st));
+    ozaki_scale_kernel<<<(unsigned)n_out, 256, 0, st>>>(V, n_k, ldv, smax);
+    JB_LAUNCH_CHECK("ozaki_scale_kernel");
+    ozaki_split_kernel<<<(unsigned)n_out, 256, 0, st>>>(V, n_k, ldv, smax, A, L.lda);
+    JB_LAUNCH_CHECK("ozaki_split_kernel");
+    return JB_OK;
+}
+
+int32_t rotate_i8_gemm(const uint8_t* ozaki_ws, int64_t n_out, int64_t n_k, const int8_t* B,
+                       int64_t b_rows, int64_t ldb, bool paired, int64_t m, const double* mean,
+                       double* X, int64_t ldx, Tile* tiles, int* status, cudaStream_t st) {
+    const OzakiLayout OL = ozaki_layout(n_out, n_k);
+    const int8_t* A = reinterpret_cast<const int8_t*>(ozaki_ws + OL.a_off);
+    const double* smax = reinterpret_cast<const double*>(ozaki_ws + OL.s_off);
+    const int MB = (int)ceil_div(n_out, 32);
+    const int NB = (int)ceil_div(m, paired ? 128 : 256);
+    const int n_tiles = MB * NB;
+    CUtensorMap ta, tb;
+    int32_t rc = make_map_i8(&ta, A, OL.rows, n_k, OL.lda, kBM);
+    if (rc) return rc;
+    rc = make_map_i8(&tb, B, b_rows, n_k, ldb, kRotBN);
+    if (rc) return rc;
+    rot_tiles_kernel<<<(unsigned)ceil_div((int64_t)n_tiles, 256), 256, 0, st>>>(MB, NB, tiles);
+    JB_LAUNCH_CHECK("rot_tiles_kernel");
+    const int grid = n_tiles < num_sms() ? n_tiles : num_sms();
+    const int num_kb = (int)ceil_div(n_k, kBK);
+    if (paired) {
+        auto kern = i8_gemm_kernel<kRotBN, kRotStages, RotEpi<true>>;
+        JB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     RotSmem::TOTAL));
+        RotEpi<true> epi{X, ldx, smax, mean, (int)n_out, (int)m};
+        kern<<<grid, kThreads, RotSmem::TOTAL, st>>>(ta, tb, tiles, n_tiles, num_kb, epi, status);
+    } else {
+        auto kern = i8_gemm_kernel<kRotBN, kRotStages, RotEpi<false>>;
+        JB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     RotSmem::TOTAL));
+        RotEpi<false> epi{X, ldx, smax, nullptr, (int)n_out, (int)m};
+        kern<<<grid, kThreads, RotSmem::TOTAL, st>>>(ta, tb, tiles, n_tiles, num_kb, epi, status);
+    }
+    JB_LAUNCH_CHECK("i8_gemm_kernel<rotate>");
+    return JB_OK;
+}
+
+}  // namespace tc
+}  // namespace jb
 
 extern "C" {
 
 int64_t jb_ozaki_workspace_size(int64_t n) {
     if (n <= 0) return -1;
-    return ozaki_layout(n).total;
+    return ozaki_layout(n, n).total;
 }
 
 int32_t jb_ozaki_prepare(const double* U, int64_t n, int64_t ldu, void* ozaki_ws,
                          int64_t ozaki_bytes, uintptr_t stream) {
     JB_CHECK_ARG(n > 0 && ldu >= n && U, "jb_ozaki_prepare: bad arguments");
     JB_CHECK_ARG(n < (1ll << 31), "jb_ozaki_prepare: n too large");
-    const OzakiLayout L = ozaki_layout(n);
+    const OzakiLayout L = ozaki_layout(n, n);
     JB_CHECK_ARG(ozaki_ws && ozaki_bytes >= L.total, "jb_ozaki_prepare: workspace too small");
-    uint8_t* ws = static_cast<uint8_t*>(ozaki_ws);
-    cudaStream_t st = as_stream(stream);
-    double* smax = reinterpret_cast<double*>(ws + L.s_off);
-    int8_t* A = reinterpret_cast<int8_t*>(ws + L.a_off);
-    // rows of eigenvector blocks past n stay zero
-    JB_CUDA(cudaMemsetAsync(A, 0, (size_t)(L.rows * L.lda), st));
-    ozaki_scale_kernel<<<(unsigned)n, 256, 0, st>>>(U, n, ldu, smax);
-    JB_LAUNCH_CHECK("ozaki_scale_kernel");
-    ozaki_split_kernel<<<(unsigned)n, 256, 0, st>>>(U, n, ldu, smax, A, L.lda);
-    JB_LAUNCH_CHECK("ozaki_split_kernel");
-    return JB_OK;
+    return ozaki_split(U, n, n, ldu, static_cast<uint8_t*>(ozaki_ws), as_stream(stream));
 }
 
 int64_t jb_rotate_i8_workspace_size(int64_t n, int64_t m) {
@@ -251,7 +288,6 @@ int32_t jb_rotate_i8(const void* ozaki_ws, int64_t n, const int8_t* codes, int64
     if (m == 0) return JB_OK;
     JB_CHECK_ARG(ozaki_ws && codes && X, "jb_rotate_i8: null pointer");
     JB_CHECK_ARG(!has_missing || mean, "jb_rotate_i8: mean needed when calls are missing");
-    const OzakiLayout OL = ozaki_layout(n);
     const RotChunkLayout L = rot_chunk_layout(n, m);
     JB_CHECK_ARG(workspace && workspace_bytes >= L.total, "jb_rotate_i8: workspace too small");
     cudaStream_t st = as_stream(stream);
@@ -259,46 +295,18 @@ int32_t jb_rotate_i8(const void* ozaki_ws, int64_t n, const int8_t* codes, int64
     int* status = reinterpret_cast<int*>(ws + L.status);
     Tile* tiles = reinterpret_cast<Tile*>(ws + L.tiles);
     const uint8_t* ows = static_cast<const uint8_t*>(ozaki_ws);
-    const int8_t* A = reinterpret_cast<const int8_t*>(ows + OL.a_off);
-    const double* smax = reinterpret_cast<const double*>(ows + OL.s_off);
-
-    const int MB = (int)ceil_div(n, 32);
-    const int cols = has_missing ? 128 : 256;
-    const int NB = (int)ceil_div(m, cols);
-    const int n_tiles = MB * NB;
-    CUtensorMap ta, tb;
-    int32_t rc = make_map_i8(&ta, A, OL.rows, n, OL.lda, kBM);
-    if (rc) return rc;
+    const int NB = (int)ceil_div(m, has_missing ? 128 : 256);
+    JB_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
     if (has_missing) {
         int8_t* B = reinterpret_cast<int8_t*>(ws + L.b_off);
         rot_pack_pairs_kernel<<<(unsigned)(NB * 128), 256, 0, st>>>(codes, ld_codes, n, m, B, L.ldb);
         JB_LAUNCH_CHECK("rot_pack_pairs_kernel");
-        rc = make_map_i8(&tb, B, (int64_t)NB * 256, n, L.ldb, kRotBN);
-    } else {
-        // no missing calls: the decoded codes are the calls themselves
-        rc = make_map_i8(&tb, codes, m, n, ld_codes, kRotBN);
+        return rotate_i8_gemm(ows, n, n, B, (int64_t)NB * 256, L.ldb, true, m, mean, X, ldx, tiles,
+                              status, st);
     }
-    if (rc) return rc;
-    JB_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
-    rot_tiles_kernel<<<(unsigned)ceil_div((int64_t)n_tiles, 256), 256, 0, st>>>(MB, NB, tiles);
-    JB_LAUNCH_CHECK("rot_tiles_kernel");
-    const int grid = n_tiles < num_sms() ? n_tiles : num_sms();
-    const int num_kb = (int)ceil_div(n, kBK);
-    if (has_missing) {
-        auto kern = i8_gemm_kernel<kRotBN, kRotStages, RotEpi<true>>;
-        JB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     RotSmem::TOTAL));
-        RotEpi<true> epi{X, ldx, smax, mean, (int)n, (int)m};
-        kern<<<grid, kThreads, RotSmem::TOTAL, st>>>(ta, tb, tiles, n_tiles, num_kb, epi, status);
-    } else {
-        auto kern = i8_gemm_kernel<kRotBN, kRotStages, RotEpi<false>>;
-        JB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     RotSmem::TOTAL));
-        RotEpi<false> epi{X, ldx, smax, nullptr, (int)n, (int)m};
-        kern<<<grid, kThreads, RotSmem::TOTAL, st>>>(ta, tb, tiles, n_tiles, num_kb, epi, status);
-    }
-    JB_LAUNCH_CHECK("i8_gemm_kernel<rotate>");
-    return JB_OK;
+    // no missing calls: the decoded codes are the calls themselves
+    return rotate_i8_gemm(ows, n, n, codes, m, ld_codes, false, m, nullptr, X, ldx, tiles, status,
+                          st);
 }
 
 int32_t jb_rotate_status(const void* workspace, int32_t* out, uintptr_t stream) {

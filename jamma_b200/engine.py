@@ -35,6 +35,7 @@ MAX_CVT = 4
 NULL_L_MIN, NULL_L_MAX, NULL_N_GRID, NULL_N_ITER = 1e-5, 1e5, 50, 20
 # log-lambda domain of the mixed form's series tables (jb_lmm_prepare precision 1)
 SERIES_L_MIN, SERIES_L_MAX = 1e-5, 1e5
+SERIES_ROWS = 1 + 128  # ones row + Chebyshev coefficients per linear sum
 
 
 def eigh_device(K: torch.Tensor, threshold: float = 1e-10) -> tuple[torch.Tensor, torch.Tensor]:
@@ -142,6 +143,14 @@ class DeviceCohort:
         _native.call("jb_lmm_prepare", lmm_mode, self.search, n, c, phi, ptr(self.evals), ptr(self.UtW), n,
                      ptr(self.Uty), n, ptr(self.lam0), self.l_min, self.l_max, self.n_grid,
                      ptr(self.ws), self.ws.numel(), st)
+        # Mixed form with the series search: the linear genotype sums of each chunk come
+        # from the int8 calls (basis U A_lin^T split into digit planes once per cohort).
+        self.series_ws = None
+        self._series_for = None
+        if self.search == 1 and SERIES_ROWS * (c + phi) <= (n + 31) // 32 * 32:
+            self.series_ws = workspace(_native.load().jb_lmm_series_workspace_size(n, c, phi))
+            _native.call("jb_lmm_series_prepare", n, c, phi, self.n_grid, ptr(self.ws), self.ws.numel(),
+                         ptr(self.U), n, ptr(self.series_ws), self.series_ws.numel(), st)
 
     # ------------------------------------------------------------ null model
     def null_model(self) -> tuple[np.ndarray | None, np.ndarray | None]:
@@ -165,7 +174,11 @@ class DeviceCohort:
         out = out if out is not None else self.alloc_out(m)
         o = _native.LmmOut(**{k: ptr(out.get(k)) for k in OUT_KEYS})
         cws = self.chunk_workspace(m)
-        _native.call("jb_lmm_chunk", self.mode, self.search, self.n, self.c, self.phi, m,
+        precision = self.search
+        if self._series_for is not None and self._series_for == (m, UtG.data_ptr()):
+            precision = 2  # linear sums already formed from this chunk's int8 calls
+        self._series_for = None
+        _native.call("jb_lmm_chunk", self.mode, precision, self.n, self.c, self.phi, m,
                      ptr(self.evals),
                      ptr(self.UtW), self.n, ptr(self.Uty), self.n, ptr(UtG), self.n,
                      ptr(self.lam0), ptr(self.logl0), self.l_min, self.l_max, self.n_grid,
@@ -190,6 +203,14 @@ class DeviceCohort:
         _native.call("jb_rotate_i8", ptr(self.ozaki), self.n, ptr(codes), ld, m, ptr(means),
                      int(bool(has_missing)), ptr(out), self.n, ptr(self._rot_ws),
                      self._rot_ws.numel(), stream_handle())
+        self._series_for = None
+        if self.series_ws is not None:
+            cws = self.chunk_workspace(m)
+            _native.call("jb_lmm_chunk_series_i8", self.n, self.c, self.phi, self.n_grid, m,
+                         ptr(self.series_ws), self.series_ws.numel(), ptr(codes), ld, ptr(means),
+                         int(bool(has_missing)), ptr(self._rot_ws), self._rot_ws.numel(), ptr(cws),
+                         cws.numel(), stream_handle())
+            self._series_for = (m, out.data_ptr())
         return out
 
     def rotate_status(self) -> int:

@@ -75,6 +75,7 @@ def job_device_bytes(n: int, phi: int, n_cvt: int, chunk: int, resident: bool) -
         n, n_cvt, phi, 50, chunk)
     b += lib.jb_rotate_i8_workspace_size(n, chunk) + chunk * n * 8 + chunk * ((n + 127) // 128 * 128)
     b += 9 * phi * chunk * 8 + 2 * n * (n_cvt + phi) * 8
+    b += lib.jb_lmm_series_workspace_size(n, n_cvt, phi)
     if not resident:
         b += 8 * n * n * 2 + lib.jb_ozaki_workspace_size(n) + n * 8  # K / U, digits, evals
     return int(b)

@@ -146,3 +146,37 @@ def test_mixed_association_matches_oracle(mode, tmp_path):
     beta = np.array([r.beta for r in res])
     relb = np.abs(beta - ref.stats["beta"]) / np.abs(ref.stats["beta"])
     assert np.mean(relb < 1e-6) >= 0.99
+
+
+@pytest.mark.parametrize("n_cvt,miss", [(1, 0.02), (2, 0.0)])
+def test_series_sums_from_int8_calls_match_the_dgemm_form(n_cvt, miss):
+    """Linear series sums formed from the int8 calls (basis U A_lin^T on the INT8 rotation
+    core, precision 2) give the same statistics as the DGEMM over the rotated chunk
+    (precision 1): both carry the 4-digit split's ~1e-9 relative error, so p-values agree
+    to 1e-6 and significance calls exactly."""
+    from jamma_b200 import engine as eng
+    from oracle import plink as OP
+
+    n, m = 640, 900
+    g = synth.genotypes(n, m, miss, seed=5)
+    K = np.corrcoef(np.nan_to_num(g, nan=1.0))
+    w, U = np.linalg.eigh(K)
+    y = synth.phenotypes(np.nan_to_num(g, nan=1.0), n_causal=10, h2=0.5, seed=6)
+    cov = synth.covariates(n, n_cvt, seed=7)
+    cohort = eng.DeviceCohort(np.where(np.abs(w) < 1e-10, 0.0, w), U, cov, y, lmm_mode=4,
+                              precision="mixed")
+    assert cohort.series_ws is not None
+    mu = np.nan_to_num(np.nanmean(g, axis=0)).astype(np.float32).astype(np.float64)
+    codes, _ = eng.decode_packed(torch.from_numpy(OP.encode_genotypes(g)).cuda(), n, None, n,
+                                 ld=cohort.code_ld)
+    means = torch.from_numpy(mu).cuda()
+    X = cohort.rotate_codes_i8(codes, means, has_missing=miss > 0)
+    got = {k: v.cpu().numpy() for k, v in cohort.associate_rotated(X).items()}  # precision 2
+    assert cohort.rotate_status() == 0
+    ref = {k: v.cpu().numpy() for k, v in cohort.associate_rotated(X).items()}  # precision 1
+    for k in ("p_wald", "p_lrt", "p_score"):
+        rel = np.abs(got[k] - ref[k]) / np.abs(ref[k])
+        assert np.mean(rel < 1e-6) >= 0.99, f"{k}: worst {rel.max():.2e}"
+        np.testing.assert_array_equal(got[k] < 5e-8, ref[k] < 5e-8)
+        np.testing.assert_array_equal(got[k] < 1e-3, ref[k] < 1e-3)
+    np.testing.assert_allclose(got["p_score"], ref["p_score"], rtol=1e-7)
