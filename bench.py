@@ -30,6 +30,9 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 HBM_PEAK_FALLBACK = 6650.0
+# DRAM read + write bytes of one INT8 rotation launch at n = 20 000, 8 192 SNPs with missing
+# calls, from one ncu capture (dram__bytes_read.sum 29.09 GB + dram__bytes_write.sum 1.31 GB)
+ROT_DRAM_BYTES = 30.40e9
 
 
 def _peaks() -> dict:
@@ -389,6 +392,11 @@ def run_ours(args) -> None:
         return ms, kern, clk.summary(), outs
 
     cohort_mixed = eng.DeviceCohort(w, U, W, y, lmm_mode=args.mode, precision="mixed")
+    tuned = None
+    if not args.no_autotune:  # rotation tile schedule (applied) and best chunk width (reported)
+        from jamma_b200 import autotune
+
+        tuned = autotune.tune(cohort_mixed, use_cache=False)
     ms, kern_ms, clocks, outs = run_form("mixed", args.steps)
     if c_status := cohort_mixed.rotate_status():
         raise RuntimeError(f"INT8 rotation pipeline status {c_status}")
@@ -416,33 +424,49 @@ def run_ours(args) -> None:
     accuracy = _accuracy(one_chunk("mixed", args.warmup), one_chunk("fp64", args.warmup))
 
     # ---------------- end to end through the public chunk API with host buffers (mixed form)
+    # Each step: pinned-host packed records + means -> device, the chunk's captured CUDA
+    # graph (decode, rotation, series sums, search, statistics), results -> pinned host.
     rec_h = rec[:m].cpu().pin_memory()
-    mean_h = means[0].cpu()
+    mean_h = means[0].cpu().pin_memory()
     res_h = {k: torch.empty((1, m), dtype=torch.float64).pin_memory() for k in outs}
+    graph = eng.ChunkGraph(cohort_mixed, m, has_missing=has_missing)
     bufs = {"UtG": UtG}
 
-    def e2e_step():
+    def e2e_graph_step():
+        graph.packed.copy_(rec_h, non_blocking=True)
+        graph.means.copy_(mean_h, non_blocking=True)
+        for k, v in graph.replay().items():
+            res_h[k].copy_(v, non_blocking=True)
+
+    def e2e_eager_step():
         rd = rec_h.to("cuda", non_blocking=True)
         md = mean_h.to("cuda", non_blocking=True)
         cd, _ = eng.decode_packed(rd, n, None, n, ld=ld)
         o = cohort_mixed.associate_codes(cd, md, out=outs, bufs=bufs, has_missing=has_missing)
         for k, v in o.items():
             res_h[k].copy_(v, non_blocking=True)
-    for _ in range(2):
-        e2e_step()
-    torch.cuda.synchronize()
-    e2e_steps = max(2, min(args.steps, 5))
-    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    a.record(st)
-    for _ in range(e2e_steps):
-        e2e_step()
-    b.record(st)
-    torch.cuda.synchronize()
-    e2e_ms = a.elapsed_time(b) / e2e_steps
-    if world > 1:
-        tt = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
+
+    def time_e2e(fn):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        k = max(2, min(args.steps, 5))
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(st)
+        for _ in range(k):
+            fn()
+        b.record(st)
+        torch.cuda.synchronize()
+        t = a.elapsed_time(b) / k
+        if world > 1:
+            tt = torch.tensor([t], device="cuda")
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        return t
+
+    e2e_ms = time_e2e(e2e_graph_step)
+    e2e_eager_ms = time_e2e(e2e_eager_step)
+    del graph
 
     # ---------------- many phenotypes per cohort (one SNP chunk, all phenotypes per warp set)
     multi = None
@@ -502,7 +526,10 @@ def run_ours(args) -> None:
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8+f64",
             "data": "synthetic (seeded device RNG; Binomial(2,p) genotypes, p~U(0.05,0.5))",
             "config": _config(args, m),
-            "gpu_launches": (6 if has_missing else 5) * args.steps,
+            # own kernels per step: decode, [pack pairs], tiles + rotation GEMM, [tiles +
+            # series GEMM], square, search (the cuBLAS DGEMM is not counted)
+            "gpu_launches": (1 + int(has_missing) + 2 + 2 * int(cohort_mixed.series_ws is not None)
+                             + 2) * args.steps,
             "kernel_ms_per_step": kern_ms,
             "fp64_form": {"value": value64, "unit": "SNPs/s", "steps": fp64_steps,
                           "kernel_ms_per_step": kern64, "speedup_mixed_vs_fp64": value / value64},
@@ -511,7 +538,13 @@ def run_ours(args) -> None:
             "kinship_int8_vs_fp64_max_rel_diff": kin_maxdiff, "eigh_s": eigh_s,
             "roofline": {"kernel": "i8_gemm_kernel<rotate> (tcgen05 kind::i8, 4 digit planes)",
                          "bound": "tensor", "achieved": achieved, "peak": i8_peak,
-                         "unit": "TOP/s", "frac": achieved / i8_peak, "traffic": None,
+                         "unit": "TOP/s", "frac": achieved / i8_peak,
+                         # DRAM bytes of one launch, one ncu capture of this workload
+                         "traffic": ROT_DRAM_BYTES if (n, m, has_missing) == (20000, 8192, True) else None,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                           "rotation launch, n=20000, 8192 SNPs, schedule 9x16 "
+                                           "(profiles/rotate_i8_RotEpi_n20000_chunk8192_dram.md)",
+                         "algorithmic_bytes": 4 * n * n + 2 * n * m + 8 * n * m,
                          "peak_source": args.int8_peak_source},
             "accuracy_mixed_vs_fp64_form": {"snps": m, "fields": accuracy},
             "search_kernel": {"kernel": "lmm_pairs_kernel (FP64 search + statistics)",
@@ -519,10 +552,17 @@ def run_ours(args) -> None:
             "cpu_baseline": cpu,
             "e2e": {"value": m / (e2e_ms / 1e3) * world, "unit": "SNPs/s",
                     "h2d_bytes_per_step": m * bps + m * 8,
-                    "d2h_bytes_per_step": len(outs) * m * 8},
+                    "d2h_bytes_per_step": len(outs) * m * 8,
+                    "path": "engine.ChunkGraph replay (CUDA graph of the chunk) with pinned-host "
+                            "copies in the timed region",
+                    "eager_value": m / (e2e_eager_ms / 1e3) * world},
             "clocks": clocks,
             "serving": serving,
             "multi_phenotype": multi,
+            "autotune": None if tuned is None else {
+                "schedule": tuned["schedule"], "best_chunk": tuned["chunk"],
+                "best_chunk_snps_per_s": tuned["snps_per_s"],
+                "trials": [{k: t[k] for k in ("chunk", "schedule", "ms")} for t in tuned["trials"]]},
             "hbm_peak_gbs": peaks.get("hbm_gbs", HBM_PEAK_FALLBACK),
         }
         print(json.dumps(line), flush=True)
@@ -560,6 +600,7 @@ def main():
                     help="phenotypes of the multi-phenotype sub-measurement (1 = skip)")
     ap.add_argument("--pheno-chunk", type=int, default=2048)
     ap.add_argument("--pheno-mode", type=int, default=4)
+    ap.add_argument("--no-autotune", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

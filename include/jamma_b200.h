@@ -190,6 +190,16 @@ int32_t jb_rotate_f64(const double* U, int64_t n, int64_t ldu, const double* B,
                       int64_t m, int64_t ldb, double* C, int64_t ldc, uintptr_t stream);
 
 /*
+ * Tile schedule of the INT8 rotation kernels (no reference counterpart: a launch
+ * parameter).  Output tiles (32 eigenvectors x 128 or 256 SNPs) are visited in groups of
+ * group_m eigenvector blocks x group_n SNP blocks, which sets which operand slices the
+ * persistent CTAs share in L2.  Process-wide; default 9 x 16; set by the autotuner
+ * (jamma_b200.autotune).  Applies to launches issued after the call.
+ */
+int32_t jb_rotate_set_schedule(int32_t group_m, int32_t group_n);
+int32_t jb_rotate_get_schedule(int32_t* group_m, int32_t* group_n);
+
+/*
  * Mixed-precision rotation on INT8 tensor cores (replaces the host UT @ G of
  * src/jamma/lmm/runner_streaming.py:409).  jb_ozaki_prepare splits the eigenvectors U
  * (n x n, column-major, ldu) once per cohort into four exact int8 digit planes with a

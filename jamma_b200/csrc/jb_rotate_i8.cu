@@ -20,6 +20,8 @@
 #include "jb_gemm_i8.cuh"
 #include "jb_rotate_i8.cuh"
 
+#include <atomic>
+
 namespace jb {
 namespace tc {
 
@@ -163,9 +165,9 @@ struct RotEpi {
 
 // Tiles over (eigenvector blocks of 32, SNP blocks) in groups of GM x GN (GN SNP blocks
 // per group column, groups visited column by column), one thread per tile: tile (mb, nb)
-// sits at its closed-form position in that order.
-__global__ void rot_tiles_kernel(int MB, int NB, Tile* out) {
-    constexpr int GM = 9, GN = 16;
+// sits at its closed-form position in that order.  The group shape sets which A (digit)
+// and B (calls) slices the persistent CTAs share in L2 at a time.
+__global__ void rot_tiles_kernel(int MB, int NB, int GM, int GN, Tile* out) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (int64_t)MB * NB) return;
     const int mb = (int)(t / NB), nb = (int)(t % NB);
@@ -185,6 +187,9 @@ using namespace jb::tc;
 namespace jb {
 namespace tc {
 using RotSmem = GemmSmem<kRotBN, kRotStages, kRotEpiSmem>;
+
+// Tile-group shape of the rotation schedule (jb_rotate_set_schedule; the autotuner's knob).
+std::atomic<int> g_group_m{9}, g_group_n{16};
 
 OzakiLayout ozaki_layout(int64_t n_out, int64_t n_k) {
     OzakiLayout L;
@@ -235,7 +240,9 @@ int32_t rotate_i8_gemm(const uint8_t* ozaki_ws, int64_t n_out, int64_t n_k, cons
     if (rc) return rc;
     rc = make_map_i8(&tb, B, b_rows, n_k, ldb, kRotBN);
     if (rc) return rc;
-    rot_tiles_kernel<<<(unsigned)ceil_div((int64_t)n_tiles, 256), 256, 0, st>>>(MB, NB, tiles);
+    rot_tiles_kernel<<<(unsigned)ceil_div((int64_t)n_tiles, 256), 256, 0, st>>>(
+        MB, NB, g_group_m.load(std::memory_order_relaxed), g_group_n.load(std::memory_order_relaxed),
+        tiles);
     JB_LAUNCH_CHECK("rot_tiles_kernel");
     const int grid = n_tiles < num_sms() ? n_tiles : num_sms();
     const int num_kb = (int)ceil_div(n_k, kBK);
@@ -307,6 +314,21 @@ int32_t jb_rotate_i8(const void* ozaki_ws, int64_t n, const int8_t* codes, int64
     // no missing calls: the decoded codes are the calls themselves
     return rotate_i8_gemm(ows, n, n, codes, m, ld_codes, false, m, nullptr, X, ldx, tiles, status,
                           st);
+}
+
+int32_t jb_rotate_set_schedule(int32_t group_m, int32_t group_n) {
+    JB_CHECK_ARG(group_m >= 1 && group_m <= 1024 && group_n >= 1 && group_n <= 1024,
+                 "jb_rotate_set_schedule: group sizes must be in 1..1024");
+    g_group_m.store(group_m, std::memory_order_relaxed);
+    g_group_n.store(group_n, std::memory_order_relaxed);
+    return JB_OK;
+}
+
+int32_t jb_rotate_get_schedule(int32_t* group_m, int32_t* group_n) {
+    JB_CHECK_ARG(group_m && group_n, "jb_rotate_get_schedule: null pointer");
+    *group_m = g_group_m.load(std::memory_order_relaxed);
+    *group_n = g_group_n.load(std::memory_order_relaxed);
+    return JB_OK;
 }
 
 int32_t jb_rotate_status(const void* workspace, int32_t* out, uintptr_t stream) {

@@ -239,6 +239,54 @@ class DeviceCohort:
         return self.associate_genotypes(G, out, UtG)
 
 
+class ChunkGraph:
+    """One chunk's device work captured as a CUDA graph over static buffers.
+
+    The captured sequence is the whole per-chunk hot path of a cohort -- decode of the
+    packed .bed records, rotation (INT8 tensor cores or FP64), the series sums and the
+    per-SNP search with its statistics -- so a replay is one launch from the host instead
+    of the eight to ten kernel and library launches of an eager chunk.  Fill ``packed``
+    (m, bytes_per_snp) and ``means`` (m,) (e.g. by non-blocking copies from pinned host
+    memory on the replaying stream), call :meth:`replay`, read ``out``.
+
+    ``m`` is fixed at capture; a shorter final chunk is run eagerly.  The graph keeps the
+    cohort's workspaces alive; capture after any eager chunk larger than ``m`` so that
+    no workspace is reallocated afterwards.
+    """
+
+    def __init__(self, cohort: "DeviceCohort", m: int, n_file: int | None = None,
+                 sample_idx: torch.Tensor | None = None, has_missing: bool = True):
+        n = cohort.n
+        n_file = n if n_file is None else n_file
+        self.cohort, self.m, self.n_file, self.sample_idx = cohort, m, n_file, sample_idx
+        self.has_missing = bool(has_missing)
+        self.packed = torch.zeros((m, (n_file + 3) // 4), dtype=torch.uint8, device="cuda")
+        self.means = torch.zeros((m,), dtype=torch.float64, device="cuda")
+        self.out = cohort.alloc_out(m)
+        self.bufs = {"UtG": empty((m, n)), "G": empty((m, n)) if cohort.precision != "mixed" else None}
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):  # eager warm-up: workspaces, handles, kernel attributes
+            self._run()
+        torch.cuda.current_stream().wait_stream(side)
+        torch.cuda.synchronize()
+        self._keep = (cohort.ws, cohort._chunk_ws, cohort._rot_ws, cohort.series_ws, cohort.ozaki)
+        self.graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self.graph):
+            self._run()
+
+    def _run(self) -> None:
+        c = self.cohort
+        codes, _ = decode_packed(self.packed, self.n_file, self.sample_idx, c.n, ld=c.code_ld)
+        c.associate_codes(codes, self.means, out=self.out,
+                          bufs={k: v for k, v in self.bufs.items() if v is not None},
+                          has_missing=self.has_missing)
+
+    def replay(self) -> dict:
+        self.graph.replay()
+        return self.out
+
+
 def decode_packed(packed: torch.Tensor, n_file: int, sample_idx: torch.Tensor | None, n: int,
                   ld: int | None = None) -> tuple[torch.Tensor, torch.Tensor]:
     """Device decode of (m, bytes_per_snp) packed records -> codes (m, ld) + counts (m, 4)."""

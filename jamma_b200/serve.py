@@ -6,15 +6,20 @@ concurrently, each on its own CUDA stream, advancing one SNP chunk at a time, so
 kernels overlap on the device and a job that arrives while others run starts as soon as
 memory frees up.  Cohorts (eigenvalues, eigenvectors and their INT8 digit planes) stay
 resident and are shared: a job on a known cohort skips kinship and eigendecomposition.
-Packed genotype records stream from pinned host memory with asynchronous copies on the
-job's stream.  Every job's arithmetic is the library's ordinary association path with
+A job's set-up (pass-1 counts, and for a new cohort the INT8 kinship and the
+eigendecomposition, whose solver synchronises its stream) runs on a worker thread, so
+the loop keeps feeding the other jobs' chunks meanwhile; jobs that need a cohort being
+built wait for that one build.  Packed genotype records stream from pinned host memory
+with asynchronous copies on the job's stream.  Every job's arithmetic is the library's ordinary association path with
 per-job buffers and a fixed chunk width, so its results do not depend on what else runs.
 """
 
 from __future__ import annotations
 
+import threading
 import time
 from collections import OrderedDict, deque
+from concurrent.futures import Future, ThreadPoolExecutor
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -59,6 +64,16 @@ class _Resident:
         self.refs = 0
 
 
+class _Building:
+    """A cohort whose kinship + eigendecomposition one worker is computing; ``waiters``
+    jobs (the builder included) will hold a reference to it."""
+
+    def __init__(self):
+        self.done = threading.Event()
+        self.waiters = 1
+        self.error: BaseException | None = None
+
+
 class _Active:
     def __init__(self, job: GwasJob, stream: torch.cuda.Stream):
         self.job, self.stream = job, stream
@@ -83,8 +98,13 @@ def job_device_bytes(n: int, phi: int, n_cvt: int, chunk: int, resident: bool) -
 
 class GwasServer:
     def __init__(self, hbm_budget_bytes: int, max_active: int = 4, chunk: int = 4096,
-                 precision: str = "mixed"):
+                 precision: str = "mixed", setup_workers: int = 2):
         require_cuda()
+        self._pool = ThreadPoolExecutor(max_workers=max(1, setup_workers),
+                                        thread_name_prefix="jb-setup")
+        self._lock = threading.Lock()  # cohorts / _building, shared with the workers
+        self._building: dict[str, _Building] = {}
+        self.preparing: list[tuple[_Active, Future]] = []
         self.budget = int(hbm_budget_bytes)
         self.max_active = max_active
         self.chunk = chunk
@@ -113,59 +133,102 @@ class GwasServer:
                 del self.cohorts[cid]
 
     def _try_admit(self) -> None:
-        while self.queue and len(self.active) < self.max_active:
+        while self.queue and len(self.active) + len(self.preparing) < self.max_active:
             job = self.queue[0]
             phi = 1 if np.ndim(job.phenotypes) == 1 else job.phenotypes.shape[1]
             c = 1 if job.covariates is None else job.covariates.shape[1]
-            need = job_device_bytes(job.n_samples, phi, c, self.chunk, job.cohort_id in self.cohorts)
-            self._evict_for(need)
-            if self.used + self._resident_bytes() + need > self.budget:
-                if not self.active:
-                    raise MemoryError(f"job {job.job_id} needs {need} bytes, over the HBM budget")
-                return
-            self.queue.popleft()
-            self._start(job, need)
+            with self._lock:
+                known = job.cohort_id in self.cohorts or job.cohort_id in self._building
+                need = job_device_bytes(job.n_samples, phi, c, self.chunk, known)
+                self._evict_for(need)
+                if self.used + self._resident_bytes() + need > self.budget:
+                    if not self.active and not self.preparing:
+                        raise MemoryError(f"job {job.job_id} needs {need} bytes, over the HBM budget")
+                    return
+                self.queue.popleft()
+                # reserve the cohort now so that eviction cannot take it before set-up
+                if job.cohort_id in self.cohorts:
+                    self.cohorts[job.cohort_id].refs += 1
+                    self.cohorts.move_to_end(job.cohort_id)
+                    build = None
+                elif job.cohort_id in self._building:
+                    self._building[job.cohort_id].waiters += 1
+                    build = False
+                else:
+                    self._building[job.cohort_id] = _Building()
+                    build = True
+            act = _Active(job, torch.cuda.Stream())
+            act.bytes = need
+            self.used += need
+            self.preparing.append((act, self._pool.submit(self._prepare, act, build)))
 
-    def _start(self, job: GwasJob, need: int) -> None:
-        stream = torch.cuda.Stream()
-        act = _Active(job, stream)
-        act.bytes = need
-        self.used += need
+    def _cohort(self, job: GwasJob, build, codes, packed, cnt, poly) -> _Resident:
+        """The job's resident cohort: already reserved (build None), built by this worker
+        (True) or awaited from the worker building it (False)."""
+        if build is None:
+            with self._lock:
+                return self.cohorts[job.cohort_id]
+        if build is False:
+            with self._lock:
+                b = self._building.get(job.cohort_id)
+            if b is not None:
+                b.done.wait()
+                if b.error is not None:
+                    raise RuntimeError(f"cohort {job.cohort_id} set-up failed") from b.error
+            with self._lock:
+                return self.cohorts[job.cohort_id]
+        with self._lock:
+            b = self._building[job.cohort_id]
+        try:  # new cohort: INT8 kinship + FP64 eigendecomposition on the device
+            n = job.n_samples
+            acc = _KinshipI8(n, int(poly.sum()))
+            kidx = np.where(poly)[0]
+            sel = torch.from_numpy(kidx).cuda()
+            cc = cnt[kidx]
+            acc.add(codes.index_select(0, sel), torch.from_numpy(cc[:, 1] / np.maximum(cc[:, 0], 1)).cuda(),
+                    bool(np.any(cc[:, 0] < n)), packed.index_select(0, sel))
+            acc.add_sum_mu2(cc[:, 1] / np.maximum(cc[:, 0], 1))
+            K = acc.finish()
+            evals, U = eng.eigh_device(K)
+            oz = eng.ozaki_split(U) if self.precision == "mixed" else None
+            torch.cuda.current_stream().synchronize()  # resident state complete for other streams
+            res = _Resident(evals, U, oz)
+        except BaseException as e:
+            with self._lock:
+                b.error = e
+                del self._building[job.cohort_id]
+            b.done.set()
+            raise
+        with self._lock:
+            res.refs = b.waiters
+            self.cohorts[job.cohort_id] = res
+            del self._building[job.cohort_id]
+        b.done.set()
+        return res
+
+    def _prepare(self, act: _Active, build) -> _Active:
+        """Worker thread: pass-1 statistics, the cohort, and the job's device state."""
+        job = act.job
         n = job.n_samples
-        with torch.cuda.stream(stream):
+        with torch.cuda.stream(act.stream):
             packed = torch.from_numpy(job.packed).pin_memory().to("cuda", non_blocking=True)
             codes, counts = eng.decode_packed(packed, n, None, n)
             cnt = counts.cpu().numpy()  # pass 1: per-SNP statistics
             mean, miss, poly = snp_stats_from_counts(cnt, n, np.float32)
             keep, af = filter_mask(mean, miss, poly, n, job.maf_threshold, job.miss_threshold)
             idx = np.where(keep)[0]
-            res = self.cohorts.get(job.cohort_id)
-            if res is None:  # new cohort: INT8 kinship + FP64 eigendecomposition on the device
-                acc = _KinshipI8(n, int(poly.sum()))
-                kidx = np.where(poly)[0]
-                sel = torch.from_numpy(kidx).cuda()
-                cc = cnt[kidx]
-                acc.add(codes.index_select(0, sel), torch.from_numpy(cc[:, 1] / np.maximum(cc[:, 0], 1)).cuda(),
-                        bool(np.any(cc[:, 0] < n)), packed.index_select(0, sel))
-                acc.add_sum_mu2(cc[:, 1] / np.maximum(cc[:, 0], 1))
-                K = acc.finish()
-                evals, U = eng.eigh_device(K)
-                oz = eng.ozaki_split(U) if self.precision == "mixed" else None
-                res = _Resident(evals, U, oz)
-                self.cohorts[job.cohort_id] = res
-            res.refs += 1
-            self.cohorts.move_to_end(job.cohort_id)
+            res = self._cohort(job, build, codes, packed, cnt, poly)
             act.cohort = eng.DeviceCohort(res.evals, res.U, job.covariates, job.phenotypes,
                                           job.lmm_mode, precision=self.precision, ozaki=res.ozaki)
             act.packed_host = torch.from_numpy(np.ascontiguousarray(job.packed[idx])).pin_memory()
             act.means = torch.from_numpy(mean[idx].astype(np.float64)).pin_memory()
             act.n_miss = miss[idx]
+            act.bufs = {"UtG": empty((self.chunk, n))}
         job.snp_indices = idx
         job.results = {k: np.empty((act.cohort.phi, idx.size)) for k in eng.MODE_KEYS[job.lmm_mode]}
         job.af, job.n_miss = af[idx], miss[idx]
         act.chunk_starts = list(range(0, idx.size, self.chunk))
-        act.bufs = {"UtG": empty((self.chunk, n))}
-        self.active.append(act)
+        return act
 
     # ------------------------------------------------------------ execution
     def _launch_chunk(self, act: _Active) -> None:
@@ -200,17 +263,30 @@ class GwasServer:
         act.inflight = keep
         return act.next >= len(act.chunk_starts) and not act.inflight
 
-    def step(self) -> None:
+    def step(self) -> bool:
+        """One pass of the loop; returns False when it found nothing to do."""
         self._try_admit()
+        busy = False
+        for item in list(self.preparing):
+            act, fut = item
+            if fut.done():
+                self.preparing.remove(item)
+                fut.result()  # re-raises a set-up failure here
+                self.active.append(act)
+                busy = True
         for act in list(self.active):
             if act.next < len(act.chunk_starts) and len(act.inflight) < 2:
                 self._launch_chunk(act)
+                busy = True
             if self._poll(act):
                 act.job.done = time.perf_counter()
                 self.finished.append(act.job)
-                self.cohorts[act.job.cohort_id].refs -= 1
+                with self._lock:
+                    self.cohorts[act.job.cohort_id].refs -= 1
                 self.used -= act.bytes
                 self.active.remove(act)
+                busy = True
+        return busy
 
     def run(self, arrivals: list[tuple[float, GwasJob]] | None = None) -> list[GwasJob]:
         """Drive the loop until every submitted (and, if given, scheduled) job is done.
@@ -220,14 +296,15 @@ class GwasServer:
         """
         pending = deque(sorted(arrivals or [], key=lambda a: a[0]))
         self.t0 = time.perf_counter()
-        while pending or self.queue or self.active:
+        while pending or self.queue or self.active or self.preparing:
             now = time.perf_counter()
             while pending and now - self.t0 >= pending[0][0]:
                 self.submit(pending.popleft()[1], now)
-            if not self.active and not self.queue and pending:
+            if not self.active and not self.queue and not self.preparing and pending:
                 time.sleep(min(0.001, max(0.0, pending[0][0] - (now - self.t0))))
                 continue
-            self.step()
+            if not self.step():
+                time.sleep(0.0002)  # let the set-up workers run (they need the GIL between calls)
         torch.cuda.synchronize()
         return self.finished
 
