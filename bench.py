@@ -258,6 +258,10 @@ def run_ours(args) -> None:
         _build.build()
     if world > 1:
         dist.barrier()
+    if args.rot_kernel is not None:
+        from jamma_b200 import _native as _nat
+
+        _nat.call("jb_rotate_set_kernel", args.rot_kernel)
     from jamma_b200 import _native, engine as eng, synth
     from jamma_b200.device import ptr, stream_handle
     from jamma_b200.kinship import _KinshipAccumulator, _KinshipI8, snp_stats_from_counts
@@ -560,9 +564,11 @@ def run_ours(args) -> None:
             "serving": serving,
             "multi_phenotype": multi,
             "autotune": None if tuned is None else {
+                "kernel": ["one CTA per tile", "CTA pairs (cta_group::2)"][tuned["kernel"]],
                 "schedule": tuned["schedule"], "best_chunk": tuned["chunk"],
                 "best_chunk_snps_per_s": tuned["snps_per_s"],
-                "trials": [{k: t[k] for k in ("chunk", "schedule", "ms")} for t in tuned["trials"]]},
+                "trials": [{k: t[k] for k in ("chunk", "kernel", "schedule", "ms")}
+                           for t in tuned["trials"]]},
             "hbm_peak_gbs": peaks.get("hbm_gbs", HBM_PEAK_FALLBACK),
         }
         print(json.dumps(line), flush=True)
@@ -601,6 +607,8 @@ def main():
     ap.add_argument("--pheno-chunk", type=int, default=2048)
     ap.add_argument("--pheno-mode", type=int, default=4)
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--rot-kernel", type=int, choices=[0, 1], default=None,
+                    help="fix the INT8 rotation kernel (0 one CTA per tile, 1 CTA pairs)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

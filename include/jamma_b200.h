@@ -200,6 +200,16 @@ int32_t jb_rotate_set_schedule(int32_t group_m, int32_t group_n);
 int32_t jb_rotate_get_schedule(int32_t* group_m, int32_t* group_n);
 
 /*
+ * GEMM variant of the INT8 rotation kernels (no reference counterpart).  0: one CTA per
+ * 128-row x 256-column output tile (tcgen05 cta_group::1).  1: clusters of two CTAs on
+ * neighbouring SMs share one 256 x 256 tile (cta_group::2, M = 256): each SM streams half
+ * of the B operand, so operand traffic from L2 per MAC falls by a third.  Results are
+ * identical (exact integer products).  Process-wide; applies to later launches.
+ */
+int32_t jb_rotate_set_kernel(int32_t variant);
+int32_t jb_rotate_get_kernel(void);
+
+/*
  * Mixed-precision rotation on INT8 tensor cores (replaces the host UT @ G of
  * src/jamma/lmm/runner_streaming.py:409).  jb_ozaki_prepare splits the eigenvectors U
  * (n x n, column-major, ldu) once per cohort into four exact int8 digit planes with a

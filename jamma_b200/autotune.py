@@ -5,8 +5,9 @@ Two knobs set how fast one cohort's SNP chunks go through the device:
 * the chunk width m (SNPs per launch sequence): larger chunks amortise launches and fill
   the 148 SMs' persistent tiles evenly, but hold n*m*8 bytes of rotated genotypes and
   more workspace, and delay the first results;
-* the tile-group shape of the INT8 rotation (``jb_rotate_set_schedule``): which operand
-  slices the persistent CTAs share in L2.
+* the INT8 rotation kernel: one CTA per output tile or CTA pairs sharing a 256-row tile
+  (``jb_rotate_set_kernel``), and its tile-group shape (``jb_rotate_set_schedule``): which
+  operand slices the persistent CTAs share in L2.
 
 ``tune(cohort)`` times real chunks of the given cohort on synthetic calls of its shape
 (CUDA events, warm-up excluded) over the candidates that fit the memory budget, applies
@@ -30,6 +31,7 @@ from jamma_b200.device import require_cuda
 
 CHUNKS = (2048, 4096, 8192, 16384)
 SCHEDULES = ((9, 16), (5, 32), (17, 8), (3, 64), (36, 4))
+KERNELS = (0, 1)  # one CTA per tile, CTA pairs
 _lock = threading.Lock()
 
 
@@ -60,6 +62,14 @@ def _store(entries: dict) -> None:
 
 def set_schedule(group_m: int, group_n: int) -> None:
     _native.call("jb_rotate_set_schedule", int(group_m), int(group_n))
+
+
+def set_kernel(variant: int) -> None:
+    _native.call("jb_rotate_set_kernel", int(variant))
+
+
+def get_kernel() -> int:
+    return int(_native.load().jb_rotate_get_kernel())
 
 
 def get_schedule() -> tuple[int, int]:
@@ -111,11 +121,11 @@ def _time_chunk(cohort, codes, means, reps: int = 3) -> float:
 
 
 def tune(cohort, memory_budget: int | None = None, chunks=CHUNKS, schedules=SCHEDULES,
-         use_cache: bool = True, reps: int = 3) -> dict:
-    """Pick the chunk width and rotation schedule for ``cohort``; returns
-    {"chunk": m, "schedule": [gm, gn], "snps_per_s": best, "trials": [...]} and applies
-    the schedule.  ``memory_budget`` caps the per-chunk device bytes (default: half of the
-    free device memory)."""
+         kernels=KERNELS, use_cache: bool = True, reps: int = 3) -> dict:
+    """Pick the chunk width, rotation kernel and schedule for ``cohort``; returns
+    {"chunk": m, "kernel": k, "schedule": [gm, gn], "snps_per_s": best, "trials": [...]}
+    and applies kernel and schedule.  ``memory_budget`` caps the per-chunk device bytes
+    (default: half of the free device memory)."""
     require_cuda()
     gpu = torch.cuda.get_device_name()
     key = _key(cohort, gpu)
@@ -123,6 +133,7 @@ def tune(cohort, memory_budget: int | None = None, chunks=CHUNKS, schedules=SCHE
         if use_cache:
             hit = _load().get(key)
             if hit is not None:
+                set_kernel(hit.get("kernel", 0))
                 set_schedule(*hit["schedule"])
                 return hit
         if memory_budget is None:
@@ -131,26 +142,29 @@ def tune(cohort, memory_budget: int | None = None, chunks=CHUNKS, schedules=SCHE
         trials = []
         m_big = max(fits)
         codes, means = _synthetic_chunk(cohort.n, m_big, cohort.code_ld)
-        best_sched, best_t = None, None
-        if cohort.precision == "mixed":  # schedule first, at the largest chunk that fits
-            for sched in schedules:
-                set_schedule(*sched)
-                t = _time_chunk(cohort, codes, means, reps)
-                trials.append({"chunk": m_big, "schedule": list(sched), "ms": t})
-                if best_t is None or t < best_t:
-                    best_sched, best_t = sched, t
+        best_sched, best_kernel, best_t = None, None, None
+        if cohort.precision == "mixed":  # kernel + schedule first, at the largest chunk that fits
+            for kern in kernels:
+                set_kernel(kern)
+                for sched in schedules:
+                    set_schedule(*sched)
+                    t = _time_chunk(cohort, codes, means, reps)
+                    trials.append({"chunk": m_big, "kernel": kern, "schedule": list(sched), "ms": t})
+                    if best_t is None or t < best_t:
+                        best_sched, best_kernel, best_t = sched, kern, t
+            set_kernel(best_kernel)
             set_schedule(*best_sched)
         else:
-            best_sched = get_schedule()
+            best_sched, best_kernel = get_schedule(), get_kernel()
         best_m, best_rate = None, -1.0
         for m in fits:
             t = _time_chunk(cohort, codes[:m], means[:m], reps)
-            trials.append({"chunk": m, "schedule": list(best_sched), "ms": t})
+            trials.append({"chunk": m, "kernel": best_kernel, "schedule": list(best_sched), "ms": t})
             rate = m / (t / 1e3)
             if rate > best_rate:
                 best_m, best_rate = m, rate
-        res = {"chunk": int(best_m), "schedule": list(best_sched), "snps_per_s": best_rate,
-               "trials": trials, "gpu": gpu}
+        res = {"chunk": int(best_m), "kernel": int(best_kernel), "schedule": list(best_sched),
+               "snps_per_s": best_rate, "trials": trials, "gpu": gpu}
         if use_cache:
             entries = _load()
             entries[key] = res

@@ -31,6 +31,7 @@ int num_sms();
 
 constexpr int kRotBN = 256;
 constexpr int kRotStages = 4;
+constexpr int kRotPairStages = 6;
 constexpr int kRotEpiSmem = 4 * 32 * 32 * 8;  // [digit][column][eigvec] doubles
 
 // ---------------------------------------------------------------- digit split
@@ -188,8 +189,34 @@ namespace jb {
 namespace tc {
 using RotSmem = GemmSmem<kRotBN, kRotStages, kRotEpiSmem>;
 
-// Tile-group shape of the rotation schedule (jb_rotate_set_schedule; the autotuner's knob).
+// Tile-group shape of the rotation schedule (jb_rotate_set_schedule; the autotuner's knob)
+// and the GEMM variant (jb_rotate_set_kernel: 0 = one CTA per tile, 1 = CTA pairs).
 std::atomic<int> g_group_m{9}, g_group_n{16};
+std::atomic<int> g_rot_kernel{0};
+using PairRotSmem = PairSmem<kRotPairStages, kRotEpiSmem>;
+
+template <bool P>
+int32_t launch_rot_pair(const CUtensorMap& ta, const CUtensorMap& tb, const Tile* tiles,
+                        int n_tiles, int num_kb, const RotEpi<P>& epi, int* status,
+                        cudaStream_t st) {
+    auto kern = i8_gemm_pair_kernel<kRotPairStages, RotEpi<P>>;
+    JB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 PairRotSmem::TOTAL));
+    // persistent: as many pairs as can be resident at once (clusters need two SMs of one GPC)
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)(2 * (num_sms() / 2)));
+    cfg.blockDim = dim3(kThreads);
+    cfg.dynamicSmemBytes = PairRotSmem::TOTAL;
+    cfg.stream = st;
+    int resident = 0;
+    JB_CUDA(cudaOccupancyMaxActiveClusters(&resident, kern, &cfg));
+    JB_CHECK_ARG(resident >= 1, "rotation: no CTA pair fits on the device");
+    const int pairs = n_tiles < resident ? n_tiles : resident;
+    kern<<<2 * pairs, kThreads, PairRotSmem::TOTAL, st>>>(ta, tb, tiles, n_tiles, num_kb, epi,
+                                                         status);
+    JB_LAUNCH_CHECK("i8_gemm_pair_kernel<rotate>");
+    return JB_OK;
+}
 
 OzakiLayout ozaki_layout(int64_t n_out, int64_t n_k) {
     OzakiLayout L;
@@ -234,10 +261,29 @@ int32_t rotate_i8_gemm(const uint8_t* ozaki_ws, int64_t n_out, int64_t n_k, cons
     const double* smax = reinterpret_cast<const double*>(ozaki_ws + OL.s_off);
     const int MB = (int)ceil_div(n_out, 32);
     const int NB = (int)ceil_div(m, paired ? 128 : 256);
-    const int n_tiles = MB * NB;
+    const int num_kb = (int)ceil_div(n_k, kBK);
     CUtensorMap ta, tb;
     int32_t rc = make_map_i8(&ta, A, OL.rows, n_k, OL.lda, kBM);
     if (rc) return rc;
+    if (g_rot_kernel.load(std::memory_order_relaxed) == 1) {
+        // CTA pairs: tile = 2 eigenvector blocks (one per CTA) x 256 B rows (128 per CTA)
+        rc = make_map_i8(&tb, B, b_rows, n_k, ldb, 128);
+        if (rc) return rc;
+        const int MB2 = (MB + 1) / 2;
+        const int n_pairs_tiles = MB2 * NB;
+        rot_tiles_kernel<<<(unsigned)ceil_div((int64_t)n_pairs_tiles, 256), 256, 0, st>>>(
+            MB2, NB, g_group_m.load(std::memory_order_relaxed),
+            g_group_n.load(std::memory_order_relaxed), tiles);
+        JB_LAUNCH_CHECK("rot_tiles_kernel");
+        if (paired)
+            return launch_rot_pair<true>(ta, tb, tiles, n_pairs_tiles, num_kb,
+                                         RotEpi<true>{X, ldx, smax, mean, (int)n_out, (int)m},
+                                         status, st);
+        return launch_rot_pair<false>(ta, tb, tiles, n_pairs_tiles, num_kb,
+                                      RotEpi<false>{X, ldx, smax, nullptr, (int)n_out, (int)m},
+                                      status, st);
+    }
+    const int n_tiles = MB * NB;
     rc = make_map_i8(&tb, B, b_rows, n_k, ldb, kRotBN);
     if (rc) return rc;
     rot_tiles_kernel<<<(unsigned)ceil_div((int64_t)n_tiles, 256), 256, 0, st>>>(
@@ -245,7 +291,6 @@ int32_t rotate_i8_gemm(const uint8_t* ozaki_ws, int64_t n_out, int64_t n_k, cons
         tiles);
     JB_LAUNCH_CHECK("rot_tiles_kernel");
     const int grid = n_tiles < num_sms() ? n_tiles : num_sms();
-    const int num_kb = (int)ceil_div(n_k, kBK);
     if (paired) {
         auto kern = i8_gemm_kernel<kRotBN, kRotStages, RotEpi<true>>;
         JB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -323,6 +368,14 @@ int32_t jb_rotate_set_schedule(int32_t group_m, int32_t group_n) {
     g_group_n.store(group_n, std::memory_order_relaxed);
     return JB_OK;
 }
+
+int32_t jb_rotate_set_kernel(int32_t variant) {
+    JB_CHECK_ARG(variant == 0 || variant == 1, "jb_rotate_set_kernel: variant must be 0 or 1");
+    g_rot_kernel.store(variant, std::memory_order_relaxed);
+    return JB_OK;
+}
+
+int32_t jb_rotate_get_kernel(void) { return g_rot_kernel.load(std::memory_order_relaxed); }
 
 int32_t jb_rotate_get_schedule(int32_t* group_m, int32_t* group_n) {
     JB_CHECK_ARG(group_m && group_n, "jb_rotate_get_schedule: null pointer");

@@ -35,12 +35,13 @@ def test_tune_caches_and_schedule_keeps_results(tmp_path, monkeypatch):
     y = synth.phenotypes(g, n_causal=5, h2=0.5, seed=4)
     cohort = eng.DeviceCohort(np.where(np.abs(w) < 1e-10, 0.0, w), U, None, y, lmm_mode=4,
                               precision="mixed")
-    default = autotune.get_schedule()
+    default, default_kernel = autotune.get_schedule(), autotune.get_kernel()
     codes, means = autotune._synthetic_chunk(n, 512, cohort.code_ld, seed=9)
     base = {k: v.cpu().numpy() for k, v in cohort.associate_codes(codes, means).items()}
     try:
         res = autotune.tune(cohort, chunks=(256, 512), reps=1)
-        assert res["chunk"] in (256, 512)
+        assert res["chunk"] in (256, 512) and res["kernel"] in autotune.KERNELS
+        assert autotune.get_kernel() == res["kernel"]
         assert tuple(res["schedule"]) in autotune.SCHEDULES
         assert autotune.get_schedule() == tuple(res["schedule"])
         cached = json.loads((tmp_path / "tune.json").read_text())
@@ -49,14 +50,16 @@ def test_tune_caches_and_schedule_keeps_results(tmp_path, monkeypatch):
         again = autotune.tune(cohort, chunks=(256, 512), reps=1)  # served from the cache
         assert again["trials"] == res["trials"]
         assert autotune.get_schedule() == tuple(res["schedule"])
-        for sched in ((3, 64), (36, 4)):
+        for kern, sched in ((0, (3, 64)), (0, (36, 4)), (1, (9, 16)), (1, (5, 32))):
+            autotune.set_kernel(kern)
             autotune.set_schedule(*sched)
             got = {k: v.cpu().numpy() for k, v in cohort.associate_codes(codes, means).items()}
             for k in base:
-                np.testing.assert_array_equal(got[k], base[k], err_msg=f"{sched} {k}")
+                np.testing.assert_array_equal(got[k], base[k], err_msg=f"{kern} {sched} {k}")
         assert cohort.rotate_status() == 0
     finally:
         autotune.set_schedule(*default)
+        autotune.set_kernel(default_kernel)
 
 
 def test_schedule_rejects_bad_groups():

@@ -180,3 +180,31 @@ def test_series_sums_from_int8_calls_match_the_dgemm_form(n_cvt, miss):
         np.testing.assert_array_equal(got[k] < 5e-8, ref[k] < 5e-8)
         np.testing.assert_array_equal(got[k] < 1e-3, ref[k] < 1e-3)
     np.testing.assert_allclose(got["p_score"], ref["p_score"], rtol=1e-7)
+
+
+@pytest.mark.parametrize("n,m,miss", [(300, 700, 0.02), (256, 512, 0.0), (97, 33, 0.1),
+                                      (1000, 300, 0.01), (2500, 1100, 0.01)])
+def test_rotate_pair_kernel_equals_single_cta_kernel(n, m, miss):
+    """CTA-pair (cta_group::2, M = 256) rotation == one-CTA rotation, bit for bit; odd
+    numbers of eigenvector blocks leave the second CTA of the last pair on zero rows."""
+    from jamma_b200 import _native
+    from jamma_b200 import engine as eng
+    from oracle import plink as OP
+
+    U = _orthogonal(n, 3 * n + m)
+    g = synth.genotypes(n, m, miss, seed=n + m)
+    mu = np.nan_to_num(np.nanmean(g, axis=0)).astype(np.float32).astype(np.float64)
+    cohort = eng.DeviceCohort(np.ones(n), U, None, np.zeros(n), lmm_mode=1, precision="mixed")
+    codes, _ = eng.decode_packed(torch.from_numpy(OP.encode_genotypes(g)).cuda(), n, None, n,
+                                 ld=cohort.code_ld)
+    means = torch.from_numpy(mu).cuda()
+    prev = _native.load().jb_rotate_get_kernel()
+    try:
+        out = {}
+        for variant in (0, 1):
+            _native.call("jb_rotate_set_kernel", variant)
+            out[variant] = cohort.rotate_codes_i8(codes, means, has_missing=miss > 0).cpu().numpy()
+            assert cohort.rotate_status() == 0, variant
+    finally:
+        _native.call("jb_rotate_set_kernel", prev)
+    np.testing.assert_array_equal(out[1], out[0])
