@@ -86,6 +86,18 @@ int32_t jb_kinship_accumulate_f64(const int8_t* codes, int64_t ld_codes, int64_t
                                   void* workspace, int64_t workspace_bytes,
                                   uintptr_t stream);
 
+/*
+ * Standardized kinship (-gk 2) accumulation: as jb_kinship_accumulate_f64 with every
+ * centred column divided by sd[j] (0 where sd[j] == 0) -- impute_center_and_standardize
+ * (src/jamma/kinship/missing.py:64-119) feeding compute_standardized_kinship
+ * (src/jamma/kinship/compute.py:229-360).  sd[j] = sqrt(mean over all n samples of the
+ * mean-imputed x^2 - mean^2), computed by the caller from the pass-1 counts.
+ */
+int32_t jb_kinship_accumulate_std_f64(const int8_t* codes, int64_t ld_codes, int64_t n,
+                                      int64_t m, const double* mean, const double* sd, double* K,
+                                      int64_t ldk, void* workspace, int64_t workspace_bytes,
+                                      uintptr_t stream);
+
 /* Symmetrise from the lower triangle and scale: K = K * scale (ldk). */
 int32_t jb_kinship_finalize(double* K, int64_t n, int64_t ldk, double scale,
                             uintptr_t stream);

@@ -3,6 +3,7 @@
 Public API (same names, arguments and error behaviour as jamma 2.0.1):
 
 - :func:`compute_centered_kinship` -- GEMMA -gk 1 relatedness matrix
+- :func:`compute_standardized_kinship` -- GEMMA -gk 2 relatedness matrix
 - :func:`eigendecompose_kinship` -- FP64 eigendecomposition with jamma's thresholding
 - :func:`run_lmm_association_streaming`, :func:`run_lmm_association_jax` -- -lmm 1..4
 - :func:`gwas` -- one-call pipeline (kinship -> eigen -> association -> .assoc.txt)
@@ -16,11 +17,17 @@ from jamma_b200.io import (
     AssocResult,
     IncrementalAssocWriter,
     read_covariate_file,
+    read_eigen_files,
     read_kinship_matrix,
     write_assoc_results,
+    write_eigen_files,
     write_kinship_matrix,
 )
-from jamma_b200.kinship import compute_centered_kinship, compute_kinship_from_bed
+from jamma_b200.kinship import (
+    compute_centered_kinship,
+    compute_kinship_from_bed,
+    compute_standardized_kinship,
+)
 from jamma_b200.lmm import run_lmm_association_jax, run_lmm_association_streaming
 
 __version__ = "0.1.0"
@@ -37,12 +44,15 @@ __all__ = [
     "IncrementalAssocWriter",
     "compute_centered_kinship",
     "compute_kinship_from_bed",
+    "compute_standardized_kinship",
     "eigendecompose_kinship",
     "gwas",
     "read_covariate_file",
+    "read_eigen_files",
     "read_kinship_matrix",
     "run_lmm_association_jax",
     "run_lmm_association_streaming",
     "write_assoc_results",
+    "write_eigen_files",
     "write_kinship_matrix",
 ]

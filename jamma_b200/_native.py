@@ -47,6 +47,7 @@ SIGNATURES: dict[str, tuple] = {
     "jb_pack_codes": (_i32, [_p, _i64, _i64, _i64, _p, _i64, _u]),
     "jb_kinship_f64_workspace_size": (_i64, [_i64, _i64]),
     "jb_kinship_accumulate_f64": (_i32, [_p, _i64, _i64, _i64, _p, _p, _i64, _p, _i64, _u]),
+    "jb_kinship_accumulate_std_f64": (_i32, [_p, _i64, _i64, _i64, _p, _p, _p, _i64, _p, _i64, _u]),
     "jb_kinship_finalize": (_i32, [_p, _i64, _i64, _f64, _u]),
     "jb_eigh_workspace_size": (_i64, [_i64]),
     "jb_eigh_f64": (_i32, [_p, _i64, _i64, _p, _f64, _p, _i64, _u]),

@@ -170,15 +170,19 @@ __global__ void impute_f64_kernel(const int8_t* __restrict__ codes, int64_t ldc,
     }
 }
 
+// Centred (sd == NULL) or standardized FP64 batch: x - mean[j] for observed codes, 0 for
+// missing ones (imputed to the mean), divided by sd[j] when given (0 where sd[j] == 0).
 __global__ void center_f64_kernel(const int8_t* __restrict__ codes, int64_t ldc, int64_t n,
                                   int64_t m, const double* __restrict__ mean,
-                                  double* __restrict__ X) {
+                                  const double* __restrict__ sd, double* __restrict__ X) {
     const int64_t j = blockIdx.y;
     const double mu = mean[j];
+    const double s = sd ? sd[j] : 1.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
          i += (int64_t)gridDim.x * blockDim.x) {
         const int8_t c = codes[j * ldc + i];
-        X[j * n + i] = (c == 3) ? 0.0 : ((double)c - mu);
+        const double v = (c == 3) ? 0.0 : ((double)c - mu);
+        X[j * n + i] = sd ? (s > 0.0 ? v / s : 0.0) : v;
     }
 }
 
@@ -275,17 +279,18 @@ int32_t jb_impute_f64(const int8_t* codes, int64_t ld_codes, int64_t n, int64_t 
 
 int64_t jb_kinship_f64_workspace_size(int64_t n, int64_t m) { return n * m * 8; }
 
-int32_t jb_kinship_accumulate_f64(const int8_t* codes, int64_t ld_codes, int64_t n, int64_t m,
-                                  const double* mean, double* K, int64_t ldk, void* workspace,
-                                  int64_t workspace_bytes, uintptr_t stream) {
-    JB_CHECK_ARG(n > 0 && m >= 0 && ldk >= n && ld_codes >= n, "jb_kinship_accumulate_f64: bad shape");
+static int32_t kinship_accumulate(const char* name, const int8_t* codes, int64_t ld_codes, int64_t n,
+                                  int64_t m, const double* mean, const double* sd, double* K,
+                                  int64_t ldk, void* workspace, int64_t workspace_bytes,
+                                  uintptr_t stream) {
+    JB_CHECK_ARG(n > 0 && m >= 0 && ldk >= n && ld_codes >= n, "%s: bad shape", name);
     if (m == 0) return JB_OK;
-    JB_CHECK_ARG(m < 65536, "jb_kinship_accumulate_f64: m must be < 65536 per call");
+    JB_CHECK_ARG(m < 65536, "%s: m must be < 65536 per call", name);
     JB_CHECK_ARG(workspace_bytes >= jb_kinship_f64_workspace_size(n, m),
-                 "jb_kinship_accumulate_f64: workspace too small");
+                 "%s: workspace too small", name);
     double* X = static_cast<double*>(workspace);
     center_f64_kernel<<<col_grid(n, m), 256, 0, as_stream(stream)>>>(codes, ld_codes, n, m, mean,
-                                                                    X);
+                                                                    sd, X);
     JB_LAUNCH_CHECK("center_f64_kernel");
     cublasHandle_t h = cublas_handle();
     if (!h) {
@@ -300,6 +305,21 @@ int32_t jb_kinship_accumulate_f64(const int8_t* codes, int64_t ld_codes, int64_t
                     K, (int)ldk);
     if (s != CUBLAS_STATUS_SUCCESS) return cublas_status(s, "cublasDsyrk");
     return JB_OK;
+}
+
+int32_t jb_kinship_accumulate_f64(const int8_t* codes, int64_t ld_codes, int64_t n, int64_t m,
+                                  const double* mean, double* K, int64_t ldk, void* workspace,
+                                  int64_t workspace_bytes, uintptr_t stream) {
+    return kinship_accumulate("jb_kinship_accumulate_f64", codes, ld_codes, n, m, mean, nullptr, K,
+                              ldk, workspace, workspace_bytes, stream);
+}
+
+int32_t jb_kinship_accumulate_std_f64(const int8_t* codes, int64_t ld_codes, int64_t n, int64_t m,
+                                      const double* mean, const double* sd, double* K, int64_t ldk,
+                                      void* workspace, int64_t workspace_bytes, uintptr_t stream) {
+    JB_CHECK_ARG(sd != nullptr, "jb_kinship_accumulate_std_f64: sd is required");
+    return kinship_accumulate("jb_kinship_accumulate_std_f64", codes, ld_codes, n, m, mean, sd, K,
+                              ldk, workspace, workspace_bytes, stream);
 }
 
 int32_t jb_kinship_finalize(double* K, int64_t n, int64_t ldk, double scale, uintptr_t stream) {

@@ -17,8 +17,10 @@ from jamma_b200.io import (
     AssocResult,
     get_plink_metadata,
     read_covariate_file,
+    read_eigen_files,
     read_kinship_matrix,
     read_phenotypes,
+    write_eigen_files,
     write_kinship_matrix,
 )
 from jamma_b200.kinship import compute_kinship_from_bed
@@ -64,29 +66,34 @@ def gwas(bfile, *, kinship_file=None, covariate_file=None, lmm_mode: int = 1, ma
         cov, _ = read_covariate_file(covariate_file)
         if cov.shape[0] != n:
             raise ValueError(f"Covariate file has {cov.shape[0]} rows but .fam has {n} samples")
+    ks = None
+    if ksnps_file is not None:
+        ks = np.array(sorted(pos[s] for s in _read_snp_list(ksnps_file) if s in pos), dtype=np.int64)
     evals = evecs = K = None
     if loco:
         pass
     elif eigenvalue_file is not None:
-        evals = np.loadtxt(eigenvalue_file, dtype=np.float64)
-        evecs = np.loadtxt(eigenvector_file, dtype=np.float64)
-    elif kinship_file is not None:
-        K = read_kinship_matrix(kinship_file, n_samples=n)
+        evals, evecs = read_eigen_files(eigenvalue_file, eigenvector_file)
     else:
-        if ksnps_file is not None:
-            raise NotImplementedError("-ksnps kinship restriction is not available in this build")
-        K = compute_kinship_from_bed(bfile)
-        if save_kinship:
-            write_kinship_matrix(K, Path(output_dir) / f"{output_prefix}.cXX.txt")
+        if kinship_file is not None:
+            K = read_kinship_matrix(kinship_file, n_samples=n)
+        else:
+            K = compute_kinship_from_bed(bfile, ksnps_indices=ks)
+            if save_kinship:
+                write_kinship_matrix(K, Path(output_dir) / f"{output_prefix}.cXX.txt")
+        if write_eigen:  # eigen files of the analysed samples (pipeline.py:549-566)
+            from jamma_b200.eigen import eigendecompose_kinship
+
+            valid = ~np.isnan(y) & (y != -9.0)
+            Kv = K if np.all(valid) else K[np.ix_(valid, valid)]
+            evals, evecs = eigendecompose_kinship(Kv, check_memory=check_memory)
+            write_eigen_files(evals, evecs, output_dir, output_prefix)
     t_k = time.perf_counter()
     out = Path(output_dir) / f"{output_prefix}.assoc.txt"
     timing: dict = {}
     if loco:
         from jamma_b200.loco import run_lmm_loco
 
-        ks = None
-        if ksnps_file is not None:
-            ks = np.array(sorted(pos[s] for s in _read_snp_list(ksnps_file) if s in pos), dtype=np.int64)
         res = run_lmm_loco(bfile, y, covariates=cov, maf_threshold=maf, miss_threshold=miss,
                            lmm_mode=lmm_mode, output_path=out, save_kinship=save_kinship,
                            kinship_output_dir=Path(output_dir), kinship_output_prefix=output_prefix,

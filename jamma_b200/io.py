@@ -163,6 +163,75 @@ def write_kinship_matrix(k: np.ndarray, path) -> None:
 
 
 # ---------------------------------------------------------------- association text
+def write_eigenvalues(eigenvalues: np.ndarray, path) -> None:
+    """GEMMA .eigenD.txt: one value per line, 10 significant digits
+    (src/jamma/lmm/eigen_io.py WriteVector format)."""
+    path = Path(path)
+    path.parent.mkdir(parents=True, exist_ok=True)
+    with open(path, "w") as f:
+        f.writelines(f"{v:.10g}\n" for v in np.asarray(eigenvalues, dtype=np.float64))
+
+
+def write_eigenvectors(eigenvectors: np.ndarray, path) -> None:
+    """GEMMA .eigenU.txt: tab-separated rows (sample i = row i, eigenvector j = column j),
+    10 significant digits, no header."""
+    path = Path(path)
+    path.parent.mkdir(parents=True, exist_ok=True)
+    with open(path, "w") as f:
+        for row in np.asarray(eigenvectors, dtype=np.float64):
+            f.write("\t".join(f"{v:.10g}" for v in row) + "\n")
+
+
+def write_eigen_files(eigenvalues, eigenvectors, output_dir, prefix: str = "result"):
+    """Write {prefix}.eigenD.txt and {prefix}.eigenU.txt; returns both paths."""
+    d = Path(output_dir) / f"{prefix}.eigenD.txt"
+    u = Path(output_dir) / f"{prefix}.eigenU.txt"
+    write_eigenvalues(eigenvalues, d)
+    write_eigenvectors(eigenvectors, u)
+    return d, u
+
+
+def read_eigen_files(eigenD_path, eigenU_path, n_samples: int | None = None):
+    """Read and cross-check a GEMMA eigen-file pair (counts, squareness, n_samples)."""
+    evals = np.loadtxt(eigenD_path, dtype=np.float64, ndmin=1)
+    evecs = np.loadtxt(eigenU_path, dtype=np.float64, ndmin=2)
+    if evecs.shape[0] != evecs.shape[1]:
+        raise ValueError(f"Eigenvector matrix must be square, got shape {evecs.shape} "
+                         f"from {eigenU_path}")
+    if evals.shape[0] != evecs.shape[0]:
+        raise ValueError(f"Eigenvalue count ({evals.shape[0]}) does not match eigenvector "
+                         f"dimensions {evecs.shape}. Files may be mismatched: "
+                         f"{eigenD_path}, {eigenU_path}")
+    if n_samples is not None and evals.shape[0] != n_samples:
+        raise ValueError(f"Eigenvalue count ({evals.shape[0]}) does not match expected "
+                         f"n_samples={n_samples}. Eigen files may be from a different dataset.")
+    return evals, evecs
+
+
+def write_gemma_log(output_dir, prefix: str, params: dict, timing: dict, command_line: str,
+                    version: str | None = None) -> Path:
+    """GEMMA-style ``{prefix}.log.txt`` with ``##`` section lines (the layout of
+    ``write_gemma_log``, src/jamma/utils/logging.py:51-117): version and date, command
+    line, one ``## key = value`` line per parameter, one ``## key time = s seconds`` line
+    per timing entry."""
+    from datetime import datetime
+
+    if version is None:
+        from jamma_b200 import __version__ as version
+    out = Path(output_dir)
+    out.mkdir(parents=True, exist_ok=True)
+    path = out / f"{prefix}.log.txt"
+    lines = ["##", f"## JAMMA Version = {version}", f"## Date = {datetime.now().isoformat()}",
+             "##", f"## Command Line Input = {command_line}", "##", "## Summary Statistics:"]
+    lines += [f"## {k} = {v}" for k, v in params.items()]
+    lines += ["##", "## Computation Time:"]
+    lines += [f"## {k} time = {v:.2f} seconds" if isinstance(v, float) else f"## {k} time = {v} seconds"
+              for k, v in timing.items()]
+    lines.append("##")
+    path.write_text("\n".join(lines) + "\n")
+    return path
+
+
 @dataclass
 class AssocResult:
     """One SNP's association record (``AssocResult``, src/jamma/lmm/stats.py:39-64)."""

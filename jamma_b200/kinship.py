@@ -1,4 +1,4 @@
-"""Centered kinship (GEMMA -gk 1) on the GPU.
+"""Centered (GEMMA -gk 1) and standardized (-gk 2) kinship on the GPU.
 
 ``compute_centered_kinship`` keeps jamma's signature and semantics
 (src/jamma/kinship/compute.py:93-226): SNPs are filtered by MAF / missing rate /
@@ -36,6 +36,18 @@ def snp_stats_from_counts(counts: np.ndarray, n: int, dtype=np.float32):
     return mean, (n - n_obs).astype(np.int64), poly
 
 
+def snp_sd_from_counts(counts: np.ndarray, n: int) -> np.ndarray:
+    """Per-SNP standard deviation of the mean-imputed genotypes over all n samples, as
+    ``impute_center_and_standardize`` forms it (src/jamma/kinship/missing.py:102-108):
+    var = mean(x_imputed^2) - mean^2 with the float64 mean over observed samples."""
+    n_obs = counts[:, 0].astype(np.float64)
+    s = counts[:, 1].astype(np.float64)
+    sq = counts[:, 2].astype(np.float64) + 4.0 * counts[:, 3].astype(np.float64)
+    mu = np.where(n_obs > 0, s / np.maximum(n_obs, 1), 0.0)
+    var = (sq + (n - n_obs) * mu * mu) / n - mu * mu
+    return np.sqrt(np.maximum(var, 0.0))
+
+
 def filter_mask(mean, miss, poly, n, maf_threshold, miss_threshold):
     """``compute_snp_filter_mask`` (src/jamma/core/snp_filter.py:59-91)."""
     af = np.asarray(mean, dtype=np.float64) / 2.0
@@ -45,7 +57,8 @@ def filter_mask(mean, miss, poly, n, maf_threshold, miss_threshold):
 
 
 class _KinshipAccumulator:
-    """FP64 centered Gram accumulated over SNP batches (``_accumulate_kinship``)."""
+    """FP64 centered (or, given per-SNP sd, standardized) Gram accumulated over SNP
+    batches (``_accumulate_kinship``)."""
 
     def __init__(self, n: int, batch: int):
         self.n, self.batch = n, batch
@@ -53,13 +66,18 @@ class _KinshipAccumulator:
         self.ws = workspace(_native.load().jb_kinship_f64_workspace_size(n, batch))
         self.p = 0
 
-    def add(self, codes: torch.Tensor, means64: torch.Tensor) -> None:
+    def add(self, codes: torch.Tensor, means64: torch.Tensor, sd64: torch.Tensor | None = None) -> None:
         m, ld = codes.shape
         for s in range(0, m, self.batch):
             e = min(s + self.batch, m)
-            _native.call("jb_kinship_accumulate_f64", ptr(codes[s:e]), ld, self.n, e - s,
-                         ptr(means64[s:e]), ptr(self.K), self.n, ptr(self.ws), self.ws.numel(),
-                         stream_handle())
+            if sd64 is None:
+                _native.call("jb_kinship_accumulate_f64", ptr(codes[s:e]), ld, self.n, e - s,
+                             ptr(means64[s:e]), ptr(self.K), self.n, ptr(self.ws), self.ws.numel(),
+                             stream_handle())
+            else:
+                _native.call("jb_kinship_accumulate_std_f64", ptr(codes[s:e]), ld, self.n, e - s,
+                             ptr(means64[s:e]), ptr(sd64[s:e]), ptr(self.K), self.n, ptr(self.ws),
+                             self.ws.numel(), stream_handle())
         self.p += m
 
     def finish(self) -> torch.Tensor:
@@ -136,8 +154,8 @@ class _KinshipI8:
 
 
 def _kinship_from_packed(packed_dev: torch.Tensor, n: int, batch_size: int, maf_threshold: float,
-                         miss_threshold: float, stat_dtype, precision: str = "fp64"
-                         ) -> tuple[torch.Tensor, int]:
+                         miss_threshold: float, stat_dtype, precision: str = "fp64",
+                         standardized: bool = False) -> tuple[torch.Tensor, int]:
     codes, counts = decode_packed(packed_dev, n, None, n)
     mean, miss, poly = snp_stats_from_counts(counts.cpu().numpy(), n, stat_dtype)
     keep, _ = filter_mask(mean, miss, poly, n, maf_threshold, miss_threshold)
@@ -150,6 +168,10 @@ def _kinship_from_packed(packed_dev: torch.Tensor, n: int, batch_size: int, maf_
     c = counts.cpu().numpy()[idx]
     mu64 = torch.from_numpy(c[:, 1] / np.maximum(c[:, 0], 1)).to("cuda")  # float64 nanmean
     sel = torch.from_numpy(idx).to("cuda")
+    if standardized:
+        acc = _KinshipAccumulator(n, max(1, min(batch_size, 8192)))
+        acc.add(codes.index_select(0, sel), mu64, torch.from_numpy(snp_sd_from_counts(c, n)).to("cuda"))
+        return acc.finish(), idx.size
     if precision == "int8":
         acc = _KinshipI8(n, idx.size)
         acc.add(codes.index_select(0, sel), mu64, bool(np.any(c[:, 0] < n)),
@@ -159,6 +181,28 @@ def _kinship_from_packed(packed_dev: torch.Tensor, n: int, batch_size: int, maf_
     acc = _KinshipAccumulator(n, max(1, min(batch_size, 8192)))
     acc.add(codes.index_select(0, sel), mu64)
     return acc.finish(), idx.size
+
+
+def compute_standardized_kinship(genotypes: np.ndarray, batch_size: int = 10000,
+                                 maf_threshold: float = 0.0, miss_threshold: float = 1.0,
+                                 check_memory: bool = True) -> np.ndarray:
+    """GEMMA -gk 2 relatedness matrix of an in-memory (n, p) genotype matrix.
+
+    Keeps ``compute_standardized_kinship``'s signature and semantics
+    (src/jamma/kinship/compute.py:229-360): the same SNP filter as -gk 1, then each kept
+    SNP is mean-imputed, centred and divided by its standard deviation over all samples
+    (``impute_center_and_standardize``, src/jamma/kinship/missing.py:64-119), and
+    K = Z Z^T / p_kept.  FP64 on the device (per-SNP weights do not fit an exact integer
+    Gram).
+    """
+    require_cuda()
+    g = np.asarray(genotypes)
+    n = g.shape[0]
+    stat_dtype = np.float32 if g.dtype == np.float32 else np.float64
+    packed = torch.from_numpy(pack_genotypes(g)).to("cuda")
+    K, _ = _kinship_from_packed(packed, n, batch_size, maf_threshold, miss_threshold, stat_dtype,
+                                "fp64", standardized=True)
+    return K.cpu().numpy()
 
 
 def compute_centered_kinship(genotypes: np.ndarray, batch_size: int = 10000,
@@ -183,11 +227,19 @@ def compute_centered_kinship(genotypes: np.ndarray, batch_size: int = 10000,
 
 def compute_kinship_from_bed(bfile, maf_threshold: float = 0.0, miss_threshold: float = 1.0,
                              chunk_size: int = 10000, sample_idx: np.ndarray | None = None,
-                             as_device: bool = False, precision: str = "fp64"):
-    """Centered kinship streamed from a .bed file (``compute_kinship_streaming``,
+                             as_device: bool = False, precision: str = "fp64",
+                             kinship_mode: int = 1, ksnps_indices: np.ndarray | None = None):
+    """Kinship streamed from a .bed file (``compute_kinship_streaming``,
     src/jamma/kinship/compute.py:502-690): pass 1 statistics, pass 2 accumulation,
     both decoded on the device.  Pass-1 means are float32 as in jamma's streaming path.
+
+    ``kinship_mode`` 1 = centered (-gk 1), 2 = standardized (-gk 2, FP64 only);
+    ``ksnps_indices`` restricts the kinship to those SNP columns (-ksnps).
     """
+    if kinship_mode not in (1, 2):
+        raise ValueError(f"invalid kinship mode {kinship_mode}; use 1 or 2")
+    if kinship_mode == 2 and precision != "fp64":
+        raise ValueError("standardized kinship (-gk 2) is computed in FP64 only")
     require_cuda()
     bed = BedFile(bfile)
     n = bed.n_samples if sample_idx is None else len(sample_idx)
@@ -201,6 +253,10 @@ def compute_kinship_from_bed(bfile, maf_threshold: float = 0.0, miss_threshold: 
     counts = np.concatenate(counts)
     mean, miss, poly = snp_stats_from_counts(counts, n, np.float32)
     keep, _ = filter_mask(mean, miss, poly, n, maf_threshold, miss_threshold)
+    if ksnps_indices is not None:
+        sub_mask = np.zeros(bed.n_snps, dtype=bool)
+        sub_mask[np.asarray(ksnps_indices, dtype=np.int64)] = True
+        keep &= sub_mask
     idx = np.where(keep)[0]
     if idx.size == 0:
         raise ValueError("No SNPs passed filtering")
@@ -215,6 +271,8 @@ def compute_kinship_from_bed(bfile, maf_threshold: float = 0.0, miss_threshold: 
         if i8:
             acc.add(codes, mu64, bool(np.any(c[:, 0] < n)), None if sidx is not None else rec)
             acc.add_sum_mu2(c[:, 1] / np.maximum(c[:, 0], 1))
+        elif kinship_mode == 2:
+            acc.add(codes, mu64, torch.from_numpy(snp_sd_from_counts(c, n)).to("cuda"))
         else:
             acc.add(codes, mu64)
     K = acc.finish()

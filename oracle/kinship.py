@@ -105,3 +105,34 @@ def loco_kinships(g: np.ndarray, chroms, maf_threshold: float = 0.0, miss_thresh
             raise ValueError(f"all filtered SNPs are on chromosome {c}")
         s_c = xc[:, sel] @ xc[:, sel].T
         yield c, (s_full - s_c) / p_loco
+
+
+def standardized_kinship(g: np.ndarray, batch_size: int = 10000, maf_threshold: float = 0.0,
+                         miss_threshold: float = 1.0) -> np.ndarray:
+    """GEMMA -gk 2 standardized relatedness matrix, FP64.
+
+    Restates ``compute_standardized_kinship`` (``src/jamma/kinship/compute.py:229-360``):
+    the same SNP filter as -gk 1 (stats in the input dtype, monomorphic SNPs dropped), then
+    per batch ``impute_center_and_standardize`` (``src/jamma/kinship/missing.py:64-119``):
+    float64 nanmean, NaN -> mean, centre, var = mean over all n of x_imputed^2 - mean^2,
+    z = centred / sqrt(var) (0 where the sd is 0); ``K += Z Z^T``; finally ``K /= p_kept``.
+    """
+    n, _ = g.shape
+    mean, miss, var = snp_stats(g)
+    mask, _ = filter_mask(mean, miss, var, n, maf_threshold, miss_threshold)
+    p = int(mask.sum())
+    if p == 0:
+        raise ValueError("No SNPs passed filtering")
+    x = np.asarray(g[:, mask], dtype=np.float64)
+    k = np.zeros((n, n))
+    for s in range(0, p, batch_size):
+        xb = x[:, s : s + batch_size]
+        with np.testing.suppress_warnings() as sup:
+            sup.filter(RuntimeWarning)
+            mu = np.nan_to_num(np.nanmean(xb, axis=0, keepdims=True), nan=0.0)
+        xi = np.where(np.isnan(xb), mu, xb)
+        sd = np.sqrt(np.mean(xi * xi, axis=0, keepdims=True) - mu * mu)
+        with np.errstate(invalid="ignore", divide="ignore"):
+            z = np.where(sd > 0, (xi - mu) / sd, 0.0)
+        k += z @ z.T
+    return k / p

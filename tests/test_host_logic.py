@@ -104,3 +104,22 @@ def test_bed_file_roundtrip(tmp_path):
     (tmp_path / "t.bed").write_bytes((tmp_path / "t.bed").read_bytes()[:-1])
     with pytest.raises(ValueError):
         jio.BedFile(tmp_path / "t")
+
+
+def test_sd_from_counts_matches_imputed_variance():
+    """sd per SNP from device counts == sqrt(mean(x_imputed^2) - mean^2) over all samples."""
+    from jamma_b200.kinship import snp_sd_from_counts
+
+    rng = np.random.default_rng(4)
+    g = rng.binomial(2, 0.3, size=(50, 40)).astype(float)
+    g[rng.random(g.shape) < 0.1] = np.nan
+    g[:, 3] = 1.0  # monomorphic
+    obs = ~np.isnan(g)
+    gz = np.nan_to_num(g)
+    counts = np.column_stack([obs.sum(0), gz.sum(0), (gz == 1).sum(0), (gz == 2).sum(0)])
+    sd = snp_sd_from_counts(counts, 50)
+    mu = np.nanmean(g, axis=0)
+    gi = np.where(obs, g, mu)
+    ref = np.sqrt(np.maximum(np.mean(gi**2, axis=0) - mu**2, 0))
+    np.testing.assert_allclose(sd, ref, rtol=1e-13, atol=1e-15)
+    assert sd[3] == 0.0

@@ -102,3 +102,27 @@ def test_golden_refine_is_deterministic_and_bracketed():
     lam, val = OL.golden_refine(f, grid, ll, 50, 20)
     np.testing.assert_allclose(lam, 3.0, rtol=5e-5)
     assert np.all(val <= 0)
+
+
+def test_standardized_kinship_known_answer():
+    """The reference's hand-computed -gk 2 case (tests/test_kinship_compute.py:257-273):
+    3 samples x 2 SNPs, each SNP mean 1 and variance 2/3 over all samples."""
+    x = np.array([[0.0, 2.0], [1.0, 1.0], [2.0, 0.0]])
+    sd = np.sqrt(2.0 / 3.0)
+    z = np.array([[-1.0 / sd, 1.0 / sd], [0.0, 0.0], [1.0 / sd, -1.0 / sd]])
+    np.testing.assert_allclose(OK.standardized_kinship(x), z @ z.T / 2, rtol=0, atol=1e-12)
+
+
+def test_standardized_kinship_missing_and_monomorphic():
+    """Missing calls are imputed before the variance (they shrink it, n in the
+    denominator); monomorphic SNPs are filtered out of p."""
+    x = np.array([[0.0, 1.0, 2.0], [np.nan, 1.0, 1.0], [2.0, 1.0, 0.0], [1.0, 1.0, np.nan]])
+    k = OK.standardized_kinship(x)
+    cols = []
+    for j in (0, 2):  # SNP 1 is monomorphic and dropped
+        c = x[:, j]
+        mu = np.nanmean(c)
+        ci = np.where(np.isnan(c), mu, c)
+        cols.append((ci - mu) / np.sqrt(np.mean(ci**2) - mu**2))
+    z = np.column_stack(cols)
+    np.testing.assert_allclose(k, z @ z.T / 2, rtol=1e-13, atol=1e-14)
