@@ -279,7 +279,7 @@ typedef struct jb_lmm_out {
  * precision 2, partly by jb_lmm_chunk_series_i8) before the per-SNP kernel runs.
  * precision: 0 = every likelihood evaluation is a direct FP64 reduction over n (plain
  * form; grid, ones and null rows by DGEMM);
- * 1 = mixed form: the c+2 genotype-dependent sums are a degree-127 Chebyshev series in
+ * 1 = mixed form: the c+2 genotype-dependent sums are a degree-95 Chebyshev series in
  * log lambda over [1e-5, 1e5] whose coefficients come from the chunk DGEMMs; log|H^-1|
  * and the genotype-free sums come from per-bracket degree-24 expansions of exact FP64
  * node values (both built by jb_lmm_prepare with precision 1); grid points and golden
@@ -327,6 +327,9 @@ int32_t jb_lmm_chunk(int32_t lmm_mode, int32_t precision, int64_t n, int32_t n_c
  * phenotype set (it depends on W and y).
  */
 int64_t jb_lmm_series_workspace_size(int64_t n, int32_t n_cvt, int32_t phi);
+/* Rows per linear sum in the series tables: the ones row + the series coefficients; the
+ * genotype-side path needs (c + phi) * rows <= n rounded up to 32. */
+int32_t jb_lmm_series_rows(void);
 int32_t jb_lmm_series_prepare(int64_t n, int32_t n_cvt, int32_t phi, int32_t n_grid,
                               const void* workspace, int64_t workspace_bytes, const double* U,
                               int64_t ldu, void* series_ws, int64_t series_bytes,

@@ -63,6 +63,7 @@ SIGNATURES: dict[str, tuple] = {
     "jb_rotate_set_kernel": (_i32, [_i32]),
     "jb_rotate_get_kernel": (_i32, []),
     "jb_lmm_series_workspace_size": (_i64, [_i64, _i32, _i32]),
+    "jb_lmm_series_rows": (_i32, []),
     "jb_lmm_series_prepare": (_i32, [_i64, _i32, _i32, _i32, _p, _i64, _p, _i64, _p, _i64, _u]),
     "jb_lmm_chunk_series_i8": (
         _i32, [_i64, _i32, _i32, _i32, _i64, _p, _i64, _p, _i64, _p, _i32, _p, _i64, _p, _i64, _u]),

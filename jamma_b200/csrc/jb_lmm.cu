@@ -84,9 +84,13 @@ struct Params {
 
 constexpr int kChebN = 25;  // interpolation nodes (degree 24) per bracket
 // Global series of the x-dependent sums: each term 1/(lambda e_i + 1) is analytic in
-// t = log lambda in the strip |Im t| < pi, so over the 23-wide domain a degree-127
-// Chebyshev series converges to ~1e-15 of the sum's scale (Bernstein ellipse rho ~ 1.31).
-constexpr int kChebG = 128;
+// t = log lambda in the strip |Im t| < pi, so over the 23-wide domain a Chebyshev series
+// converges geometrically (Bernstein ellipse rho ~ 1.31): degree 95 leaves ~1e-13 of the
+// sum's scale, far below the ~1e-9 relative error of the INT8-rotated genotypes the sums
+// are formed from, and golden-section decisions match those of exact sums.
+constexpr int kChebG = 96;
+constexpr int kCoefPerLane = kChebG / 32;  // coefficients k = lane + 32 i held by each lane
+static_assert(kChebG % 32 == 0, "series length must be a multiple of the warp size");
 constexpr double kDomainLo = 1e-5, kDomainHi = 1e5;
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -399,9 +403,9 @@ __device__ __forceinline__ void lane_cheb(double x, double& tl, double& t32) {
     t32 = fma(2.0 * t16, t16, -1.0);
 }
 
-// T_k(x) for the kChebG = 128 coefficients a lane owns: k = lane + 32 i, i = 0..3.
+// T_k(x) for the coefficients a lane owns: k = lane + 32 i, i < kCoefPerLane.
 struct LaneT {
-    double t[4];
+    double t[kCoefPerLane];
 };
 __device__ __forceinline__ LaneT lane_cheb_global(double x) {
     const int lane = threadIdx.x & 31;
@@ -411,8 +415,9 @@ __device__ __forceinline__ LaneT lane_cheb_global(double x) {
     LaneT r;
     r.t[0] = tl;
     r.t[1] = fma(2.0 * t32, tl, -(lane == 0 ? t32 : tm));  // T_{l+32}
-    r.t[2] = fma(2.0 * t32, r.t[1], -r.t[0]);             // T_{l+64}
-    r.t[3] = fma(2.0 * t32, r.t[2], -r.t[1]);             // T_{l+96}
+#pragma unroll
+    for (int i = 2; i < kCoefPerLane; ++i)
+        r.t[i] = fma(2.0 * t32, r.t[i - 1], -r.t[i - 2]);   // T_{l+32i}
     return r;
 }
 
@@ -420,7 +425,7 @@ __device__ __forceinline__ LaneT lane_cheb_global(double x) {
 // (lane l holds k = l + 32 i of every series), loaded once per SNP.
 template <int C>
 struct GlobalCoef {
-    double c[Lay<C>::NX][4];
+    double c[Lay<C>::NX][kCoefPerLane];
 };
 template <int C>
 __device__ __forceinline__ GlobalCoef<C> load_global_coef(const Params& p, int64_t j, int f) {
@@ -428,7 +433,7 @@ __device__ __forceinline__ GlobalCoef<C> load_global_coef(const Params& p, int64
     const int64_t cp = C + p.phi;
     GlobalCoef<C> g;
 #pragma unroll
-    for (int i = 0; i < 4; ++i) {
+    for (int i = 0; i < kCoefPerLane; ++i) {
         const int64_t r = 1 + lane + 32 * i;
         const double* rl = p.CL + j * p.ldcl + r * cp;
 #pragma unroll
@@ -447,9 +452,8 @@ __device__ __forceinline__ void coop_xsums(const Params& p, const GlobalCoef<C>&
 #pragma unroll
     for (int q = 0; q < Lay<C>::NX; ++q) {
         double v = g.c[q][0] * T.t[0];
-        v = fma(g.c[q][1], T.t[1], v);
-        v = fma(g.c[q][2], T.t[2], v);
-        v = fma(g.c[q][3], T.t[3], v);
+#pragma unroll
+        for (int i = 1; i < kCoefPerLane; ++i) v = fma(g.c[q][i], T.t[i], v);
         xs[q] = warp_sum(v);
     }
 }
@@ -676,8 +680,18 @@ __device__ __forceinline__ void beta_se(const PabOut<C>& pb, double px_yy, doubl
     se = valid ? sqrt(var) : jnan();
 }
 
+// 4 warps per block; with one covariate at least 5 blocks per SM (<= 102 registers, 20
+// resident warps to hide FP64 and shuffle latency), fewer for wider covariate sets whose
+// per-warp state would otherwise spill.
+constexpr int kPairsThreads = 128;
+template <int C>
+struct PairsOccupancy {
+    static constexpr int kMinBlocks = C == 1 ? 5 : (C == 2 ? 3 : 2);
+};
+
 template <int C, bool INTERP>
-__global__ void __launch_bounds__(256) lmm_pairs_kernel(const Params p) {
+__global__ void __launch_bounds__(kPairsThreads, PairsOccupancy<C>::kMinBlocks)
+    lmm_pairs_kernel(const Params p) {
     using L = Lay<C>;
     const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (wid >= p.m * p.phi) return;
@@ -1261,11 +1275,11 @@ __global__ void linspace_kernel(double* out, double start, double stop, int num)
 template <int C>
 int32_t launch_pairs(const Params& p, cudaStream_t st) {
     const int64_t warps = p.m * p.phi;
-    const int64_t blocks = ceil_div(warps * 32, 256);
+    const int64_t blocks = ceil_div(warps * 32, kPairsThreads);
     if (p.cheb)
-        lmm_pairs_kernel<C, true><<<(unsigned)blocks, 256, 0, st>>>(p);
+        lmm_pairs_kernel<C, true><<<(unsigned)blocks, kPairsThreads, 0, st>>>(p);
     else
-        lmm_pairs_kernel<C, false><<<(unsigned)blocks, 256, 0, st>>>(p);
+        lmm_pairs_kernel<C, false><<<(unsigned)blocks, kPairsThreads, 0, st>>>(p);
     JB_LAUNCH_CHECK("lmm_pairs_kernel");
     return JB_OK;
 }
@@ -1383,6 +1397,8 @@ int64_t jb_lmm_chunk_workspace_size(int64_t n, int32_t n_cvt, int32_t phi, int32
     if (n <= 0 || n_cvt < 1 || phi < 1 || n_grid < 1 || m < 0) return -1;
     return chunk_layout(n, n_cvt, phi, n_grid, m > 0 ? m : 1).total;
 }
+
+int32_t jb_lmm_series_rows(void) { return 1 + kChebG; }
 
 int64_t jb_lmm_series_workspace_size(int64_t n, int32_t n_cvt, int32_t phi) {
     if (n <= 0 || n_cvt < 1 || n_cvt > kMaxCvt || phi < 1) return -1;

@@ -202,15 +202,22 @@ int32_t launch_rot_pair(const CUtensorMap& ta, const CUtensorMap& tb, const Tile
     auto kern = i8_gemm_pair_kernel<kRotPairStages, RotEpi<P>>;
     JB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  PairRotSmem::TOTAL));
-    // persistent: as many pairs as can be resident at once (clusters need two SMs of one GPC)
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3((unsigned)(2 * (num_sms() / 2)));
-    cfg.blockDim = dim3(kThreads);
-    cfg.dynamicSmemBytes = PairRotSmem::TOTAL;
-    cfg.stream = st;
-    int resident = 0;
-    JB_CUDA(cudaOccupancyMaxActiveClusters(&resident, kern, &cfg));
-    JB_CHECK_ARG(resident >= 1, "rotation: no CTA pair fits on the device");
+    // persistent: as many pairs as can be resident at once (clusters need two SMs of one
+    // GPC); queried once per device and kernel, so launches inside graph capture skip it
+    static std::atomic<int> cached[2][64];
+    int dev = 0;
+    JB_CUDA(cudaGetDevice(&dev));
+    int resident = dev < 64 ? cached[P ? 1 : 0][dev].load(std::memory_order_relaxed) : 0;
+    if (resident <= 0) {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(2 * (num_sms() / 2)));
+        cfg.blockDim = dim3(kThreads);
+        cfg.dynamicSmemBytes = PairRotSmem::TOTAL;
+        cfg.stream = st;
+        JB_CUDA(cudaOccupancyMaxActiveClusters(&resident, kern, &cfg));
+        JB_CHECK_ARG(resident >= 1, "rotation: no CTA pair fits on the device");
+        if (dev < 64) cached[P ? 1 : 0][dev].store(resident, std::memory_order_relaxed);
+    }
     const int pairs = n_tiles < resident ? n_tiles : resident;
     kern<<<2 * pairs, kThreads, PairRotSmem::TOTAL, st>>>(ta, tb, tiles, n_tiles, num_kb, epi,
                                                          status);

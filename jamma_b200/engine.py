@@ -35,7 +35,6 @@ MAX_CVT = 4
 NULL_L_MIN, NULL_L_MAX, NULL_N_GRID, NULL_N_ITER = 1e-5, 1e5, 50, 20
 # log-lambda domain of the mixed form's series tables (jb_lmm_prepare precision 1)
 SERIES_L_MIN, SERIES_L_MAX = 1e-5, 1e5
-SERIES_ROWS = 1 + 128  # ones row + Chebyshev coefficients per linear sum
 
 
 def eigh_device(K: torch.Tensor, threshold: float = 1e-10) -> tuple[torch.Tensor, torch.Tensor]:
@@ -147,7 +146,8 @@ class DeviceCohort:
         # from the int8 calls (basis U A_lin^T split into digit planes once per cohort).
         self.series_ws = None
         self._series_for = None
-        if self.search == 1 and SERIES_ROWS * (c + phi) <= (n + 31) // 32 * 32:
+        series_rows = _native.load().jb_lmm_series_rows()  # ones row + series coefficients
+        if self.search == 1 and series_rows * (c + phi) <= (n + 31) // 32 * 32:
             self.series_ws = workspace(_native.load().jb_lmm_series_workspace_size(n, c, phi))
             _native.call("jb_lmm_series_prepare", n, c, phi, self.n_grid, ptr(self.ws), self.ws.numel(),
                          ptr(self.U), n, ptr(self.series_ws), self.series_ws.numel(), st)
@@ -246,11 +246,14 @@ class ChunkGraph:
     packed .bed records, rotation (INT8 tensor cores or FP64), the series sums and the
     per-SNP search with its statistics -- so a replay is one launch from the host instead
     of the eight to ten kernel and library launches of an eager chunk.  Fill ``packed``
-    (m, bytes_per_snp) and ``means`` (m,) (e.g. by non-blocking copies from pinned host
-    memory on the replaying stream), call :meth:`replay`, read ``out``.
+    (m, bytes_per_snp) and ``means`` (m,) on the replaying stream (e.g. non-blocking
+    copies from pinned host memory), call :meth:`replay`, read ``out``.  Work queued on one
+    stream is ordered, so refilling the inputs for the next chunk right after a replay is
+    safe; a chunk shorter than ``m`` uses the first rows and ignores the rest.
 
-    ``m`` is fixed at capture; a shorter final chunk is run eagerly.  The graph keeps the
-    cohort's workspaces alive; capture after any eager chunk larger than ``m`` so that
+    Capture runs on a private stream without synchronising the device, with thread-local
+    capture rules, so other streams and threads keep working meanwhile.  The graph keeps
+    the cohort's workspaces alive; capture after any eager chunk larger than ``m`` so that
     no workspace is reallocated afterwards.
     """
 
@@ -262,24 +265,33 @@ class ChunkGraph:
         self.has_missing = bool(has_missing)
         self.packed = torch.zeros((m, (n_file + 3) // 4), dtype=torch.uint8, device="cuda")
         self.means = torch.zeros((m,), dtype=torch.float64, device="cuda")
+        self.codes = torch.zeros((m, cohort.code_ld), dtype=torch.int8, device="cuda")
+        self.counts = torch.zeros((m, 4), dtype=torch.int32, device="cuda")
         self.out = cohort.alloc_out(m)
-        self.bufs = {"UtG": empty((m, n)), "G": empty((m, n)) if cohort.precision != "mixed" else None}
+        self.bufs = {"UtG": empty((m, n))}
+        if cohort.precision != "mixed":
+            self.bufs["G"] = empty((m, n))
+        caller = torch.cuda.current_stream()
         side = torch.cuda.Stream()
-        side.wait_stream(torch.cuda.current_stream())
-        with torch.cuda.stream(side):  # eager warm-up: workspaces, handles, kernel attributes
-            self._run()
-        torch.cuda.current_stream().wait_stream(side)
-        torch.cuda.synchronize()
-        self._keep = (cohort.ws, cohort._chunk_ws, cohort._rot_ws, cohort.series_ws, cohort.ozaki)
-        self.graph = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(self.graph):
-            self._run()
+        side.wait_stream(caller)
+        with torch.cuda.stream(side):
+            self._run()  # eager warm-up: workspaces, library handles, kernel attributes
+            self._keep = (cohort.ws, cohort._chunk_ws, cohort._rot_ws, cohort.series_ws,
+                          cohort.ozaki)
+            self.graph = torch.cuda.CUDAGraph()
+            self.graph.capture_begin(capture_error_mode="thread_local")
+            try:
+                self._run()
+            finally:
+                self.graph.capture_end()
+        caller.wait_stream(side)
 
     def _run(self) -> None:
         c = self.cohort
-        codes, _ = decode_packed(self.packed, self.n_file, self.sample_idx, c.n, ld=c.code_ld)
-        c.associate_codes(codes, self.means, out=self.out,
-                          bufs={k: v for k, v in self.bufs.items() if v is not None},
+        _native.call("jb_decode_bed", ptr(self.packed), self.packed.shape[1], self.m,
+                     ptr(self.sample_idx), c.n, ptr(self.codes), c.code_ld, ptr(self.counts),
+                     stream_handle())
+        c.associate_codes(self.codes, self.means, out=self.out, bufs=self.bufs,
                           has_missing=self.has_missing)
 
     def replay(self) -> dict:

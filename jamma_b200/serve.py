@@ -223,7 +223,9 @@ class GwasServer:
             act.packed_host = torch.from_numpy(np.ascontiguousarray(job.packed[idx])).pin_memory()
             act.means = torch.from_numpy(mean[idx].astype(np.float64)).pin_memory()
             act.n_miss = miss[idx]
-            act.bufs = {"UtG": empty((self.chunk, n))}
+            # the job's chunk work as one CUDA graph, replayed for every chunk
+            act.graph = eng.ChunkGraph(act.cohort, min(self.chunk, max(1, idx.size)),
+                                       has_missing=True)
         job.snp_indices = idx
         job.results = {k: np.empty((act.cohort.phi, idx.size)) for k in eng.MODE_KEYS[job.lmm_mode]}
         job.af, job.n_miss = af[idx], miss[idx]
@@ -235,19 +237,20 @@ class GwasServer:
         s = act.chunk_starts[act.next]
         e = min(s + self.chunk, act.job.snp_indices.size)
         act.next += 1
-        n = act.job.n_samples
+        g = act.graph
         with torch.cuda.stream(act.stream):
-            rec = act.packed_host[s:e].to("cuda", non_blocking=True)
-            mu = act.means[s:e].to("cuda", non_blocking=True)
-            codes, _ = eng.decode_packed(rec, n, None, n, ld=act.cohort.code_ld)
-            out = act.cohort.associate_codes(codes, mu, bufs=act.bufs,
-                                             has_missing=bool(np.any(act.n_miss[s:e] > 0)))
-            host = {k: torch.empty(v.shape, dtype=torch.float64).pin_memory() for k, v in out.items()}
+            # stream order: these copies wait for the previous replay to finish with the
+            # static buffers, and the next chunk's copies wait for this replay
+            g.packed[: e - s].copy_(act.packed_host[s:e], non_blocking=True)
+            g.means[: e - s].copy_(act.means[s:e], non_blocking=True)
+            out = g.replay()
+            host = {k: torch.empty((v.shape[0], e - s), dtype=torch.float64).pin_memory()
+                    for k, v in out.items()}
             for k, v in out.items():
-                host[k].copy_(v, non_blocking=True)
+                host[k].copy_(v[:, : e - s], non_blocking=True)
             ev = torch.cuda.Event()
             ev.record(act.stream)
-        act.inflight.append((ev, host, s, e, rec, mu, codes, out))
+        act.inflight.append((ev, host, s, e))
 
     def _poll(self, act: _Active) -> bool:
         """Collect finished chunks; returns True when the job is complete."""
