@@ -322,8 +322,12 @@ def run_ours(args) -> None:
 
     torch.cuda.synchronize()
     t = time.perf_counter()
+    if args.profile_phase == "kinship":  # the INT8 kinship is the profiler range
+        torch.cuda.profiler.start()
     K = kinship("int8")
     torch.cuda.synchronize()
+    if args.profile_phase == "kinship":
+        torch.cuda.profiler.stop()
     kinship_s = time.perf_counter() - t
     kinship_fp64_s = None
     if not args.skip_fp64_kinship:
@@ -397,7 +401,7 @@ def run_ours(args) -> None:
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         # the mixed form's timed steps are the profiler range (ncu --profile-from-start off)
-        prof = precision == "mixed"
+        prof = precision == "mixed" and args.profile_phase == "assoc"
         with ClockSampler(local) as clk:
             if prof:
                 torch.cuda.profiler.start()
@@ -634,6 +638,8 @@ def main():
     ap.add_argument("--pheno-chunk", type=int, default=2048)
     ap.add_argument("--pheno-mode", type=int, default=4)
     ap.add_argument("--no-autotune", action="store_true")
+    ap.add_argument("--profile-phase", choices=["assoc", "kinship"], default="assoc",
+                    help="which phase torch.cuda.profiler.start/stop brackets")
     ap.add_argument("--rot-kernel", type=int, choices=[0, 1], default=None,
                     help="fix the INT8 rotation kernel (0 one CTA per tile, 1 CTA pairs)")
     args = ap.parse_args()

@@ -224,12 +224,12 @@ int32_t jb_rotate_get_kernel(void);
 /*
  * Mixed-precision rotation on INT8 tensor cores (replaces the host UT @ G of
  * src/jamma/lmm/runner_streaming.py:409).  jb_ozaki_prepare splits the eigenvectors U
- * (n x n, column-major, ldu) once per cohort into four exact int8 digit planes with a
+ * (n x n, column-major, ldu) once per cohort into four int8 digit planes (base 254) with a
  * per-eigenvector scale (ozaki workspace: jb_ozaki_workspace_size).  jb_rotate_i8 then
  * forms X = U^T G for m SNPs given as decoded codes (SNP-major, ld_codes a multiple of
  * 16; 3 = missing, mean-imputed with mean[j] without centring): every digit product
  * accumulates exactly in int32 on tcgen05 and the epilogue recombines in FP64
- * (|error| <= ~2^-29 max|U_col| * sum|g|).  has_missing = 0 promises the chunk holds
+ * (|error| <= ~2.4e-10 max|U_col| * sum|g|: four base-254 digits).  has_missing = 0 promises the chunk holds
  * no missing call.  workspace: jb_rotate_i8_workspace_size(n, m); its first int32 is a
  * pipeline status word (0 = OK), read with jb_rotate_status (synchronises).
  */

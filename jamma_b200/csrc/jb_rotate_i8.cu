@@ -1,10 +1,12 @@
 // Mixed-precision eigenvector rotation x~ = U^T g on INT8 tensor cores.
 //
 // Each eigenvector u_i (column i of U) is scaled by s_i = max_k |U_ki| / 127 and split
-// into four signed 8-bit digit planes, U_ki = s_i * sum_{t<4} q_t(k,i) 128^-t (+ error
-// below s_i * 2^-22); the split is exact arithmetic in FP64.  Genotype calls are exact
-// int8 values, so every digit product  C_t = q_t^T z  accumulates exactly in int32 on
-// tcgen05 (kind::i8), and the epilogue recombines  x~_i = s_i * sum_t 128^-t C_t  in FP64.
+// into four signed 8-bit digit planes in base 254, U_ki = s_i * sum_{t<4} q_t(k,i) 254^-t
+// (+ error below s_i * 0.5 * 254^-3, i.e. ~2.4e-10 of max |U_ki|): with round-to-nearest
+// digits every remainder lies in [-0.5, 0.5], so the next digit (remainder * 254) stays
+// within [-127, 127].  Genotype calls are exact int8 values, so every digit product
+// C_t = q_t^T z accumulates exactly in int32 on tcgen05 (kind::i8; |C_t| <= 254 n), and the
+// epilogue recombines  x~_i = s_i * sum_t 254^-t C_t  in FP64.
 //
 // Missing calls are mean-imputed without centring (src/jamma/lmm/runner_streaming.py:
 // 427-434): g_j = z_j + mu_j m_j with m_j the missing mask, so  x~ = U^T z + mu_j U^T m.
@@ -29,6 +31,10 @@ int32_t make_map_i8(CUtensorMap* map, const void* base, int64_t rows, int64_t k,
                     int box_rows);
 int num_sms();
 
+constexpr double kDigitBase = 254.0;
+// 254^-t, t = 0..3, for the FP64 recombination of the digit products
+__device__ __constant__ double kDigitWeight[4] = {1.0, 1.0 / 254.0, 1.0 / (254.0 * 254.0),
+                                                  1.0 / (254.0 * 254.0 * 254.0)};
 constexpr int kRotBN = 256;
 constexpr int kRotStages = 4;
 constexpr int kRotPairStages = 6;
@@ -66,8 +72,8 @@ __global__ void ozaki_split_kernel(const double* __restrict__ U, int64_t n, int6
 #pragma unroll
             for (int t = 0; t < 4; ++t) {
                 const double r = rint(a);
-                q[t] = (int8_t)r;
-                a = (a - r) * 128.0;  // exact; |a| <= 64
+                q[t] = (int8_t)r;             // |r| <= 127
+                a = (a - r) * kDigitBase;     // a - r exact, |a - r| <= 0.5 -> |a| <= 127
             }
         }
 #pragma unroll
@@ -126,7 +132,7 @@ struct RotEpi {
         const int i = mb * 32 + lane;                 // eigenvector of this lane (any digit)
         constexpr int kCols = PAIRED ? 128 : 256;
         const int j_base = nb * kCols;
-        const double w = ldexp(1.0, -7 * q);          // 128^-q
+        const double w = kDigitWeight[q];              // 254^-q
         double sc = 0.0;
         if (i < n) sc = smax[i] * (1.0 / 127.0);
 #pragma unroll 1
