@@ -123,7 +123,8 @@ int32_t jb_kinship_finalize(double* K, int64_t n, int64_t ldk, double scale,
  *   T is symmetric, so R + R^T + T = Q + Q^T); the missing-call terms read the chunk's
  *   packed .bed records (m x bytes_per_snp, all n samples, same SNP order as codes).
  *   partial: jb_kinship_i8_partial_size(n, m) bytes of scratch for the ordered
- *   (deterministic) two-stage reduction of a and b.
+ *   (deterministic) two-stage reduction of a and b and for each sample's bitmask of
+ *   missing SNPs in the chunk (the sparse pass walks it in SNP order).
  * jb_kinship_i8_finalize: K (n x n, ldk) = symmetric combination above / p_kept.
  */
 int64_t jb_gram_i8_workspace_size(int64_t n);

@@ -184,36 +184,50 @@ __global__ void kin_vectors_reduce_kernel(int64_t n, int64_t nblk, const double*
 }
 
 // Sparse terms for one SNP chunk.  For every sample k and every SNP j of the chunk that
-// is missing at k: Q[:, k] += mu_j Z[:, j] + (mu_j^2 / 2) M[:, j]  (Q = R + T/2).  The
-// SNP columns are read from the 2-bit packed .bed records (4x less traffic than int8
-// codes).  One CTA per (k, block of 2048 samples i); each thread owns 8 consecutive
-// samples (one 16-bit packed load per missing SNP, four loads in flight) and keeps their
-// sums in registers.
-__device__ __forceinline__ void kin_sparse_accum(uint32_t w, double u, double (&r)[8],
-                                                 double (&tt)[8]) {
-    const double u2h = 0.5 * u * u, u2 = 2.0 * u;
+// is missing at k: Q[:, k] += mu_j Z[:, j] + (mu_j^2 / 2) M[:, j]  (Q = R + T/2), i.e. per
+// sample i one add of v_j(code_ij) with v_j = {00: 2 mu_j, 01 (missing): mu_j^2 / 2,
+// 10: mu_j, 11: 0} (count-A1 codes).  SNP columns are read from the 2-bit packed .bed
+// records (4x less traffic than int8 codes).
+//
+// Pass 1 (kin_missing_mask_kernel): each sample's missing SNPs of the chunk as a bitmask
+// (one ballot per 32 SNPs of the sample-major codes), so pass 2 needs no per-block
+// compaction.  Pass 2 (kin_sparse_kernel): one CTA per (k, block of 2048 samples i); the
+// CTA walks k's set bits in increasing SNP order (every thread the same j, so the FP64
+// summation order is fixed) four at a time, each thread owning 8 consecutive samples (one
+// 16-bit packed load per SNP, four in flight).
+__global__ void kin_missing_mask_kernel(const int8_t* __restrict__ Cs, int64_t ldcs, int64_t m,
+                                        uint32_t* __restrict__ mask, int64_t words) {
+    const int64_t k = blockIdx.x;
+    const int lane = threadIdx.x & 31;
+    for (int64_t j0 = 0; j0 < words * 32; j0 += blockDim.x) {
+        const int64_t j = j0 + threadIdx.x;
+        const bool miss = j < m && Cs[k * ldcs + j] == 3;
+        const uint32_t bal = __ballot_sync(0xffffffffu, miss);
+        if (lane == 0 && (j >> 5) < words) mask[k * words + (j >> 5)] = bal;
+    }
+}
+
+__device__ __forceinline__ void kin_sparse_accum(uint32_t w, double u, double (&r)[8]) {
+    const double v0 = 2.0 * u, v1 = 0.5 * u * u;  // codes 00 (two copies), 01 (missing)
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
-        // count-A1 codes: 00 -> 2, 01 -> missing, 10 -> 1, 11 -> 0
         const uint32_t code = (w >> (2 * q)) & 3u;
-        r[q] += code == 0u ? u2 : (code == 2u ? u : 0.0);
-        tt[q] += code == 1u ? u2h : 0.0;
+        r[q] += (code & 2u) ? ((code & 1u) ? 0.0 : u) : ((code & 1u) ? v1 : v0);
     }
 }
 
 __global__ void __launch_bounds__(256) kin_sparse_kernel(const uint8_t* __restrict__ packed,
-                                                          int64_t bps, const int8_t* __restrict__ Cs,
-                                                          int64_t ldcs, int64_t n, int64_t m,
+                                                          int64_t bps,
+                                                          const uint32_t* __restrict__ mask,
+                                                          int64_t words, int64_t n,
                                                           const double* __restrict__ mu,
                                                           double* __restrict__ Q, int64_t ldq) {
     const int64_t k = blockIdx.x;
     const int64_t i0 = (int64_t)blockIdx.y * 2048 + 8 * threadIdx.x;
-    __shared__ int32_t list[2048];
-    __shared__ int wcnt[8];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double r[8], tt[8];
+    const uint32_t* __restrict__ mk = mask + k * words;
+    double r[8];
 #pragma unroll
-    for (int e = 0; e < 8; ++e) r[e] = tt[e] = 0.0;
+    for (int e = 0; e < 8; ++e) r[e] = 0.0;
     const int64_t b0 = i0 >> 2;  // first packed byte of this thread's 8 samples
     const bool full = (i0 + 8 <= n) && ((bps & 1) == 0);
     auto load = [&](int64_t j) -> uint32_t {
@@ -224,49 +238,41 @@ __global__ void __launch_bounds__(256) kin_sparse_kernel(const uint8_t* __restri
             if (b0 + q < bps) w = (w & ~(0xffu << (8 * q))) | ((uint32_t)rec[b0 + q] << (8 * q));
         return w;
     };
-    for (int64_t jb = 0; jb < m; jb += 2048) {
-        // Missing SNPs of sample k in this block, listed in increasing SNP order (ballot +
-        // warp prefix), so the FP64 accumulation order -- and the kinship -- is the same
-        // on every run.
-        int c = 0;
-        for (int64_t r0 = jb; r0 < m && r0 < jb + 2048; r0 += 256) {
-            const int64_t j = r0 + threadIdx.x;
-            const bool miss = j < m && j < jb + 2048 && Cs[k * ldcs + j] == 3;
-            const unsigned bal = __ballot_sync(0xffffffffu, miss);
-            if (lane == 0) wcnt[warp] = __popc(bal);
-            __syncthreads();
-            int off = c, tot = 0;
-#pragma unroll
-            for (int w = 0; w < 8; ++w) {
-                off += w < warp ? wcnt[w] : 0;
-                tot += wcnt[w];
-            }
-            if (miss) list[off + __popc(bal & ((1u << lane) - 1u))] = (int32_t)j;
-            c += tot;
-            __syncthreads();
+    // next missing SNP of sample k in increasing order (uniform across the CTA), -1 at end
+    int64_t wi = -1;
+    uint32_t word = 0;
+    auto next = [&]() -> int64_t {
+        while (word == 0) {
+            if (++wi >= words) return -1;
+            word = __ldg(mk + wi);
         }
-        if (i0 < n) {
-            int e = 0;
-            for (; e + 4 <= c; e += 4) {
-                const int64_t j0 = list[e], j1 = list[e + 1], j2 = list[e + 2], j3 = list[e + 3];
-                const uint32_t w0 = load(j0), w1 = load(j1), w2 = load(j2), w3 = load(j3);
-                const double u0 = mu[j0], u1 = mu[j1], u2 = mu[j2], u3 = mu[j3];
-                kin_sparse_accum(w0, u0, r, tt);
-                kin_sparse_accum(w1, u1, r, tt);
-                kin_sparse_accum(w2, u2, r, tt);
-                kin_sparse_accum(w3, u3, r, tt);
-            }
-            for (; e < c; ++e) {
-                const int64_t j = list[e];
-                kin_sparse_accum(load(j), mu[j], r, tt);
-            }
+        const int b = __ffs(word) - 1;
+        word &= word - 1;
+        return wi * 32 + b;
+    };
+    if (i0 < n) {
+        int64_t j0 = next(), j1 = next(), j2 = next(), j3 = next();
+        while (j3 >= 0) {
+            const uint32_t w0 = load(j0), w1 = load(j1), w2 = load(j2), w3 = load(j3);
+            const double u0 = __ldg(mu + j0), u1 = __ldg(mu + j1), u2 = __ldg(mu + j2),
+                         u3 = __ldg(mu + j3);
+            kin_sparse_accum(w0, u0, r);
+            kin_sparse_accum(w1, u1, r);
+            kin_sparse_accum(w2, u2, r);
+            kin_sparse_accum(w3, u3, r);
+            j0 = next();
+            j1 = next();
+            j2 = next();
+            j3 = next();
         }
-        __syncthreads();
+        if (j0 >= 0) kin_sparse_accum(load(j0), __ldg(mu + j0), r);
+        if (j1 >= 0) kin_sparse_accum(load(j1), __ldg(mu + j1), r);
+        if (j2 >= 0) kin_sparse_accum(load(j2), __ldg(mu + j2), r);
     }
 #pragma unroll
     for (int q = 0; q < 8; ++q) {
         const int64_t i = i0 + q;
-        if (i < n) Q[k * ldq + i] += r[q] + tt[q];  // Q[i, k] (column-major, column k)
+        if (i < n) Q[k * ldq + i] += r[q];  // Q[i, k] (column-major, column k)
     }
 }
 
@@ -485,7 +491,9 @@ int32_t jb_codes_to_sample_major(const int8_t* codes, int64_t ld_codes, int64_t 
 
 int64_t jb_kinship_i8_partial_size(int64_t n, int64_t m) {
     if (n <= 0 || m < 0) return -1;
-    return 2 * ceil_div(m > 0 ? m : 1, 256) * n * 8;
+    const int64_t mm = m > 0 ? m : 1;
+    // FP64 partial sums of the a / b vectors, then the per-sample missing-SNP bitmasks
+    return 2 * ceil_div(mm, 256) * n * 8 + n * ceil_div(mm, 32) * 4;
 }
 
 int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes, const uint8_t* packed,
@@ -510,8 +518,12 @@ int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes, const u
     if (Cs) {
         JB_CHECK_ARG(RT && ldr >= n && ldcs >= m && packed && 4 * bytes_per_snp >= n,
                      "jb_kinship_i8_corrections: Q buffer and packed records needed");
+        const int64_t words = ceil_div(m, 32);
+        uint32_t* mask = reinterpret_cast<uint32_t*>(pb + nblk * n);
+        kin_missing_mask_kernel<<<(unsigned)n, 256, 0, st>>>(Cs, ldcs, m, mask, words);
+        JB_LAUNCH_CHECK("kin_missing_mask_kernel");
         dim3 grid((unsigned)n, (unsigned)ceil_div(n, 2048), 1);
-        kin_sparse_kernel<<<grid, 256, 0, st>>>(packed, bytes_per_snp, Cs, ldcs, n, m, mu, RT, ldr);
+        kin_sparse_kernel<<<grid, 256, 0, st>>>(packed, bytes_per_snp, mask, words, n, mu, RT, ldr);
         JB_LAUNCH_CHECK("kin_sparse_kernel");
     }
     return JB_OK;
