@@ -191,10 +191,10 @@ __global__ void kin_vectors_reduce_kernel(int64_t n, int64_t nblk, const double*
 //
 // Pass 1 (kin_missing_mask_kernel): each sample's missing SNPs of the chunk as a bitmask
 // (one ballot per 32 SNPs of the sample-major codes), so pass 2 needs no per-block
-// compaction.  Pass 2 (kin_sparse_kernel): one CTA per (k, block of 2048 samples i); the
+// compaction.  Pass 2 (kin_sparse_kernel): one CTA per (k, block of 4096 samples i); the
 // CTA walks k's set bits in increasing SNP order (every thread the same j, so the FP64
-// summation order is fixed) four at a time, each thread owning 8 consecutive samples (one
-// 16-bit packed load per SNP, four in flight).
+// summation order is fixed) four at a time, each thread owning 16 consecutive samples (one
+// 32-bit packed load per SNP, four in flight).
 __global__ void kin_missing_mask_kernel(const int8_t* __restrict__ Cs, int64_t ldcs, int64_t m,
                                         uint32_t* __restrict__ mask, int64_t words) {
     const int64_t k = blockIdx.x;
@@ -207,12 +207,21 @@ __global__ void kin_missing_mask_kernel(const int8_t* __restrict__ Cs, int64_t l
     }
 }
 
-__device__ __forceinline__ void kin_sparse_accum(uint32_t w, double u, double (&r)[8]) {
-    const double v0 = 2.0 * u, v1 = 0.5 * u * u;  // codes 00 (two copies), 01 (missing)
+// One SNP j for a thread's kSparseSpt consecutive samples (2 bits each in `w`): call value
+// 0/1/2 as a double built from its high word alone (2.0 and 1.0 have zero low words), one
+// FMA with mu_j, and mu_j^2 / 2 added for a missing call.  mu * call is exact, so the sums
+// equal adding v_j(code) directly.
+constexpr int kSparseSpt = 16;  // samples per thread (one 32-bit packed load)
+
+__device__ __forceinline__ void kin_sparse_accum(uint32_t w, double u, double (&r)[kSparseSpt]) {
+    const double u2h = 0.5 * u * u;
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < kSparseSpt; ++q) {
+        // count-A1 codes: 00 -> 2 copies, 01 -> missing, 10 -> 1 copy, 11 -> 0 copies
         const uint32_t code = (w >> (2 * q)) & 3u;
-        r[q] += (code & 2u) ? ((code & 1u) ? 0.0 : u) : ((code & 1u) ? v1 : v0);
+        const int hi = code == 0u ? 0x40000000 : (code == 2u ? 0x3FF00000 : 0);
+        r[q] = fma(u, __hiloint2double(hi, 0), r[q]);
+        if (code == 1u) r[q] += u2h;
     }
 }
 
@@ -222,19 +231,20 @@ __global__ void __launch_bounds__(256) kin_sparse_kernel(const uint8_t* __restri
                                                           int64_t words, int64_t n,
                                                           const double* __restrict__ mu,
                                                           double* __restrict__ Q, int64_t ldq) {
+    constexpr int kBytes = kSparseSpt / 4;  // packed bytes per thread
     const int64_t k = blockIdx.x;
-    const int64_t i0 = (int64_t)blockIdx.y * 2048 + 8 * threadIdx.x;
+    const int64_t i0 = (int64_t)blockIdx.y * (256 * kSparseSpt) + kSparseSpt * threadIdx.x;
     const uint32_t* __restrict__ mk = mask + k * words;
-    double r[8];
+    double r[kSparseSpt];
 #pragma unroll
-    for (int e = 0; e < 8; ++e) r[e] = 0.0;
-    const int64_t b0 = i0 >> 2;  // first packed byte of this thread's 8 samples
-    const bool full = (i0 + 8 <= n) && ((bps & 1) == 0);
+    for (int e = 0; e < kSparseSpt; ++e) r[e] = 0.0;
+    const int64_t b0 = i0 >> 2;  // first packed byte of this thread's samples
+    const bool full = (i0 + kSparseSpt <= n) && ((bps & 3) == 0);
     auto load = [&](int64_t j) -> uint32_t {
         const uint8_t* rec = packed + j * bps;
-        if (full) return *reinterpret_cast<const uint16_t*>(rec + b0);
-        uint32_t w = 0xffffu;  // padding decodes as 0 copies
-        for (int q = 0; q < 2; ++q)
+        if (full) return *reinterpret_cast<const uint32_t*>(rec + b0);
+        uint32_t w = 0xffffffffu;  // padding decodes as 0 copies
+        for (int q = 0; q < kBytes; ++q)
             if (b0 + q < bps) w = (w & ~(0xffu << (8 * q))) | ((uint32_t)rec[b0 + q] << (8 * q));
         return w;
     };
@@ -270,7 +280,7 @@ __global__ void __launch_bounds__(256) kin_sparse_kernel(const uint8_t* __restri
         if (j2 >= 0) kin_sparse_accum(load(j2), __ldg(mu + j2), r);
     }
 #pragma unroll
-    for (int q = 0; q < 8; ++q) {
+    for (int q = 0; q < kSparseSpt; ++q) {
         const int64_t i = i0 + q;
         if (i < n) Q[k * ldq + i] += r[q];  // Q[i, k] (column-major, column k)
     }
@@ -522,7 +532,7 @@ int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes, const u
         uint32_t* mask = reinterpret_cast<uint32_t*>(pb + nblk * n);
         kin_missing_mask_kernel<<<(unsigned)n, 256, 0, st>>>(Cs, ldcs, m, mask, words);
         JB_LAUNCH_CHECK("kin_missing_mask_kernel");
-        dim3 grid((unsigned)n, (unsigned)ceil_div(n, 2048), 1);
+        dim3 grid((unsigned)n, (unsigned)ceil_div(n, 256 * kSparseSpt), 1);
         kin_sparse_kernel<<<grid, 256, 0, st>>>(packed, bytes_per_snp, mask, words, n, mu, RT, ldr);
         JB_LAUNCH_CHECK("kin_sparse_kernel");
     }
