@@ -127,6 +127,27 @@ int32_t jb_kinship_finalize(double* K, int64_t n, int64_t ldk, double scale,
  *   missing SNPs in the chunk (the sparse pass walks it in SNP order).
  * jb_kinship_i8_finalize: K (n x n, ldk) = symmetric combination above / p_kept.
  */
+/*
+ * jb_kinship_i8_corrections_tc: the same a, b and Q = R + T/2 updates as
+ * jb_kinship_i8_corrections (no reference counterpart: an evaluation of
+ * impute_and_center's missing-call terms, src/jamma/kinship/missing.py:22-61), with the
+ * dense part R = Z diag(mu) M^T on the INT8 tensor cores: mu_j as four base-254 digits
+ * (|error| <= 4.8e-10 per mu_j, mu_j in [0, 2]) interleaved along N of one GEMM per chunk
+ * whose A operand is the chunk's columns col0..col0+m of the sample-major Gram operand Zs
+ * (col0 and ldz multiples of 16); T/2 = M diag(mu^2/2) M^T from per-SNP missing-sample
+ * lists.  Faster than the sparse walk when calls are missing at more than a few per mille.
+ * max_missing: capacity for the chunk's missing calls (the sum over its SNPs of n - n_obs,
+ * known from pass-1 counts); workspace: jb_kinship_i8_tc_workspace_size(n, m,
+ * max_missing) bytes, first int32 a status word read with jb_gram_status (non-zero after a
+ * pipeline timeout or an exceeded capacity).
+ */
+int64_t jb_kinship_i8_tc_workspace_size(int64_t n, int64_t m, int64_t max_missing);
+int32_t jb_kinship_i8_corrections_tc(const int8_t* codes, int64_t ld_codes, const int8_t* Zs,
+                                     int64_t ldz, int64_t col0, const int8_t* Cs, int64_t ldcs,
+                                     int64_t n, int64_t m, const double* mu, double* a, double* b,
+                                     double* RT, int64_t ldr, int64_t max_missing,
+                                     void* workspace, int64_t workspace_bytes, uintptr_t stream);
+
 int64_t jb_gram_i8_workspace_size(int64_t n);
 int32_t jb_gram_i8(const int8_t* Zs, int64_t n, int64_t p, int64_t ldz, int32_t* C,
                    int64_t ldc, void* workspace, int64_t workspace_bytes, uintptr_t stream);

@@ -15,6 +15,7 @@
 // on the CUDA cores.
 #include "jb_common.cuh"
 #include "jb_gemm_i8.cuh"
+#include "jb_rotate_i8.cuh"
 
 #include <mutex>
 #include <vector>
@@ -286,6 +287,188 @@ __global__ void __launch_bounds__(256) kin_sparse_kernel(const uint8_t* __restri
     }
 }
 
+// ---------------------------------------------------------------- tensor-core correction
+// The same sparse terms on INT8 tensor cores, for chunks with many missing calls.
+//   R = Z diag(mu) M^T   (Z: calls, missing -> 0; M: missing masks; n x m each)
+// With mu_j = (2/127) sum_{t<4} 254^-t d_t(mu_j) (four base-254 digits of mu_j * 127/2,
+// error <= 4.8e-10 per mu_j), R = (2/127) sum_t 254^-t Z B_t^T, B_t = M diag(d_t), whose
+// int32 products are exact.  The digit planes are interleaved along N -- row 4k + t of B
+// is B_t's row k -- so one GEMM per chunk (M = n samples i, N = 4n, K = m SNPs) leaves
+// every (i, k) with its four planes in one tile, and the epilogue adds
+// (2/127) (((C3 w3 + C2 w2) + C1 w1) + C0) to Q[i, k].  The missing x missing term
+// T/2 = M diag(mu^2/2) M^T stays sparse (kin_mm_kernel).
+constexpr double kMuScale = 2.0 / 127.0;
+__device__ __constant__ double kPlaneW[4] = {1.0, 1.0 / 254.0, 1.0 / (254.0 * 254.0),
+                                             1.0 / (254.0 * 254.0 * 254.0)};
+
+__device__ __forceinline__ void mu_digits(double mu, int8_t (&d)[4]) {
+    double a = mu * (127.0 / 2.0);  // [0, 127]
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        const double r = rint(a);
+        d[t] = (int8_t)r;
+        a = (a - r) * 254.0;  // remainder within +-0.5 -> next digit within +-127
+    }
+}
+
+// B (4n x ldb, K-major): B[(4k + t) * ldb + j] = d_t(mu_j) if sample k is missing at SNP j.
+__global__ void kin_rmask_kernel(const int8_t* __restrict__ Cs, int64_t ldcs, int64_t m,
+                                 const double* __restrict__ mu, int8_t* __restrict__ B,
+                                 int64_t ldb) {
+    const int64_t k = blockIdx.y;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < ldb;
+         j += (int64_t)gridDim.x * blockDim.x) {
+        int8_t d[4] = {0, 0, 0, 0};
+        if (j < m && Cs[k * ldcs + j] == 3) mu_digits(mu[j], d);
+#pragma unroll
+        for (int t = 0; t < 4; ++t) B[(4 * k + t) * ldb + j] = d[t];
+    }
+}
+
+struct KinREpi {
+    static constexpr int kSmem = 0;
+    double* Q;
+    int64_t ldq;
+    int n;
+    __device__ __forceinline__ void run(int mb, int nb, uint32_t taddr, int q, int lane,
+                                        uint8_t*) const {
+        const int i = mb * kBM + 32 * q + lane;
+#pragma unroll 1
+        for (int c0 = 0; c0 < 256; c0 += 32) {
+            uint32_t v[32];
+            tmem_ld32(taddr + (uint32_t)c0, v);
+            if (i < n) {
+#pragma unroll
+                for (int kk = 0; kk < 8; ++kk) {
+                    const int k = (nb * 256 + c0) / 4 + kk;
+                    if (k < n) {
+                        const double x =
+                            (((double)(int32_t)v[4 * kk + 3] * kPlaneW[3] +
+                              (double)(int32_t)v[4 * kk + 2] * kPlaneW[2]) +
+                             (double)(int32_t)v[4 * kk + 1] * kPlaneW[1]) +
+                            (double)(int32_t)v[4 * kk];
+                        Q[(int64_t)k * ldq + i] += x * kMuScale;
+                    }
+                }
+            }
+        }
+    }
+};
+
+// Per-SNP missing-sample lists (CSR, samples in increasing order): counts, one-block
+// exclusive scan, ordered ballot fill.
+__global__ void kin_snp_miss_count_kernel(const int8_t* __restrict__ codes, int64_t ldc, int64_t n,
+                                          int32_t* __restrict__ cnt) {
+    const int64_t j = blockIdx.x;
+    int c = 0;
+    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) c += codes[j * ldc + i] == 3;
+    __shared__ int red[32];
+    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
+        cnt[j] = t;
+    }
+}
+
+// offsets[0..m] = exclusive scan of cnt (one CTA of 1024 threads, contiguous segments).
+__global__ void kin_scan_kernel(const int32_t* __restrict__ cnt, int64_t m,
+                                int64_t* __restrict__ offsets) {
+    __shared__ int64_t part[1024];
+    const int t = threadIdx.x;
+    const int64_t per = (m + 1023) / 1024, s0 = t * per, s1 = s0 + per < m ? s0 + per : m;
+    int64_t sum = 0;
+    for (int64_t j = s0; j < s1; ++j) sum += cnt[j];
+    part[t] = sum;
+    __syncthreads();
+    if (t == 0) {
+        int64_t acc = 0;
+        for (int w = 0; w < 1024; ++w) {
+            const int64_t v = part[w];
+            part[w] = acc;
+            acc += v;
+        }
+        offsets[m] = acc;
+    }
+    __syncthreads();
+    int64_t acc = part[t];
+    for (int64_t j = s0; j < s1; ++j) {
+        offsets[j] = acc;
+        acc += cnt[j];
+    }
+}
+
+__global__ void kin_snp_miss_fill_kernel(const int8_t* __restrict__ codes, int64_t ldc, int64_t n,
+                                         const int64_t* __restrict__ offsets,
+                                         int32_t* __restrict__ idx, int64_t cap,
+                                         int* __restrict__ err) {
+    const int64_t j = blockIdx.x;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __shared__ int wcnt[8];
+    int64_t pos = offsets[j];
+    for (int64_t r0 = 0; r0 < n; r0 += 256) {
+        const int64_t i = r0 + threadIdx.x;
+        const bool miss = i < n && codes[j * ldc + i] == 3;
+        const unsigned bal = __ballot_sync(0xffffffffu, miss);
+        if (lane == 0) wcnt[warp] = __popc(bal);
+        __syncthreads();
+        int64_t off = pos, tot = 0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) {
+            off += w < warp ? wcnt[w] : 0;
+            tot += wcnt[w];
+        }
+        if (miss) {
+            const int64_t e = off + __popc(bal & ((1u << lane) - 1u));
+            if (e < cap)
+                idx[e] = (int32_t)i;
+            else
+                atomicCAS(err, 0, 300);  // list capacity exceeded: entry skipped
+        }
+        pos += tot;
+        __syncthreads();
+    }
+}
+
+// T/2 term: Q[i, k] += sum_{j missing at k and at i} mu_j^2 / 2.  One CTA per (k, segment
+// of kMmSeg samples) accumulates in shared memory, one SNP at a time (a SNP's list holds
+// distinct samples; a barrier separates SNPs), so every entry sums in SNP order.
+constexpr int kMmSeg = 4096;
+__global__ void __launch_bounds__(256) kin_mm_kernel(const uint32_t* __restrict__ mask,
+                                                     int64_t words,
+                                                     const int64_t* __restrict__ offsets,
+                                                     const int32_t* __restrict__ idx,
+                                                     int64_t cap, const double* __restrict__ mu,
+                                                     int64_t n, double* __restrict__ Q,
+                                                     int64_t ldq) {
+    __shared__ double acc[kMmSeg];
+    const int64_t k = blockIdx.x;
+    const int64_t s0 = (int64_t)blockIdx.y * kMmSeg;
+    for (int e = threadIdx.x; e < kMmSeg; e += blockDim.x) acc[e] = 0.0;
+    __syncthreads();
+    const uint32_t* __restrict__ mk = mask + k * words;
+    for (int64_t w = 0; w < words; ++w) {
+        uint32_t word = __ldg(mk + w);  // uniform across the CTA
+        while (word) {
+            const int64_t j = w * 32 + __ffs(word) - 1;
+            word &= word - 1;
+            const double h = 0.5 * mu[j] * mu[j];
+            const int64_t e1 = offsets[j + 1] < cap ? offsets[j + 1] : cap;  // filled entries only
+            for (int64_t e = offsets[j] + threadIdx.x; e < e1; e += blockDim.x) {
+                const int64_t i = idx[e] - s0;
+                if (i >= 0 && i < kMmSeg) acc[i] += h;
+            }
+            __syncthreads();
+        }
+    }
+    for (int e = threadIdx.x; e < kMmSeg; e += blockDim.x) {
+        const int64_t i = s0 + e;
+        if (i < n && acc[e] != 0.0) Q[k * ldq + i] += acc[e];
+    }
+}
+
 // K = (C - a_i - a_j + s - b_i - b_j + Q_ij + Q_ji) / p, symmetric, column-major.
 __global__ void kin_finalize_i8_kernel(const int32_t* __restrict__ C, int64_t ldc, int64_t n,
                                        const double* __restrict__ a, const double* __restrict__ b,
@@ -536,6 +719,112 @@ int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes, const u
         kin_sparse_kernel<<<grid, 256, 0, st>>>(packed, bytes_per_snp, mask, words, n, mu, RT, ldr);
         JB_LAUNCH_CHECK("kin_sparse_kernel");
     }
+    return JB_OK;
+}
+
+// Workspace of jb_kinship_i8_corrections_tc.
+struct KinTcWs {
+    int64_t status, pa, mask, tiles, B, ldb, cnt, offsets, idx, total;
+};
+static KinTcWs kin_tc_ws(int64_t n, int64_t m, int64_t max_missing) {
+    KinTcWs w;
+    const int64_t mm = m > 0 ? m : 1;
+    const int64_t nblk = ceil_div(mm, 256), words = ceil_div(mm, 32);
+    const int64_t MB = ceil_div(n, kBM), NB = ceil_div(4 * n, 256);
+    auto a256 = [](int64_t x) { return (x + 255) / 256 * 256; };
+    int64_t off = 0;
+    w.status = off;
+    off += 256;
+    w.pa = off;
+    off += a256(2 * nblk * n * 8);
+    w.mask = off;
+    off += a256(n * words * 4);
+    w.tiles = off;
+    off += a256(MB * NB * (int64_t)sizeof(Tile));
+    w.ldb = (mm + 127) / 128 * 128;
+    w.B = off;
+    off += a256(4 * n * w.ldb);
+    w.cnt = off;
+    off += a256(mm * 4);
+    w.offsets = off;
+    off += a256((mm + 1) * 8);
+    w.idx = off;
+    off += a256((max_missing > 0 ? max_missing : 1) * 4);
+    w.total = off;
+    return w;
+}
+
+int64_t jb_kinship_i8_tc_workspace_size(int64_t n, int64_t m, int64_t max_missing) {
+    if (n <= 0 || m < 0 || max_missing < 0) return -1;
+    return kin_tc_ws(n, m, max_missing).total;
+}
+
+int32_t jb_kinship_i8_corrections_tc(const int8_t* codes, int64_t ld_codes, const int8_t* Zs,
+                                     int64_t ldz, int64_t col0, const int8_t* Cs, int64_t ldcs,
+                                     int64_t n, int64_t m, const double* mu, double* a, double* b,
+                                     double* RT, int64_t ldr, int64_t max_missing,
+                                     void* workspace, int64_t workspace_bytes, uintptr_t stream) {
+    JB_CHECK_ARG(n > 0 && m >= 0 && ld_codes >= n && ldr >= n && ldcs >= m,
+                 "jb_kinship_i8_corrections_tc: bad shape");
+    if (m == 0) return JB_OK;
+    JB_CHECK_ARG(codes && Zs && Cs && mu && a && b && RT, "jb_kinship_i8_corrections_tc: null pointer");
+    JB_CHECK_ARG(m < 65536 && 4 * n < (1ll << 31), "jb_kinship_i8_corrections_tc: chunk too large");
+    JB_CHECK_ARG(col0 % 16 == 0 && ldz % 16 == 0 && ldz >= col0 + m,
+                 "jb_kinship_i8_corrections_tc: Zs column block must start on 16 bytes");
+    const KinTcWs L = kin_tc_ws(n, m, max_missing);
+    JB_CHECK_ARG(workspace && workspace_bytes >= L.total, "jb_kinship_i8_corrections_tc: workspace too small");
+    cudaStream_t st = as_stream(stream);
+    uint8_t* ws = static_cast<uint8_t*>(workspace);
+    int* status = reinterpret_cast<int*>(ws + L.status);
+    JB_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
+    // a, b: ordered two-stage sums (as jb_kinship_i8_corrections)
+    const int64_t nblk = ceil_div(m, 256);
+    double* pa = reinterpret_cast<double*>(ws + L.pa);
+    double* pb = pa + nblk * n;
+    kin_vectors_partial_kernel<<<dim3((unsigned)ceil_div(n, 256), (unsigned)nblk), 256, 0, st>>>(
+        codes, ld_codes, n, m, mu, pa, pb);
+    JB_LAUNCH_CHECK("kin_vectors_partial_kernel");
+    kin_vectors_reduce_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, st>>>(n, nblk, pa, pb, a, b);
+    JB_LAUNCH_CHECK("kin_vectors_reduce_kernel");
+    // R on the tensor cores
+    int8_t* B = reinterpret_cast<int8_t*>(ws + L.B);
+    kin_rmask_kernel<<<dim3((unsigned)ceil_div(L.ldb, 256), (unsigned)n), 256, 0, st>>>(
+        Cs, ldcs, m, mu, B, L.ldb);
+    JB_LAUNCH_CHECK("kin_rmask_kernel");
+    const int MB = (int)ceil_div(n, kBM), NB = (int)ceil_div(4 * n, 256);
+    Tile* tiles = reinterpret_cast<Tile*>(ws + L.tiles);
+    int32_t rc = launch_group_tiles(MB, NB, 8, 16, tiles, st);
+    if (rc) return rc;
+    CUtensorMap ta, tb;
+    rc = make_map_i8(&ta, Zs + col0, n, m, ldz, kBM);
+    if (rc) return rc;
+    rc = make_map_i8(&tb, B, 4 * n, m, L.ldb, 256);
+    if (rc) return rc;
+    auto kern = i8_gemm_kernel<kGramBN, kGramStages, KinREpi>;
+    JB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, GramSmem::TOTAL));
+    const int n_tiles = MB * NB;
+    KinREpi epi{RT, ldr, (int)n};
+    kern<<<n_tiles < num_sms() ? n_tiles : num_sms(), kThreads, GramSmem::TOTAL, st>>>(
+        ta, tb, tiles, n_tiles, (int)ceil_div(m, kBK), epi, status);
+    JB_LAUNCH_CHECK("i8_gemm_kernel<kinship R>");
+    // T/2 from per-SNP missing lists and per-sample masks
+    const int64_t words = ceil_div(m, 32);
+    uint32_t* mask = reinterpret_cast<uint32_t*>(ws + L.mask);
+    kin_missing_mask_kernel<<<(unsigned)n, 256, 0, st>>>(Cs, ldcs, m, mask, words);
+    JB_LAUNCH_CHECK("kin_missing_mask_kernel");
+    int32_t* cnt = reinterpret_cast<int32_t*>(ws + L.cnt);
+    int64_t* offsets = reinterpret_cast<int64_t*>(ws + L.offsets);
+    int32_t* idx = reinterpret_cast<int32_t*>(ws + L.idx);
+    kin_snp_miss_count_kernel<<<(unsigned)m, 256, 0, st>>>(codes, ld_codes, n, cnt);
+    JB_LAUNCH_CHECK("kin_snp_miss_count_kernel");
+    kin_scan_kernel<<<1, 1024, 0, st>>>(cnt, m, offsets);
+    JB_LAUNCH_CHECK("kin_scan_kernel");
+    kin_snp_miss_fill_kernel<<<(unsigned)m, 256, 0, st>>>(codes, ld_codes, n, offsets, idx,
+                                                          max_missing, status);
+    JB_LAUNCH_CHECK("kin_snp_miss_fill_kernel");
+    kin_mm_kernel<<<dim3((unsigned)n, (unsigned)ceil_div(n, kMmSeg)), 256, 0, st>>>(
+        mask, words, offsets, idx, max_missing, mu, n, RT, ldr);
+    JB_LAUNCH_CHECK("kin_mm_kernel");
     return JB_OK;
 }
 

@@ -231,6 +231,13 @@ int32_t launch_rot_pair(const CUtensorMap& ta, const CUtensorMap& tb, const Tile
     return JB_OK;
 }
 
+int32_t launch_group_tiles(int MB, int NB, int GM, int GN, Tile* out, cudaStream_t st) {
+    const int64_t n_tiles = (int64_t)MB * NB;
+    rot_tiles_kernel<<<(unsigned)ceil_div(n_tiles, 256), 256, 0, st>>>(MB, NB, GM, GN, out);
+    JB_LAUNCH_CHECK("rot_tiles_kernel");
+    return JB_OK;
+}
+
 OzakiLayout ozaki_layout(int64_t n_out, int64_t n_k) {
     OzakiLayout L;
     L.lda = (n_k + 127) / 128 * 128;

@@ -22,6 +22,9 @@ struct RotChunkLayout {
 };
 RotChunkLayout rot_chunk_layout(int64_t n, int64_t m);
 
+// Full MB x NB tile grid in groups of GM x GN tiles (closed-form order, one thread per tile).
+int32_t launch_group_tiles(int MB, int NB, int GM, int GN, Tile* out, cudaStream_t st);
+
 // Split the n_out columns of V (column-major, length n_k, stride ldv) into ws.
 int32_t ozaki_split(const double* V, int64_t n_k, int64_t n_out, int64_t ldv, uint8_t* ws,
                     cudaStream_t st);

@@ -86,13 +86,22 @@ class _KinshipAccumulator:
         return self.K
 
 
+# Missing-call density (fraction of a chunk's calls) above which the correction terms run
+# on the INT8 tensor cores instead of the sparse walk over each sample's missing SNPs.
+TC_MISSING_DENSITY = 0.003
+
+
 class _KinshipI8:
     """Exact INT8 tensor-core Gram + FP64 centring / missing-call corrections.
+
+    MAX_CHUNK: SNPs per correction call (longer chunks are split).
 
     SNP chunks are transposed into the sample-major int8 operand (missing -> 0) and
     their correction vectors accumulated; ``finish`` runs the tcgen05 Gram once over all
     kept SNPs and combines the terms (see jb_gram.cu for the identity used).
     """
+
+    MAX_CHUNK = 16384
 
     def __init__(self, n: int, p_kept: int):
         self.n, self.p = n, p_kept
@@ -103,12 +112,26 @@ class _KinshipI8:
         self.RT = None
         self.sum_mu2 = 0.0
         self.col = 0
+        self._status: list[torch.Tensor] = []
+        self._density_scale = 1.0
 
     def add(self, codes: torch.Tensor, mu64: torch.Tensor, has_missing: bool,
-            packed: torch.Tensor | None = None) -> None:
+            packed: torch.Tensor | None = None, n_missing: int | None = None) -> None:
         """Add a chunk of decoded codes (m, ld); ``packed`` are the same SNPs' .bed records
-        (needed when ``has_missing``)."""
+        (used by the sparse missing-call correction).  ``n_missing``: the chunk's number of
+        missing calls (from pass-1 counts); with it, chunks whose missing calls exceed
+        TC_MISSING_DENSITY take the tensor-core correction."""
         m, ld = codes.shape
+        if m > self.MAX_CHUNK:  # the correction kernels take at most MAX_CHUNK SNPs per call
+            for s in range(0, m, self.MAX_CHUNK):
+                e = min(s + self.MAX_CHUNK, m)
+                # the whole chunk's count bounds every part's list capacity; the density
+                # test uses the chunk's average
+                self._density_scale = m / (e - s)
+                self.add(codes[s:e], mu64[s:e], has_missing, None if packed is None else packed[s:e],
+                         n_missing)
+            self._density_scale = 1.0
+            return
         st = stream_handle()
         Cs = None
         if has_missing:
@@ -117,6 +140,16 @@ class _KinshipI8:
             Cs = torch.empty((self.n, m), dtype=torch.int8, device="cuda")
         _native.call("jb_codes_to_sample_major", ptr(codes), ld, self.n, m, ptr(self.Zs), self.ldz,
                      self.col, ptr(Cs), m, st)
+        if (has_missing and n_missing is not None and self.col % 16 == 0
+                and n_missing > TC_MISSING_DENSITY * self.n * m * self._density_scale):
+            lib = _native.load()
+            ws = workspace(lib.jb_kinship_i8_tc_workspace_size(self.n, m, int(n_missing)))
+            _native.call("jb_kinship_i8_corrections_tc", ptr(codes), ld, ptr(self.Zs), self.ldz,
+                         self.col, ptr(Cs), m, self.n, m, ptr(mu64), ptr(self.a), ptr(self.b),
+                         ptr(self.RT), self.n, int(n_missing), ptr(ws), ws.numel(), st)
+            self._status.append(ws[:4].clone())  # status word, checked in finish()
+            self.col += m
+            return
         if has_missing and packed is None:
             packed = torch.empty((m, (self.n + 3) // 4), dtype=torch.uint8, device="cuda")
             _native.call("jb_pack_codes", ptr(codes), ld, self.n, m, ptr(packed), packed.shape[1], st)
@@ -146,6 +179,10 @@ class _KinshipI8:
 
     def finish(self) -> torch.Tensor:
         n = self.n
+        if self._status:
+            st = torch.cat(self._status).view(torch.int32).cpu().numpy()
+            if np.any(st != 0):
+                raise RuntimeError(f"tensor-core kinship correction reported status {st[st != 0][0]}")
         C = self.gram()
         K = torch.empty((n, n), dtype=torch.float64, device="cuda")
         _native.call("jb_kinship_i8_finalize", ptr(C), n, n, ptr(self.a), ptr(self.b), self.sum_mu2,
@@ -175,7 +212,7 @@ def _kinship_from_packed(packed_dev: torch.Tensor, n: int, batch_size: int, maf_
     if precision == "int8":
         acc = _KinshipI8(n, idx.size)
         acc.add(codes.index_select(0, sel), mu64, bool(np.any(c[:, 0] < n)),
-                packed_dev.index_select(0, sel))
+                packed_dev.index_select(0, sel), n_missing=int((n - c[:, 0]).sum()))
         acc.add_sum_mu2(c[:, 1] / np.maximum(c[:, 0], 1))
         return acc.finish(), idx.size
     acc = _KinshipAccumulator(n, max(1, min(batch_size, 8192)))
@@ -269,7 +306,8 @@ def compute_kinship_from_bed(bfile, maf_threshold: float = 0.0, miss_threshold: 
         c = counts[sub]
         mu64 = torch.from_numpy(c[:, 1] / np.maximum(c[:, 0], 1)).to("cuda")
         if i8:
-            acc.add(codes, mu64, bool(np.any(c[:, 0] < n)), None if sidx is not None else rec)
+            acc.add(codes, mu64, bool(np.any(c[:, 0] < n)), None if sidx is not None else rec,
+                    n_missing=int((n - c[:, 0]).sum()))
             acc.add_sum_mu2(c[:, 1] / np.maximum(c[:, 0], 1))
         elif kinship_mode == 2:
             acc.add(codes, mu64, torch.from_numpy(snp_sd_from_counts(c, n)).to("cuda"))

@@ -209,3 +209,23 @@ def test_rotate_pair_kernel_equals_single_cta_kernel(n, m, miss):
     finally:
         _native.call("jb_rotate_set_kernel", prev)
     np.testing.assert_array_equal(out[1], out[0])
+
+
+@pytest.mark.parametrize("miss", [0.01, 0.05])
+def test_tensor_core_and_sparse_missing_corrections_agree(miss, monkeypatch):
+    """The missing-call correction on INT8 tensor cores (digit planes of mu) and the sparse
+    walk give the same kinship, both within 1e-10 of the oracle."""
+    from jamma_b200 import kinship as KM
+
+    n, p = 700, 1024
+    g = synth.genotypes(n, p, miss, seed=int(miss * 1000))
+    ref = OK.centered_kinship(g)
+    out = {}
+    for name, thr in (("tc", 0.0), ("sparse", 2.0)):
+        monkeypatch.setattr(KM, "TC_MISSING_DENSITY", thr)
+        out[name] = KM.compute_centered_kinship(g, batch_size=256, precision="int8")
+        assert np.abs(out[name] - ref).max() <= 1e-10 * np.abs(ref).max(), name
+    # four base-254 digits carry mu_j to 4.8e-10; summed over a sample's missing SNPs and
+    # divided by p that stays near 1e-11 of the kinship's scale
+    assert np.abs(out["tc"] - out["sparse"]).max() <= 5e-11 * np.abs(ref).max()
+    np.testing.assert_array_equal(out["tc"], out["tc"].T)
