@@ -314,8 +314,7 @@ def run_ours(args) -> None:
             cc = kin_counts[sub]
             mu = torch.from_numpy(cc[:, 1] / np.maximum(cc[:, 0], 1)).cuda()
             if form == "int8":
-                acc.add(codes_k, mu, bool(np.any(cc[:, 0] < n)), rec_k,
-                        n_missing=int((n - cc[:, 0]).sum()))
+                acc.add(codes_k, mu, bool(np.any(cc[:, 0] < n)), n_missing=int((n - cc[:, 0]).sum()))
                 acc.add_sum_mu2(cc[:, 1] / np.maximum(cc[:, 0], 1))
             else:
                 acc.add(codes_k, mu)

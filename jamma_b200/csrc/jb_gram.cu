@@ -184,18 +184,137 @@ __global__ void kin_vectors_reduce_kernel(int64_t n, int64_t nblk, const double*
     b[i] += sb;
 }
 
-// Sparse terms for one SNP chunk.  For every sample k and every SNP j of the chunk that
-// is missing at k: Q[:, k] += mu_j Z[:, j] + (mu_j^2 / 2) M[:, j]  (Q = R + T/2), i.e. per
-// sample i one add of v_j(code_ij) with v_j = {00: 2 mu_j, 01 (missing): mu_j^2 / 2,
-// 10: mu_j, 11: 0} (count-A1 codes).  SNP columns are read from the 2-bit packed .bed
-// records (4x less traffic than int8 codes).
+// Missing-call terms for one SNP chunk (at most kSpMaxChunk SNPs):
+//   Q[i, k] += R_ik + T_ik / 2,   R_ik = sum_{j in miss(k)} mu_j z_ij,
+//                                 T_ik = sum_{j in miss(k) and miss(i)} mu_j^2
+// (z_ij the 0/1/2 call, 0 where missing).  R is n x nnz(M) multiply-adds: with 1 % of calls
+// missing that is 1 % of a dense Z diag(mu) M^T, so it runs on the FP64 pipe from
+// registers rather than densely on the tensor cores.  T has n nnz(M) p terms (p the
+// missing fraction) and comes from per-SNP lists of missing samples.
 //
-// Pass 1 (kin_missing_mask_kernel): each sample's missing SNPs of the chunk as a bitmask
-// (one ballot per 32 SNPs of the sample-major codes), so pass 2 needs no per-block
-// compaction.  Pass 2 (kin_sparse_kernel): one CTA per (k, block of 4096 samples i); the
-// CTA walks k's set bits in increasing SNP order (every thread the same j, so the FP64
-// summation order is fixed) four at a time, each thread owning 16 consecutive samples (one
-// 32-bit packed load per SNP, four in flight).
+// kin_sp_count_kernel / kin_sp_fill_kernel (one warp per SNP): the chunk's calls as
+// "dosage words" (16 samples per uint32, 2 bits each: the call, 0 where missing) and, per
+// (SNP j, block b of kSpBlock samples), the block-local indices of j's missing samples
+// (CSR, rows j * nb + b, offsets from kin_scan_kernel).
+//
+// kin_sp_kernel: one CTA per (sample k, block b of 4096 samples i).  The CTA turns k's
+// missing-SNP bitmask into an increasing list in shared memory, adds T/2 for its block
+// from the per-SNP lists (exact: mu_j^2/2 in 2^-44 fixed point, int64 shared atomics, so
+// the order of the adds does not matter), then walks the list once for R with every
+// thread owning 16 consecutive samples in registers (one dosage word per SNP).
+constexpr int kSpThreads = 256;
+constexpr int kSpSpt = 16;                      // samples per thread = one dosage word
+constexpr int kSpBlock = kSpThreads * kSpSpt;  // samples per CTA
+constexpr int kSpWords = kSpBlock / 16;        // dosage words per CTA
+constexpr int kSpMaxChunk = 16384;             // SNPs per call (list in shared memory)
+constexpr double kSpTScale = 17592186044416.0; // 2^44
+constexpr double kSpTInv = 1.0 / 17592186044416.0;
+
+struct SpSmem {
+    unsigned long long acc[kSpBlock];  // T/2 of the block, fixed point
+    uint16_t jl[kSpMaxChunk];          // k's missing SNPs, increasing
+    int warp_sum[kSpThreads / 32];
+};
+
+// 16 samples s0..s0+15 of one SNP row of int8 codes (0/1/2 calls, 3 missing; samples at
+// or beyond n read as call 0): z = the calls, 2 bits each (missing -> 0); miss = bit 2q
+// set where sample s0 + q is missing.
+__device__ __forceinline__ void sp_load16(const int8_t* __restrict__ row, int64_t s0, int64_t n,
+                                          bool vec, uint32_t& z, uint32_t& miss) {
+    uint32_t x[4] = {0u, 0u, 0u, 0u};
+    if (vec && s0 + 16 <= n) {
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(row + s0));
+        x[0] = v.x;
+        x[1] = v.y;
+        x[2] = v.z;
+        x[3] = v.w;
+    } else {
+        for (int q = 0; q < 16; ++q)
+            if (s0 + q < n) x[q >> 2] |= (uint32_t)(uint8_t)row[s0 + q] << (8 * (q & 3));
+    }
+    z = 0u;
+    miss = 0u;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        const uint32_t m3 = __vcmpeq4(x[e], 0x03030303u);  // 0xff in each missing byte
+        const uint32_t c = x[e] & ~m3 & 0x03030303u;
+        const uint32_t pz = (c & 0x3u) | ((c >> 6) & 0xCu) | ((c >> 12) & 0x30u) | ((c >> 18) & 0xC0u);
+        const uint32_t pm = (m3 & 0x1u) | ((m3 >> 6) & 0x4u) | ((m3 >> 12) & 0x10u) | ((m3 >> 18) & 0x40u);
+        z |= pz << (8 * e);
+        miss |= pm << (8 * e);
+    }
+}
+
+__device__ __forceinline__ int warp_sum_i(int v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+__global__ void __launch_bounds__(256) kin_sp_count_kernel(const int8_t* __restrict__ codes,
+                                                           int64_t ldc, int64_t n, int64_t m,
+                                                           int64_t wpr, int nb, int vec,
+                                                           uint32_t* __restrict__ zb,
+                                                           int32_t* __restrict__ cnt) {
+    const int64_t j = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (j >= m) return;  // warp-uniform
+    const int8_t* row = codes + j * ldc;
+    for (int bb = 0; bb < nb; ++bb) {
+        int c = 0;
+        const int64_t w1 = (int64_t)(bb + 1) * kSpWords < wpr ? (int64_t)(bb + 1) * kSpWords : wpr;
+        for (int64_t wi = (int64_t)bb * kSpWords + lane; wi < w1; wi += 32) {
+            uint32_t z, miss;
+            sp_load16(row, wi * 16, n, vec != 0, z, miss);
+            if (zb) zb[j * wpr + wi] = z;
+            c += __popc(miss);
+        }
+        c = warp_sum_i(c);
+        if (lane == 0) cnt[j * nb + bb] = c;
+    }
+}
+
+__global__ void __launch_bounds__(256) kin_sp_fill_kernel(const int8_t* __restrict__ codes,
+                                                          int64_t ldc, int64_t n, int64_t m,
+                                                          int64_t wpr, int nb, int vec,
+                                                          const int64_t* __restrict__ off,
+                                                          uint16_t* __restrict__ idx, int64_t cap,
+                                                          int* __restrict__ err) {
+    const int64_t j = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (j >= m) return;  // warp-uniform
+    const int8_t* row = codes + j * ldc;
+    for (int bb = 0; bb < nb; ++bb) {
+        int64_t pos = off[j * nb + bb];
+#pragma unroll 1
+        for (int it = 0; it < kSpWords / 32; ++it) {
+            const int64_t wl = (int64_t)it * 32 + lane, wi = (int64_t)bb * kSpWords + wl;
+            uint32_t z = 0u, miss = 0u;
+            if (wi < wpr) sp_load16(row, wi * 16, n, vec != 0, z, miss);
+            const int c = __popc(miss);
+            int incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            int64_t e = pos + incl - c;
+            while (miss) {
+                const int bit = __ffs(miss) - 1;
+                miss &= miss - 1u;
+                if (e < cap)
+                    idx[e] = (uint16_t)(wl * 16 + (bit >> 1));
+                else
+                    atomicCAS(err, 0, 300);  // list capacity exceeded: entry skipped
+                ++e;
+            }
+            pos += __shfl_sync(0xffffffffu, incl, 31);
+        }
+    }
+}
+
+// Each sample's missing SNPs of the chunk as a bitmask (one ballot per 32 SNPs of the
+// sample-major codes).
 __global__ void kin_missing_mask_kernel(const int8_t* __restrict__ Cs, int64_t ldcs, int64_t m,
                                         uint32_t* __restrict__ mask, int64_t words) {
     const int64_t k = blockIdx.x;
@@ -208,82 +327,132 @@ __global__ void kin_missing_mask_kernel(const int8_t* __restrict__ Cs, int64_t l
     }
 }
 
-// One SNP j for a thread's kSparseSpt consecutive samples (2 bits each in `w`): call value
-// 0/1/2 as a double built from its high word alone (2.0 and 1.0 have zero low words), one
-// FMA with mu_j, and mu_j^2 / 2 added for a missing call.  mu * call is exact, so the sums
-// equal adding v_j(code) directly.
-constexpr int kSparseSpt = 16;  // samples per thread (one 32-bit packed load)
-
-__device__ __forceinline__ void kin_sparse_accum(uint32_t w, double u, double (&r)[kSparseSpt]) {
-    const double u2h = 0.5 * u * u;
+// One SNP for a thread's 16 samples.  A call z becomes the double 4 + z or 4 + z/4 from its
+// high word alone: the two bits land at bits 18-19 (value z) or 16-17 (value z/4) of the
+// high word 0x40100000 (4.0) with one shift per sample pair and one LOP3 per sample, and
+// one FMA with mu_j accumulates it.  The offset 4 sum_j mu_j is removed afterwards (4 mu
+// is exact, so a thread with only zero calls ends with exactly 4 x the plain sum).
+__device__ __forceinline__ void sp_word(uint32_t w, double u, double (&r)[kSpSpt]) {
 #pragma unroll
-    for (int q = 0; q < kSparseSpt; ++q) {
-        // count-A1 codes: 00 -> 2 copies, 01 -> missing, 10 -> 1 copy, 11 -> 0 copies
-        const uint32_t code = (w >> (2 * q)) & 3u;
-        const int hi = code == 0u ? 0x40000000 : (code == 2u ? 0x3FF00000 : 0);
-        r[q] = fma(u, __hiloint2double(hi, 0), r[q]);
-        if (code == 1u) r[q] += u2h;
+    for (int p = 0; p < 8; ++p) {
+        const uint32_t t = p <= 4 ? (w << (16 - 4 * p)) : (w >> (4 * p - 16));
+        const int lo_s = (int)((t & 0x00030000u) | 0x40100000u);  // sample 2p: 4 + z/4
+        const int hi_s = (int)((t & 0x000C0000u) | 0x40100000u);  // sample 2p+1: 4 + z
+        r[2 * p] = fma(u, __hiloint2double(lo_s, 0), r[2 * p]);
+        r[2 * p + 1] = fma(u, __hiloint2double(hi_s, 0), r[2 * p + 1]);
     }
 }
 
-__global__ void __launch_bounds__(256) kin_sparse_kernel(const uint8_t* __restrict__ packed,
-                                                          int64_t bps,
-                                                          const uint32_t* __restrict__ mask,
-                                                          int64_t words, int64_t n,
-                                                          const double* __restrict__ mu,
-                                                          double* __restrict__ Q, int64_t ldq) {
-    constexpr int kBytes = kSparseSpt / 4;  // packed bytes per thread
+template <bool kR>
+__global__ void __launch_bounds__(kSpThreads, 3) kin_sp_kernel(
+    const uint32_t* __restrict__ zb, int64_t wpr, const uint32_t* __restrict__ mask,
+    int64_t words, const int64_t* __restrict__ off, const uint16_t* __restrict__ idx,
+    int64_t cap, int nb, const double* __restrict__ mu, int64_t n, double* __restrict__ Q,
+    int64_t ldq) {
+    extern __shared__ __align__(16) unsigned char sp_smem_raw[];
+    SpSmem& S = *reinterpret_cast<SpSmem*>(sp_smem_raw);
     const int64_t k = blockIdx.x;
-    const int64_t i0 = (int64_t)blockIdx.y * (256 * kSparseSpt) + kSparseSpt * threadIdx.x;
+    const int b = blockIdx.y;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // k's missing SNPs in increasing order: thread t owns mask words 2t, 2t+1
     const uint32_t* __restrict__ mk = mask + k * words;
-    double r[kSparseSpt];
+    uint32_t m0 = 2 * tid < words ? __ldg(mk + 2 * tid) : 0u;
+    uint32_t m1 = 2 * tid + 1 < words ? __ldg(mk + 2 * tid + 1) : 0u;
+    const int c = __popc(m0) + __popc(m1);
+    int incl = c;
 #pragma unroll
-    for (int e = 0; e < kSparseSpt; ++e) r[e] = 0.0;
-    const int64_t b0 = i0 >> 2;  // first packed byte of this thread's samples
-    const bool full = (i0 + kSparseSpt <= n) && ((bps & 3) == 0);
-    auto load = [&](int64_t j) -> uint32_t {
-        const uint8_t* rec = packed + j * bps;
-        if (full) return *reinterpret_cast<const uint32_t*>(rec + b0);
-        uint32_t w = 0xffffffffu;  // padding decodes as 0 copies
-        for (int q = 0; q < kBytes; ++q)
-            if (b0 + q < bps) w = (w & ~(0xffu << (8 * q))) | ((uint32_t)rec[b0 + q] << (8 * q));
-        return w;
-    };
-    // next missing SNP of sample k in increasing order (uniform across the CTA), -1 at end
-    int64_t wi = -1;
-    uint32_t word = 0;
-    auto next = [&]() -> int64_t {
-        while (word == 0) {
-            if (++wi >= words) return -1;
-            word = __ldg(mk + wi);
-        }
-        const int b = __ffs(word) - 1;
-        word &= word - 1;
-        return wi * 32 + b;
-    };
-    if (i0 < n) {
-        int64_t j0 = next(), j1 = next(), j2 = next(), j3 = next();
-        while (j3 >= 0) {
-            const uint32_t w0 = load(j0), w1 = load(j1), w2 = load(j2), w3 = load(j3);
-            const double u0 = __ldg(mu + j0), u1 = __ldg(mu + j1), u2 = __ldg(mu + j2),
-                         u3 = __ldg(mu + j3);
-            kin_sparse_accum(w0, u0, r);
-            kin_sparse_accum(w1, u1, r);
-            kin_sparse_accum(w2, u2, r);
-            kin_sparse_accum(w3, u3, r);
-            j0 = next();
-            j1 = next();
-            j2 = next();
-            j3 = next();
-        }
-        if (j0 >= 0) kin_sparse_accum(load(j0), __ldg(mu + j0), r);
-        if (j1 >= 0) kin_sparse_accum(load(j1), __ldg(mu + j1), r);
-        if (j2 >= 0) kin_sparse_accum(load(j2), __ldg(mu + j2), r);
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
     }
+    if (lane == 31) S.warp_sum[warp] = incl;
+    for (int e = tid; e < kSpBlock; e += kSpThreads) S.acc[e] = 0ull;
+    __syncthreads();
+    int pos = incl - c, cnt = 0;
 #pragma unroll
-    for (int q = 0; q < kSparseSpt; ++q) {
+    for (int w = 0; w < kSpThreads / 32; ++w) {
+        pos += w < warp ? S.warp_sum[w] : 0;
+        cnt += S.warp_sum[w];
+    }
+    while (m0) {
+        S.jl[pos++] = (uint16_t)(64 * tid + __ffs(m0) - 1);
+        m0 &= m0 - 1u;
+    }
+    while (m1) {
+        S.jl[pos++] = (uint16_t)(64 * tid + 32 + __ffs(m1) - 1);
+        m1 &= m1 - 1u;
+    }
+    __syncthreads();
+    // T/2 for this block: every sample of the block missing at one of k's missing SNPs.
+    // Thread t takes list entries t, t + 256, ... (one SNP's list each, read four entries
+    // at a time so the loads overlap).
+    for (int p = tid; p < cnt; p += kSpThreads) {
+        const int64_t j = S.jl[p];
+        const int64_t e0 = off[j * nb + b];
+        int64_t e1 = off[j * nb + b + 1];
+        e1 = e1 < cap ? e1 : cap;  // filled entries only
+        const double u = __ldg(mu + j);
+        const unsigned long long h = (unsigned long long)__double2ll_rn(0.5 * u * u * kSpTScale);
+        for (int64_t e = e0; e < e1; e += 4) {
+            int v[4];
+#pragma unroll
+            for (int x = 0; x < 4; ++x) v[x] = e + x < e1 ? (int)__ldg(idx + e + x) : -1;
+#pragma unroll
+            for (int x = 0; x < 4; ++x)
+                if (v[x] >= 0) atomicAdd(&S.acc[v[x]], h);
+        }
+    }
+    double r[kSpSpt];
+#pragma unroll
+    for (int q = 0; q < kSpSpt; ++q) r[q] = 0.0;
+    double s = 0.0;
+    const int64_t wi = (int64_t)b * kSpWords + tid;
+    if (kR) {
+        const bool act = wi < wpr;
+        const uint32_t* __restrict__ zc = zb + (act ? wi : 0);
+        uint32_t wn[4];
+        double un[4];
+        auto fetch = [&](int p0) {
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                const int p = p0 + e;
+                if (p < cnt) {
+                    const int64_t j = S.jl[p];
+                    un[e] = __ldg(mu + j);
+                    wn[e] = act ? __ldg(zc + j * wpr) : 0u;
+                } else {
+                    un[e] = 0.0;
+                    wn[e] = 0u;
+                }
+            }
+        };
+        fetch(0);
+#pragma unroll 1
+        for (int p0 = 0; p0 < cnt; p0 += 4) {
+            uint32_t w[4];
+            double u[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                w[e] = wn[e];
+                u[e] = un[e];
+            }
+            fetch(p0 + 4);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) {
+                s += u[e];
+                sp_word(w[e], u[e], r);
+            }
+        }
+    }
+    __syncthreads();  // T/2 complete
+    const double s4 = 4.0 * s;
+    const int64_t i0 = (int64_t)b * kSpBlock + (int64_t)tid * kSpSpt;
+#pragma unroll
+    for (int q = 0; q < kSpSpt; ++q) {
         const int64_t i = i0 + q;
-        if (i < n) Q[k * ldq + i] += r[q];  // Q[i, k] (column-major, column k)
+        double v = (double)(long long)S.acc[tid * kSpSpt + q] * kSpTInv;
+        if (kR) v += (q & 1) ? (r[q] - s4) : 4.0 * (r[q] - s4);
+        if (i < n && v != 0.0) Q[k * ldq + i] += v;  // Q[i, k] (column-major, column k)
     }
 }
 
@@ -355,24 +524,6 @@ struct KinREpi {
     }
 };
 
-// Per-SNP missing-sample lists (CSR, samples in increasing order): counts, one-block
-// exclusive scan, ordered ballot fill.
-__global__ void kin_snp_miss_count_kernel(const int8_t* __restrict__ codes, int64_t ldc, int64_t n,
-                                          int32_t* __restrict__ cnt) {
-    const int64_t j = blockIdx.x;
-    int c = 0;
-    for (int64_t i = threadIdx.x; i < n; i += blockDim.x) c += codes[j * ldc + i] == 3;
-    __shared__ int red[32];
-    for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = c;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        int t = 0;
-        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += red[w];
-        cnt[j] = t;
-    }
-}
-
 // offsets[0..m] = exclusive scan of cnt (one CTA of 1024 threads, contiguous segments).
 __global__ void kin_scan_kernel(const int32_t* __restrict__ cnt, int64_t m,
                                 int64_t* __restrict__ offsets) {
@@ -397,75 +548,6 @@ __global__ void kin_scan_kernel(const int32_t* __restrict__ cnt, int64_t m,
     for (int64_t j = s0; j < s1; ++j) {
         offsets[j] = acc;
         acc += cnt[j];
-    }
-}
-
-__global__ void kin_snp_miss_fill_kernel(const int8_t* __restrict__ codes, int64_t ldc, int64_t n,
-                                         const int64_t* __restrict__ offsets,
-                                         int32_t* __restrict__ idx, int64_t cap,
-                                         int* __restrict__ err) {
-    const int64_t j = blockIdx.x;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    __shared__ int wcnt[8];
-    int64_t pos = offsets[j];
-    for (int64_t r0 = 0; r0 < n; r0 += 256) {
-        const int64_t i = r0 + threadIdx.x;
-        const bool miss = i < n && codes[j * ldc + i] == 3;
-        const unsigned bal = __ballot_sync(0xffffffffu, miss);
-        if (lane == 0) wcnt[warp] = __popc(bal);
-        __syncthreads();
-        int64_t off = pos, tot = 0;
-#pragma unroll
-        for (int w = 0; w < 8; ++w) {
-            off += w < warp ? wcnt[w] : 0;
-            tot += wcnt[w];
-        }
-        if (miss) {
-            const int64_t e = off + __popc(bal & ((1u << lane) - 1u));
-            if (e < cap)
-                idx[e] = (int32_t)i;
-            else
-                atomicCAS(err, 0, 300);  // list capacity exceeded: entry skipped
-        }
-        pos += tot;
-        __syncthreads();
-    }
-}
-
-// T/2 term: Q[i, k] += sum_{j missing at k and at i} mu_j^2 / 2.  One CTA per (k, segment
-// of kMmSeg samples) accumulates in shared memory, one SNP at a time (a SNP's list holds
-// distinct samples; a barrier separates SNPs), so every entry sums in SNP order.
-constexpr int kMmSeg = 4096;
-__global__ void __launch_bounds__(256) kin_mm_kernel(const uint32_t* __restrict__ mask,
-                                                     int64_t words,
-                                                     const int64_t* __restrict__ offsets,
-                                                     const int32_t* __restrict__ idx,
-                                                     int64_t cap, const double* __restrict__ mu,
-                                                     int64_t n, double* __restrict__ Q,
-                                                     int64_t ldq) {
-    __shared__ double acc[kMmSeg];
-    const int64_t k = blockIdx.x;
-    const int64_t s0 = (int64_t)blockIdx.y * kMmSeg;
-    for (int e = threadIdx.x; e < kMmSeg; e += blockDim.x) acc[e] = 0.0;
-    __syncthreads();
-    const uint32_t* __restrict__ mk = mask + k * words;
-    for (int64_t w = 0; w < words; ++w) {
-        uint32_t word = __ldg(mk + w);  // uniform across the CTA
-        while (word) {
-            const int64_t j = w * 32 + __ffs(word) - 1;
-            word &= word - 1;
-            const double h = 0.5 * mu[j] * mu[j];
-            const int64_t e1 = offsets[j + 1] < cap ? offsets[j + 1] : cap;  // filled entries only
-            for (int64_t e = offsets[j] + threadIdx.x; e < e1; e += blockDim.x) {
-                const int64_t i = idx[e] - s0;
-                if (i >= 0 && i < kMmSeg) acc[i] += h;
-            }
-            __syncthreads();
-        }
-    }
-    for (int e = threadIdx.x; e < kMmSeg; e += blockDim.x) {
-        const int64_t i = s0 + e;
-        if (i < n && acc[e] != 0.0) Q[k * ldq + i] += acc[e];
     }
 }
 
@@ -682,81 +764,117 @@ int32_t jb_codes_to_sample_major(const int8_t* codes, int64_t ld_codes, int64_t 
     return JB_OK;
 }
 
-int64_t jb_kinship_i8_partial_size(int64_t n, int64_t m) {
-    if (n <= 0 || m < 0) return -1;
-    const int64_t mm = m > 0 ? m : 1;
-    // FP64 partial sums of the a / b vectors, then the per-sample missing-SNP bitmasks
-    return 2 * ceil_div(mm, 256) * n * 8 + n * ceil_div(mm, 32) * 4;
-}
-
-int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes, const uint8_t* packed,
-                                  int64_t bytes_per_snp, const int8_t* Cs, int64_t ldcs, int64_t n,
-                                  int64_t m, const double* mu, double* a, double* b, double* RT,
-                                  int64_t ldr, void* partial, int64_t partial_bytes,
-                                  uintptr_t stream) {
-    JB_CHECK_ARG(n > 0 && m >= 0 && ld_codes >= n, "jb_kinship_i8_corrections: bad shape");
-    if (m == 0) return JB_OK;
-    cudaStream_t st = as_stream(stream);
-    JB_CHECK_ARG(ceil_div(m, 256) < 65536, "jb_kinship_i8_corrections: chunk too large");
-    JB_CHECK_ARG(partial && partial_bytes >= jb_kinship_i8_partial_size(n, m),
-                 "jb_kinship_i8_corrections: partial-sum buffer too small");
-    const int64_t nblk = ceil_div(m, 256);
-    double* pa = static_cast<double*>(partial);
-    double* pb = pa + nblk * n;
-    kin_vectors_partial_kernel<<<dim3((unsigned)ceil_div(n, 256), (unsigned)nblk), 256, 0, st>>>(
-        codes, ld_codes, n, m, mu, pa, pb);
-    JB_LAUNCH_CHECK("kin_vectors_partial_kernel");
-    kin_vectors_reduce_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, st>>>(n, nblk, pa, pb, a, b);
-    JB_LAUNCH_CHECK("kin_vectors_reduce_kernel");
-    if (Cs) {
-        JB_CHECK_ARG(RT && ldr >= n && ldcs >= m && packed && 4 * bytes_per_snp >= n,
-                     "jb_kinship_i8_corrections: Q buffer and packed records needed");
-        const int64_t words = ceil_div(m, 32);
-        uint32_t* mask = reinterpret_cast<uint32_t*>(pb + nblk * n);
-        kin_missing_mask_kernel<<<(unsigned)n, 256, 0, st>>>(Cs, ldcs, m, mask, words);
-        JB_LAUNCH_CHECK("kin_missing_mask_kernel");
-        dim3 grid((unsigned)n, (unsigned)ceil_div(n, 256 * kSparseSpt), 1);
-        kin_sparse_kernel<<<grid, 256, 0, st>>>(packed, bytes_per_snp, mask, words, n, mu, RT, ldr);
-        JB_LAUNCH_CHECK("kin_sparse_kernel");
-    }
-    return JB_OK;
-}
-
-// Workspace of jb_kinship_i8_corrections_tc.
-struct KinTcWs {
-    int64_t status, pa, mask, tiles, B, ldb, cnt, offsets, idx, total;
+// Workspace of the correction entry points (tc: with the tensor-core R operand).
+struct KinCorrWs {
+    int64_t status, pa, mask, zb, cnt, off, idx, tiles, B, ldb, total, wpr, words;
+    int nb;
 };
-static KinTcWs kin_tc_ws(int64_t n, int64_t m, int64_t max_missing) {
-    KinTcWs w;
+static KinCorrWs kin_corr_ws(int64_t n, int64_t m, int64_t max_missing, bool tc) {
+    KinCorrWs w;
     const int64_t mm = m > 0 ? m : 1;
-    const int64_t nblk = ceil_div(mm, 256), words = ceil_div(mm, 32);
-    const int64_t MB = ceil_div(n, kBM), NB = ceil_div(4 * n, 256);
+    const int64_t nblk = ceil_div(mm, 256);
     auto a256 = [](int64_t x) { return (x + 255) / 256 * 256; };
+    w.words = ceil_div(mm, 32);
+    w.wpr = ceil_div(n, 16);
+    w.nb = (int)ceil_div(n, kSpBlock);
     int64_t off = 0;
     w.status = off;
     off += 256;
     w.pa = off;
     off += a256(2 * nblk * n * 8);
     w.mask = off;
-    off += a256(n * words * 4);
-    w.tiles = off;
-    off += a256(MB * NB * (int64_t)sizeof(Tile));
-    w.ldb = (mm + 127) / 128 * 128;
-    w.B = off;
-    off += a256(4 * n * w.ldb);
+    off += a256(n * w.words * 4);
+    w.zb = off;
+    off += tc ? 0 : a256(mm * w.wpr * 4);
     w.cnt = off;
-    off += a256(mm * 4);
-    w.offsets = off;
-    off += a256((mm + 1) * 8);
+    off += a256(mm * w.nb * 4);
+    w.off = off;
+    off += a256((mm * w.nb + 1) * 8);
     w.idx = off;
-    off += a256((max_missing > 0 ? max_missing : 1) * 4);
+    off += a256((max_missing > 0 ? max_missing : 1) * 2);
+    w.ldb = (mm + 127) / 128 * 128;
+    w.tiles = off;
+    off += tc ? a256(ceil_div(n, kBM) * ceil_div(4 * n, 256) * (int64_t)sizeof(Tile)) : 0;
+    w.B = off;
+    off += tc ? a256(4 * n * w.ldb) : 0;
     w.total = off;
     return w;
 }
 
+// a, b: ordered two-stage sums over the chunk's SNPs.
+static int32_t kin_vectors(const int8_t* codes, int64_t ld_codes, int64_t n, int64_t m,
+                           const double* mu, double* a, double* b, double* pa, cudaStream_t st) {
+    const int64_t nblk = ceil_div(m, 256);
+    double* pb = pa + nblk * n;
+    kin_vectors_partial_kernel<<<dim3((unsigned)ceil_div(n, 256), (unsigned)nblk), 256, 0, st>>>(
+        codes, ld_codes, n, m, mu, pa, pb);
+    JB_LAUNCH_CHECK("kin_vectors_partial_kernel");
+    kin_vectors_reduce_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, st>>>(n, nblk, pa, pb, a, b);
+    JB_LAUNCH_CHECK("kin_vectors_reduce_kernel");
+    return JB_OK;
+}
+
+// Q += T/2 (with_r: + R) for one chunk: per-sample masks, per-SNP lists, kin_sp_kernel.
+static int32_t kin_missing_terms(const int8_t* codes, int64_t ld_codes, const int8_t* Cs,
+                                 int64_t ldcs, int64_t n, int64_t m, const double* mu, double* RT,
+                                 int64_t ldr, int64_t max_missing, const KinCorrWs& L,
+                                 uint8_t* ws, bool with_r, cudaStream_t st) {
+    int* status = reinterpret_cast<int*>(ws + L.status);
+    uint32_t* mask = reinterpret_cast<uint32_t*>(ws + L.mask);
+    uint32_t* zb = with_r ? reinterpret_cast<uint32_t*>(ws + L.zb) : nullptr;
+    int32_t* cnt = reinterpret_cast<int32_t*>(ws + L.cnt);
+    int64_t* off = reinterpret_cast<int64_t*>(ws + L.off);
+    uint16_t* idx = reinterpret_cast<uint16_t*>(ws + L.idx);
+    const int vec = ((reinterpret_cast<uintptr_t>(codes) & 15) == 0 && ld_codes % 16 == 0) ? 1 : 0;
+    kin_missing_mask_kernel<<<(unsigned)n, 256, 0, st>>>(Cs, ldcs, m, mask, L.words);
+    JB_LAUNCH_CHECK("kin_missing_mask_kernel");
+    const unsigned snp_blocks = (unsigned)ceil_div(m, 8);
+    kin_sp_count_kernel<<<snp_blocks, 256, 0, st>>>(codes, ld_codes, n, m, L.wpr, L.nb, vec, zb, cnt);
+    JB_LAUNCH_CHECK("kin_sp_count_kernel");
+    kin_scan_kernel<<<1, 1024, 0, st>>>(cnt, m * L.nb, off);
+    JB_LAUNCH_CHECK("kin_scan_kernel");
+    kin_sp_fill_kernel<<<snp_blocks, 256, 0, st>>>(codes, ld_codes, n, m, L.wpr, L.nb, vec, off, idx,
+                                                   max_missing, status);
+    JB_LAUNCH_CHECK("kin_sp_fill_kernel");
+    auto kern = with_r ? kin_sp_kernel<true> : kin_sp_kernel<false>;
+    JB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SpSmem)));
+    kern<<<dim3((unsigned)n, (unsigned)L.nb), kSpThreads, sizeof(SpSmem), st>>>(
+        zb, L.wpr, mask, L.words, off, idx, max_missing, L.nb, mu, n, RT, ldr);
+    JB_LAUNCH_CHECK("kin_sp_kernel");
+    return JB_OK;
+}
+
+int64_t jb_kinship_i8_corrections_workspace_size(int64_t n, int64_t m, int64_t max_missing) {
+    if (n <= 0 || m < 0 || max_missing < 0) return -1;
+    return kin_corr_ws(n, m, max_missing, false).total;
+}
+
+int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes, const int8_t* Cs,
+                                  int64_t ldcs, int64_t n, int64_t m, const double* mu, double* a,
+                                  double* b, double* RT, int64_t ldr, int64_t max_missing,
+                                  void* workspace, int64_t workspace_bytes, uintptr_t stream) {
+    JB_CHECK_ARG(n > 0 && m >= 0 && ld_codes >= n && max_missing >= 0,
+                 "jb_kinship_i8_corrections: bad shape");
+    if (m == 0) return JB_OK;
+    JB_CHECK_ARG(m <= kSpMaxChunk, "jb_kinship_i8_corrections: at most %d SNPs per call", kSpMaxChunk);
+    JB_CHECK_ARG(codes && mu && a && b, "jb_kinship_i8_corrections: null pointer");
+    JB_CHECK_ARG(n * ceil_div(n, kSpBlock) < (1ll << 31) && n < (1ll << 31),
+                 "jb_kinship_i8_corrections: n too large");
+    const KinCorrWs L = kin_corr_ws(n, m, max_missing, false);
+    JB_CHECK_ARG(workspace && workspace_bytes >= L.total,
+                 "jb_kinship_i8_corrections: workspace too small");
+    cudaStream_t st = as_stream(stream);
+    uint8_t* ws = static_cast<uint8_t*>(workspace);
+    JB_CUDA(cudaMemsetAsync(ws + L.status, 0, sizeof(int), st));
+    int32_t rc = kin_vectors(codes, ld_codes, n, m, mu, a, b, reinterpret_cast<double*>(ws + L.pa), st);
+    if (rc || !Cs) return rc;
+    JB_CHECK_ARG(RT && ldr >= n && ldcs >= m, "jb_kinship_i8_corrections: Q buffer needed");
+    return kin_missing_terms(codes, ld_codes, Cs, ldcs, n, m, mu, RT, ldr, max_missing, L, ws, true, st);
+}
+
 int64_t jb_kinship_i8_tc_workspace_size(int64_t n, int64_t m, int64_t max_missing) {
     if (n <= 0 || m < 0 || max_missing < 0) return -1;
-    return kin_tc_ws(n, m, max_missing).total;
+    return kin_corr_ws(n, m, max_missing, true).total;
 }
 
 int32_t jb_kinship_i8_corrections_tc(const int8_t* codes, int64_t ld_codes, const int8_t* Zs,
@@ -764,28 +882,21 @@ int32_t jb_kinship_i8_corrections_tc(const int8_t* codes, int64_t ld_codes, cons
                                      int64_t n, int64_t m, const double* mu, double* a, double* b,
                                      double* RT, int64_t ldr, int64_t max_missing,
                                      void* workspace, int64_t workspace_bytes, uintptr_t stream) {
-    JB_CHECK_ARG(n > 0 && m >= 0 && ld_codes >= n && ldr >= n && ldcs >= m,
+    JB_CHECK_ARG(n > 0 && m >= 0 && ld_codes >= n && ldr >= n && ldcs >= m && max_missing >= 0,
                  "jb_kinship_i8_corrections_tc: bad shape");
     if (m == 0) return JB_OK;
     JB_CHECK_ARG(codes && Zs && Cs && mu && a && b && RT, "jb_kinship_i8_corrections_tc: null pointer");
-    JB_CHECK_ARG(m < 65536 && 4 * n < (1ll << 31), "jb_kinship_i8_corrections_tc: chunk too large");
+    JB_CHECK_ARG(m <= kSpMaxChunk && 4 * n < (1ll << 31), "jb_kinship_i8_corrections_tc: chunk too large");
     JB_CHECK_ARG(col0 % 16 == 0 && ldz % 16 == 0 && ldz >= col0 + m,
                  "jb_kinship_i8_corrections_tc: Zs column block must start on 16 bytes");
-    const KinTcWs L = kin_tc_ws(n, m, max_missing);
+    const KinCorrWs L = kin_corr_ws(n, m, max_missing, true);
     JB_CHECK_ARG(workspace && workspace_bytes >= L.total, "jb_kinship_i8_corrections_tc: workspace too small");
     cudaStream_t st = as_stream(stream);
     uint8_t* ws = static_cast<uint8_t*>(workspace);
     int* status = reinterpret_cast<int*>(ws + L.status);
     JB_CUDA(cudaMemsetAsync(status, 0, sizeof(int), st));
-    // a, b: ordered two-stage sums (as jb_kinship_i8_corrections)
-    const int64_t nblk = ceil_div(m, 256);
-    double* pa = reinterpret_cast<double*>(ws + L.pa);
-    double* pb = pa + nblk * n;
-    kin_vectors_partial_kernel<<<dim3((unsigned)ceil_div(n, 256), (unsigned)nblk), 256, 0, st>>>(
-        codes, ld_codes, n, m, mu, pa, pb);
-    JB_LAUNCH_CHECK("kin_vectors_partial_kernel");
-    kin_vectors_reduce_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, st>>>(n, nblk, pa, pb, a, b);
-    JB_LAUNCH_CHECK("kin_vectors_reduce_kernel");
+    int32_t rc = kin_vectors(codes, ld_codes, n, m, mu, a, b, reinterpret_cast<double*>(ws + L.pa), st);
+    if (rc) return rc;
     // R on the tensor cores
     int8_t* B = reinterpret_cast<int8_t*>(ws + L.B);
     kin_rmask_kernel<<<dim3((unsigned)ceil_div(L.ldb, 256), (unsigned)n), 256, 0, st>>>(
@@ -793,7 +904,7 @@ int32_t jb_kinship_i8_corrections_tc(const int8_t* codes, int64_t ld_codes, cons
     JB_LAUNCH_CHECK("kin_rmask_kernel");
     const int MB = (int)ceil_div(n, kBM), NB = (int)ceil_div(4 * n, 256);
     Tile* tiles = reinterpret_cast<Tile*>(ws + L.tiles);
-    int32_t rc = launch_group_tiles(MB, NB, 8, 16, tiles, st);
+    rc = launch_group_tiles(MB, NB, 8, 16, tiles, st);
     if (rc) return rc;
     CUtensorMap ta, tb;
     rc = make_map_i8(&ta, Zs + col0, n, m, ldz, kBM);
@@ -807,25 +918,8 @@ int32_t jb_kinship_i8_corrections_tc(const int8_t* codes, int64_t ld_codes, cons
     kern<<<n_tiles < num_sms() ? n_tiles : num_sms(), kThreads, GramSmem::TOTAL, st>>>(
         ta, tb, tiles, n_tiles, (int)ceil_div(m, kBK), epi, status);
     JB_LAUNCH_CHECK("i8_gemm_kernel<kinship R>");
-    // T/2 from per-SNP missing lists and per-sample masks
-    const int64_t words = ceil_div(m, 32);
-    uint32_t* mask = reinterpret_cast<uint32_t*>(ws + L.mask);
-    kin_missing_mask_kernel<<<(unsigned)n, 256, 0, st>>>(Cs, ldcs, m, mask, words);
-    JB_LAUNCH_CHECK("kin_missing_mask_kernel");
-    int32_t* cnt = reinterpret_cast<int32_t*>(ws + L.cnt);
-    int64_t* offsets = reinterpret_cast<int64_t*>(ws + L.offsets);
-    int32_t* idx = reinterpret_cast<int32_t*>(ws + L.idx);
-    kin_snp_miss_count_kernel<<<(unsigned)m, 256, 0, st>>>(codes, ld_codes, n, cnt);
-    JB_LAUNCH_CHECK("kin_snp_miss_count_kernel");
-    kin_scan_kernel<<<1, 1024, 0, st>>>(cnt, m, offsets);
-    JB_LAUNCH_CHECK("kin_scan_kernel");
-    kin_snp_miss_fill_kernel<<<(unsigned)m, 256, 0, st>>>(codes, ld_codes, n, offsets, idx,
-                                                          max_missing, status);
-    JB_LAUNCH_CHECK("kin_snp_miss_fill_kernel");
-    kin_mm_kernel<<<dim3((unsigned)n, (unsigned)ceil_div(n, kMmSeg)), 256, 0, st>>>(
-        mask, words, offsets, idx, max_missing, mu, n, RT, ldr);
-    JB_LAUNCH_CHECK("kin_mm_kernel");
-    return JB_OK;
+    // T/2 from the per-SNP missing lists
+    return kin_missing_terms(codes, ld_codes, Cs, ldcs, n, m, mu, RT, ldr, max_missing, L, ws, false, st);
 }
 
 int32_t jb_kinship_i8_finalize(const int32_t* C, int64_t ldc, int64_t n, const double* a,

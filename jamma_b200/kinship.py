@@ -87,8 +87,8 @@ class _KinshipAccumulator:
 
 
 # Missing-call density (fraction of a chunk's calls) above which the correction terms run
-# on the INT8 tensor cores instead of the sparse walk over each sample's missing SNPs.
-TC_MISSING_DENSITY = 0.003
+# on the INT8 tensor cores instead of the FP64 walk over each sample's missing SNPs.
+TC_MISSING_DENSITY = 0.03
 
 
 class _KinshipI8:
@@ -116,20 +116,21 @@ class _KinshipI8:
         self._density_scale = 1.0
 
     def add(self, codes: torch.Tensor, mu64: torch.Tensor, has_missing: bool,
-            packed: torch.Tensor | None = None, n_missing: int | None = None) -> None:
-        """Add a chunk of decoded codes (m, ld); ``packed`` are the same SNPs' .bed records
-        (used by the sparse missing-call correction).  ``n_missing``: the chunk's number of
-        missing calls (from pass-1 counts); with it, chunks whose missing calls exceed
+            n_missing: int | None = None) -> None:
+        """Add a chunk of decoded codes (m, ld).  ``n_missing``: the chunk's number of
+        missing calls (from pass-1 counts; counted on the device when not given), the
+        capacity of its per-SNP missing lists; chunks whose missing calls exceed
         TC_MISSING_DENSITY take the tensor-core correction."""
         m, ld = codes.shape
+        if has_missing and n_missing is None:
+            n_missing = int((codes[:, : self.n] == 3).sum())
         if m > self.MAX_CHUNK:  # the correction kernels take at most MAX_CHUNK SNPs per call
             for s in range(0, m, self.MAX_CHUNK):
                 e = min(s + self.MAX_CHUNK, m)
                 # the whole chunk's count bounds every part's list capacity; the density
                 # test uses the chunk's average
                 self._density_scale = m / (e - s)
-                self.add(codes[s:e], mu64[s:e], has_missing, None if packed is None else packed[s:e],
-                         n_missing)
+                self.add(codes[s:e], mu64[s:e], has_missing, n_missing)
             self._density_scale = 1.0
             return
         st = stream_handle()
@@ -140,24 +141,21 @@ class _KinshipI8:
             Cs = torch.empty((self.n, m), dtype=torch.int8, device="cuda")
         _native.call("jb_codes_to_sample_major", ptr(codes), ld, self.n, m, ptr(self.Zs), self.ldz,
                      self.col, ptr(Cs), m, st)
-        if (has_missing and n_missing is not None and self.col % 16 == 0
-                and n_missing > TC_MISSING_DENSITY * self.n * m * self._density_scale):
-            lib = _native.load()
-            ws = workspace(lib.jb_kinship_i8_tc_workspace_size(self.n, m, int(n_missing)))
+        lib = _native.load()
+        cap = int(n_missing) if has_missing else 0
+        if has_missing and self.col % 16 == 0 and \
+                n_missing > TC_MISSING_DENSITY * self.n * m * self._density_scale:
+            ws = workspace(lib.jb_kinship_i8_tc_workspace_size(self.n, m, cap))
             _native.call("jb_kinship_i8_corrections_tc", ptr(codes), ld, ptr(self.Zs), self.ldz,
                          self.col, ptr(Cs), m, self.n, m, ptr(mu64), ptr(self.a), ptr(self.b),
-                         ptr(self.RT), self.n, int(n_missing), ptr(ws), ws.numel(), st)
+                         ptr(self.RT), self.n, cap, ptr(ws), ws.numel(), st)
+        else:
+            ws = workspace(lib.jb_kinship_i8_corrections_workspace_size(self.n, m, cap))
+            _native.call("jb_kinship_i8_corrections", ptr(codes), ld, ptr(Cs), m, self.n, m,
+                         ptr(mu64), ptr(self.a), ptr(self.b), ptr(self.RT), self.n, cap, ptr(ws),
+                         ws.numel(), st)
+        if has_missing:
             self._status.append(ws[:4].clone())  # status word, checked in finish()
-            self.col += m
-            return
-        if has_missing and packed is None:
-            packed = torch.empty((m, (self.n + 3) // 4), dtype=torch.uint8, device="cuda")
-            _native.call("jb_pack_codes", ptr(codes), ld, self.n, m, ptr(packed), packed.shape[1], st)
-        bps = 0 if packed is None else packed.shape[1]
-        part = workspace(_native.load().jb_kinship_i8_partial_size(self.n, m))
-        _native.call("jb_kinship_i8_corrections", ptr(codes), ld, ptr(packed), bps, ptr(Cs), m,
-                     self.n, m, ptr(mu64), ptr(self.a), ptr(self.b), ptr(self.RT), self.n, ptr(part),
-                     part.numel(), st)
         self.col += m
 
     def add_sum_mu2(self, mu64_host: np.ndarray) -> None:
@@ -212,7 +210,7 @@ def _kinship_from_packed(packed_dev: torch.Tensor, n: int, batch_size: int, maf_
     if precision == "int8":
         acc = _KinshipI8(n, idx.size)
         acc.add(codes.index_select(0, sel), mu64, bool(np.any(c[:, 0] < n)),
-                packed_dev.index_select(0, sel), n_missing=int((n - c[:, 0]).sum()))
+                n_missing=int((n - c[:, 0]).sum()))
         acc.add_sum_mu2(c[:, 1] / np.maximum(c[:, 0], 1))
         return acc.finish(), idx.size
     acc = _KinshipAccumulator(n, max(1, min(batch_size, 8192)))
@@ -306,8 +304,7 @@ def compute_kinship_from_bed(bfile, maf_threshold: float = 0.0, miss_threshold: 
         c = counts[sub]
         mu64 = torch.from_numpy(c[:, 1] / np.maximum(c[:, 0], 1)).to("cuda")
         if i8:
-            acc.add(codes, mu64, bool(np.any(c[:, 0] < n)), None if sidx is not None else rec,
-                    n_missing=int((n - c[:, 0]).sum()))
+            acc.add(codes, mu64, bool(np.any(c[:, 0] < n)), n_missing=int((n - c[:, 0]).sum()))
             acc.add_sum_mu2(c[:, 1] / np.maximum(c[:, 0], 1))
         elif kinship_mode == 2:
             acc.add(codes, mu64, torch.from_numpy(snp_sd_from_counts(c, n)).to("cuda"))

@@ -87,7 +87,7 @@ def compute_loco_kinship(bfile, maf_threshold: float = 0.0, miss_threshold: floa
             c = counts[part]
             mu = torch.from_numpy(c[:, 1] / np.maximum(c[:, 0], 1)).cuda()
             if precision == "int8":
-                acc.add(codes, mu, bool(np.any(c[:, 0] < n)), rec, n_missing=int((n - c[:, 0]).sum()))
+                acc.add(codes, mu, bool(np.any(c[:, 0] < n)), n_missing=int((n - c[:, 0]).sum()))
                 acc.add_sum_mu2(c[:, 1] / np.maximum(c[:, 0], 1))
             else:
                 acc.add(codes, mu)

@@ -186,8 +186,7 @@ class GwasServer:
             sel = torch.from_numpy(kidx).cuda()
             cc = cnt[kidx]
             acc.add(codes.index_select(0, sel), torch.from_numpy(cc[:, 1] / np.maximum(cc[:, 0], 1)).cuda(),
-                    bool(np.any(cc[:, 0] < n)), packed.index_select(0, sel),
-                    n_missing=int((n - cc[:, 0]).sum()))
+                    bool(np.any(cc[:, 0] < n)), n_missing=int((n - cc[:, 0]).sum()))
             acc.add_sum_mu2(cc[:, 1] / np.maximum(cc[:, 0], 1))
             K = acc.finish()
             evals, U = eng.eigh_device(K)
