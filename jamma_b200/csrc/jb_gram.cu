@@ -327,19 +327,26 @@ __global__ void kin_missing_mask_kernel(const int8_t* __restrict__ Cs, int64_t l
     }
 }
 
-// One SNP for a thread's 16 samples.  A call z becomes the double 4 + z or 4 + z/4 from its
-// high word alone: the two bits land at bits 18-19 (value z) or 16-17 (value z/4) of the
-// high word 0x40100000 (4.0) with one shift per sample pair and one LOP3 per sample, and
-// one FMA with mu_j accumulates it.  The offset 4 sum_j mu_j is removed afterwards (4 mu
-// is exact, so a thread with only zero calls ends with exactly 4 x the plain sum).
+// One SNP for a thread's 16 samples.  A call z becomes the double 4 + z built in one
+// 64-bit integer multiply-add: the call's two bits, masked at bit position pos (20..30) of
+// w or of w shifted by 10 or 20, times 2^(50 - pos) land at bits 50-51 -- the top two
+// mantissa bits -- of the bit pattern of 4.0 (exponent 2, so they weigh 1 and 2), and the
+// result is already the register pair the FMA with mu_j reads.  The offset 4 sum_j mu_j is
+// removed afterwards (4 mu is exact, so a sample with only zero calls ends with exactly
+// 4 x the plain sum).
+__device__ __forceinline__ double sp_call_double(uint32_t masked, uint32_t mult) {
+    unsigned long long d;
+    asm("mad.wide.u32 %0, %1, %2, %3;" : "=l"(d) : "r"(masked), "r"(mult), "l"(0x4010000000000000ull));
+    return __longlong_as_double((long long)d);
+}
+
 __device__ __forceinline__ void sp_word(uint32_t w, double u, double (&r)[kSpSpt]) {
+    const uint32_t g[3] = {w << 20, w << 10, w};  // samples 0-4, 5-9, 10-15 at bits 20-31
 #pragma unroll
-    for (int p = 0; p < 8; ++p) {
-        const uint32_t t = p <= 4 ? (w << (16 - 4 * p)) : (w >> (4 * p - 16));
-        const int lo_s = (int)((t & 0x00030000u) | 0x40100000u);  // sample 2p: 4 + z/4
-        const int hi_s = (int)((t & 0x000C0000u) | 0x40100000u);  // sample 2p+1: 4 + z
-        r[2 * p] = fma(u, __hiloint2double(lo_s, 0), r[2 * p]);
-        r[2 * p + 1] = fma(u, __hiloint2double(hi_s, 0), r[2 * p + 1]);
+    for (int q = 0; q < kSpSpt; ++q) {
+        const int gi = q < 5 ? 0 : (q < 10 ? 1 : 2);
+        const int pos = 2 * q + (gi == 0 ? 20 : (gi == 1 ? 10 : 0));
+        r[q] = fma(u, sp_call_double(g[gi] & (3u << pos), 1u << (50 - pos)), r[q]);
     }
 }
 
@@ -384,9 +391,10 @@ __global__ void __launch_bounds__(kSpThreads, 3) kin_sp_kernel(
     }
     __syncthreads();
     // T/2 for this block: every sample of the block missing at one of k's missing SNPs.
-    // Thread t takes list entries t, t + 256, ... (one SNP's list each, read four entries
-    // at a time so the loads overlap).
-    for (int p = tid; p < cnt; p += kSpThreads) {
+    // Lane l of warp w takes list entries 8 l + w (+ 256 r): a short list spreads over all
+    // eight warps, which then reach the R walk and the final barrier together.  Each entry
+    // is one SNP's list, read four entries at a time so the loads overlap.
+    for (int p = lane * (kSpThreads / 32) + warp; p < cnt; p += kSpThreads) {
         const int64_t j = S.jl[p];
         const int64_t e0 = off[j * nb + b];
         int64_t e1 = off[j * nb + b + 1];
@@ -451,7 +459,7 @@ __global__ void __launch_bounds__(kSpThreads, 3) kin_sp_kernel(
     for (int q = 0; q < kSpSpt; ++q) {
         const int64_t i = i0 + q;
         double v = (double)(long long)S.acc[tid * kSpSpt + q] * kSpTInv;
-        if (kR) v += (q & 1) ? (r[q] - s4) : 4.0 * (r[q] - s4);
+        if (kR) v += r[q] - s4;
         if (i < n && v != 0.0) Q[k * ldq + i] += v;  // Q[i, k] (column-major, column k)
     }
 }
