@@ -118,8 +118,8 @@ int32_t jb_kinship_finalize(double* K, int64_t n, int64_t ldk, double scale,
  *   kind::i8).  Zs: n x p, row stride ldz bytes.  workspace: jb_gram_i8_workspace_size;
  *   its first int32 is a status word (non-zero if a pipeline wait timed out), read with
  *   jb_gram_status (synchronises the stream).
- * jb_kinship_i8_corrections: accumulate a, b (n doubles each) and, when Cs is given
- *   (the chunk has missing calls), Q = R + T/2 into RT (column-major n x n, ld ldr;
+ * jb_kinship_i8_corrections: accumulate a, b (n doubles each) and, when has_missing
+ *   is non-zero (the chunk has missing calls), Q = R + T/2 into RT (column-major n x n, ld ldr;
  *   T is symmetric, so R + R^T + T = Q + Q^T).  At most 16384 SNPs per call.  R runs as
  *   FP64 multiply-adds over each sample's missing SNPs (n per missing call), T/2 from
  *   per-SNP lists of missing samples in exact 2^-44 fixed point.  max_missing: capacity
@@ -146,10 +146,10 @@ int32_t jb_kinship_finalize(double* K, int64_t n, int64_t ldk, double scale,
  */
 int64_t jb_kinship_i8_tc_workspace_size(int64_t n, int64_t m, int64_t max_missing);
 int32_t jb_kinship_i8_corrections_tc(const int8_t* codes, int64_t ld_codes, const int8_t* Zs,
-                                     int64_t ldz, int64_t col0, const int8_t* Cs, int64_t ldcs,
-                                     int64_t n, int64_t m, const double* mu, double* a, double* b,
-                                     double* RT, int64_t ldr, int64_t max_missing,
-                                     void* workspace, int64_t workspace_bytes, uintptr_t stream);
+                                     int64_t ldz, int64_t col0, int64_t n, int64_t m,
+                                     const double* mu, double* a, double* b, double* RT,
+                                     int64_t ldr, int64_t max_missing, void* workspace,
+                                     int64_t workspace_bytes, uintptr_t stream);
 
 int64_t jb_gram_i8_workspace_size(int64_t n);
 int32_t jb_gram_i8(const int8_t* Zs, int64_t n, int64_t p, int64_t ldz, int32_t* C,
@@ -175,11 +175,10 @@ int32_t jb_codes_to_sample_major(const int8_t* codes, int64_t ld_codes, int64_t 
                                  int64_t m, int8_t* Zs, int64_t ldz, int64_t col0,
                                  int8_t* Cs, int64_t ldcs, uintptr_t stream);
 int64_t jb_kinship_i8_corrections_workspace_size(int64_t n, int64_t m, int64_t max_missing);
-int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes, const int8_t* Cs,
-                                  int64_t ldcs, int64_t n, int64_t m, const double* mu,
-                                  double* a, double* b, double* RT, int64_t ldr,
-                                  int64_t max_missing, void* workspace,
-                                  int64_t workspace_bytes, uintptr_t stream);
+int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes, int32_t has_missing,
+                                  int64_t n, int64_t m, const double* mu, double* a, double* b,
+                                  double* RT, int64_t ldr, int64_t max_missing,
+                                  void* workspace, int64_t workspace_bytes, uintptr_t stream);
 int32_t jb_kinship_i8_finalize(const int32_t* C, int64_t ldc, int64_t n, const double* a,
                                const double* b, double sum_mu2, const double* RT,
                                int64_t ldr, int64_t p_kept, double* K, int64_t ldk,

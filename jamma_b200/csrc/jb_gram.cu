@@ -147,27 +147,85 @@ __global__ void codes_to_sample_major_kernel(const int8_t* __restrict__ codes, i
     }
 }
 
+// The same transpose for Zs alone when codes and Zs allow 4-byte accesses: 64 SNPs x 64
+// samples per CTA, every thread loading 4 samples of one SNP and storing 4 SNPs of one
+// sample as one uint32 each.
+__global__ void __launch_bounds__(256) codes_to_sample_major_vec_kernel(
+    const int8_t* __restrict__ codes, int64_t ldc, int64_t n, int64_t m, int8_t* __restrict__ Zs,
+    int64_t ldz, int64_t col0) {
+    __shared__ uint32_t t[64][17];  // t[j][i / 4]: samples i..i+3 of SNP j
+    const int64_t j0 = (int64_t)blockIdx.x * 64, i0 = (int64_t)blockIdx.y * 64;
+    for (int r = threadIdx.x; r < 64 * 16; r += 256) {
+        const int jj = r >> 4, ii = (r & 15) * 4;
+        const int64_t j = j0 + jj, i = i0 + ii;
+        uint32_t v = 0u;
+        if (j < m) {
+            const int8_t* p = codes + j * ldc + i;
+            if (i + 4 <= n)
+                v = __ldg(reinterpret_cast<const uint32_t*>(p));
+            else
+                for (int e = 0; e < 4; ++e)
+                    if (i + e < n) v |= (uint32_t)(uint8_t)p[e] << (8 * e);
+        }
+        t[jj][ii >> 2] = v;
+    }
+    __syncthreads();
+    for (int r = threadIdx.x; r < 64 * 16; r += 256) {
+        const int ii = r >> 4, jq = (r & 15) * 4;  // sample ii, SNPs jq..jq+3
+        const int64_t i = i0 + ii, j = j0 + jq;
+        if (i >= n || j >= m) continue;
+        uint32_t w = 0u;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            uint32_t b = (t[jq + e][ii >> 2] >> (8 * (ii & 3))) & 0xffu;
+            w |= (b == 3u ? 0u : b) << (8 * e);  // missing -> 0
+        }
+        int8_t* q = Zs + i * ldz + col0 + j;
+        if (j + 4 <= m)
+            *reinterpret_cast<uint32_t*>(q) = w;
+        else
+            for (int e = 0; j + e < m; ++e) q[e] = (int8_t)(w >> (8 * e));
+    }
+}
+
 // a_i = sum_j Z_ij mu_j and b_i = sum_{j missing at i} mu_j^2 from SNP-major codes, in
 // two deterministic stages: block (256 samples) x (256 SNPs) partial sums, then an
 // ordered sum over the SNP blocks (no atomics, so results are bit-reproducible).
 __global__ void kin_vectors_partial_kernel(const int8_t* __restrict__ codes, int64_t ldc,
-                                           int64_t n, int64_t m, const double* __restrict__ mu,
+                                           int64_t n, int64_t m, int vec,
+                                           const double* __restrict__ mu,
                                            double* __restrict__ pa, double* __restrict__ pb) {
-    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t i0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) * 4;  // 4 samples
     const int64_t jb = blockIdx.y;
-    if (i >= n) return;
-    double sa = 0.0, sb = 0.0;
+    if (i0 >= n) return;
+    double sa[4] = {0.0, 0.0, 0.0, 0.0}, sb[4] = {0.0, 0.0, 0.0, 0.0};
     const int64_t j0 = jb * 256, j1 = j0 + 256 < m ? j0 + 256 : m;
+    const bool full = vec && i0 + 4 <= n;
     for (int64_t j = j0; j < j1; ++j) {
-        const int8_t c = codes[j * ldc + i];
-        const double u = __ldg(mu + j);
-        if (c == 3)
-            sb = fma(u, u, sb);
+        const int8_t* p = codes + j * ldc + i0;
+        uint32_t v = 0u;
+        if (full)
+            v = __ldg(reinterpret_cast<const uint32_t*>(p));
         else
-            sa = fma((double)c, u, sa);
+            for (int e = 0; e < 4; ++e)
+                if (i0 + e < n) v |= (uint32_t)(uint8_t)p[e] << (8 * e);
+        const double u = __ldg(mu + j);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const uint32_t c = (v >> (8 * e)) & 0xffu;
+            if (c == 3u)
+                sb[e] = fma(u, u, sb[e]);
+            else
+                sa[e] = fma((double)c, u, sa[e]);
+        }
     }
-    pa[jb * n + i] = sa;
-    pb[jb * n + i] = sb;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+        if (i0 + e < n) {
+            pa[jb * n + i0 + e] = sa[e];
+            pb[jb * n + i0 + e] = sb[e];
+        }
+    }
 }
 
 __global__ void kin_vectors_reduce_kernel(int64_t n, int64_t nblk, const double* __restrict__ pa,
@@ -313,18 +371,41 @@ __global__ void __launch_bounds__(256) kin_sp_fill_kernel(const int8_t* __restri
     }
 }
 
-// Each sample's missing SNPs of the chunk as a bitmask (one ballot per 32 SNPs of the
-// sample-major codes).
-__global__ void kin_missing_mask_kernel(const int8_t* __restrict__ Cs, int64_t ldcs, int64_t m,
-                                        uint32_t* __restrict__ mask, int64_t words) {
-    const int64_t k = blockIdx.x;
-    const int lane = threadIdx.x & 31;
-    for (int64_t j0 = 0; j0 < words * 32; j0 += blockDim.x) {
-        const int64_t j = j0 + threadIdx.x;
-        const bool miss = j < m && Cs[k * ldcs + j] == 3;
-        const uint32_t bal = __ballot_sync(0xffffffffu, miss);
-        if (lane == 0 && (j >> 5) < words) mask[k * words + (j >> 5)] = bal;
+// Each sample's missing SNPs of the chunk as bitmasks (mask[k * words + w], bit b = SNP
+// 32 w + b missing at sample k) from the SNP-major codes: a warp takes a tile of 32 SNPs x
+// 32 samples, each lane the 32 calls of one SNP, and 32 ballots transpose the bit tile.
+__global__ void __launch_bounds__(256) kin_mask_kernel(const int8_t* __restrict__ codes,
+                                                       int64_t ldc, int64_t n, int64_t m, int vec,
+                                                       uint32_t* __restrict__ mask, int64_t words) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int64_t jt = blockIdx.x;
+    const int64_t s0 = ((int64_t)blockIdx.y * 8 + warp) * 32;
+    if (s0 >= n) return;  // warp-uniform
+    const int64_t j = jt * 32 + lane;
+    uint32_t mm = 0u;  // bit q: sample s0 + q missing at SNP j
+    if (j < m) {
+        const int8_t* row = codes + j * ldc + s0;
+        if (vec && s0 + 32 <= n) {
+            const uint4 a = __ldg(reinterpret_cast<const uint4*>(row));
+            const uint4 c = __ldg(reinterpret_cast<const uint4*>(row + 16));
+            const uint32_t x[8] = {a.x, a.y, a.z, a.w, c.x, c.y, c.z, c.w};
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const uint32_t m3 = __vcmpeq4(x[e], 0x03030303u);
+                mm |= ((m3 & 1u) | ((m3 >> 7) & 2u) | ((m3 >> 14) & 4u) | ((m3 >> 21) & 8u)) << (4 * e);
+            }
+        } else {
+            for (int q = 0; q < 32; ++q)
+                if (s0 + q < n && row[q] == 3) mm |= 1u << q;
+        }
     }
+    uint32_t out = 0u;
+#pragma unroll
+    for (int q = 0; q < 32; ++q) {
+        const uint32_t bal = __ballot_sync(0xffffffffu, (mm >> q) & 1u);
+        if (lane == q) out = bal;
+    }
+    if (s0 + lane < n) mask[(s0 + lane) * words + jt] = out;
 }
 
 // One SNP for a thread's 16 samples.  A call z becomes the double 4 + z built in one
@@ -488,15 +569,16 @@ __device__ __forceinline__ void mu_digits(double mu, int8_t (&d)[4]) {
     }
 }
 
-// B (4n x ldb, K-major): B[(4k + t) * ldb + j] = d_t(mu_j) if sample k is missing at SNP j.
-__global__ void kin_rmask_kernel(const int8_t* __restrict__ Cs, int64_t ldcs, int64_t m,
+// B (4n x ldb, K-major): B[(4k + t) * ldb + j] = d_t(mu_j) if sample k is missing at SNP j
+// (bit j of k's missing-SNP mask).
+__global__ void kin_rmask_kernel(const uint32_t* __restrict__ mask, int64_t words, int64_t m,
                                  const double* __restrict__ mu, int8_t* __restrict__ B,
                                  int64_t ldb) {
     const int64_t k = blockIdx.y;
     for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < ldb;
          j += (int64_t)gridDim.x * blockDim.x) {
         int8_t d[4] = {0, 0, 0, 0};
-        if (j < m && Cs[k * ldcs + j] == 3) mu_digits(mu[j], d);
+        if (j < m && ((__ldg(mask + k * words + (j >> 5)) >> (j & 31)) & 1u)) mu_digits(mu[j], d);
 #pragma unroll
         for (int t = 0; t < 4; ++t) B[(4 * k + t) * ldb + j] = d[t];
     }
@@ -765,6 +847,16 @@ int32_t jb_codes_to_sample_major(const int8_t* codes, int64_t ld_codes, int64_t 
     JB_CHECK_ARG(!Cs || ldcs >= m, "jb_codes_to_sample_major: ldcs too small");
     if (n == 0 || m == 0) return JB_OK;
     JB_CHECK_ARG(ceil_div(n, 32) < 65536, "jb_codes_to_sample_major: n too large");
+    const bool vec = Zs && !Cs && (reinterpret_cast<uintptr_t>(codes) & 3) == 0 && ld_codes % 4 == 0 &&
+                     (reinterpret_cast<uintptr_t>(Zs) & 3) == 0 && ldz % 4 == 0 && col0 % 4 == 0;
+    if (vec) {
+        JB_CHECK_ARG(ceil_div(n, 64) < 65536, "jb_codes_to_sample_major: n too large");
+        dim3 grid((unsigned)ceil_div(m, 64), (unsigned)ceil_div(n, 64), 1);
+        codes_to_sample_major_vec_kernel<<<grid, 256, 0, as_stream(stream)>>>(codes, ld_codes, n, m, Zs,
+                                                                              ldz, col0);
+        JB_LAUNCH_CHECK("codes_to_sample_major_vec_kernel");
+        return JB_OK;
+    }
     dim3 grid((unsigned)ceil_div(m, 32), (unsigned)ceil_div(n, 32), 1);
     codes_to_sample_major_kernel<<<grid, dim3(32, 8), 0, as_stream(stream)>>>(codes, ld_codes, n,
                                                                               m, Zs, ldz, col0, Cs, ldcs);
@@ -814,19 +906,32 @@ static int32_t kin_vectors(const int8_t* codes, int64_t ld_codes, int64_t n, int
                            const double* mu, double* a, double* b, double* pa, cudaStream_t st) {
     const int64_t nblk = ceil_div(m, 256);
     double* pb = pa + nblk * n;
-    kin_vectors_partial_kernel<<<dim3((unsigned)ceil_div(n, 256), (unsigned)nblk), 256, 0, st>>>(
-        codes, ld_codes, n, m, mu, pa, pb);
+    const int vec = ((reinterpret_cast<uintptr_t>(codes) & 3) == 0 && ld_codes % 4 == 0) ? 1 : 0;
+    kin_vectors_partial_kernel<<<dim3((unsigned)ceil_div(n, 1024), (unsigned)nblk), 256, 0, st>>>(
+        codes, ld_codes, n, m, vec, mu, pa, pb);
     JB_LAUNCH_CHECK("kin_vectors_partial_kernel");
     kin_vectors_reduce_kernel<<<(unsigned)ceil_div(n, 256), 256, 0, st>>>(n, nblk, pa, pb, a, b);
     JB_LAUNCH_CHECK("kin_vectors_reduce_kernel");
     return JB_OK;
 }
 
-// Q += T/2 (with_r: + R) for one chunk: per-sample masks, per-SNP lists, kin_sp_kernel.
-static int32_t kin_missing_terms(const int8_t* codes, int64_t ld_codes, const int8_t* Cs,
-                                 int64_t ldcs, int64_t n, int64_t m, const double* mu, double* RT,
-                                 int64_t ldr, int64_t max_missing, const KinCorrWs& L,
-                                 uint8_t* ws, bool with_r, cudaStream_t st) {
+// Per-sample missing-SNP bitmasks of the chunk into the workspace.
+static int32_t kin_masks(const int8_t* codes, int64_t ld_codes, int64_t n, int64_t m,
+                         const KinCorrWs& L, uint8_t* ws, cudaStream_t st) {
+    uint32_t* mask = reinterpret_cast<uint32_t*>(ws + L.mask);
+    const int vec = ((reinterpret_cast<uintptr_t>(codes) & 15) == 0 && ld_codes % 16 == 0) ? 1 : 0;
+    JB_CHECK_ARG(ceil_div(n, 256) < 65536, "kinship corrections: n too large");
+    kin_mask_kernel<<<dim3((unsigned)L.words, (unsigned)ceil_div(n, 256)), 256, 0, st>>>(
+        codes, ld_codes, n, m, vec, mask, L.words);
+    JB_LAUNCH_CHECK("kin_mask_kernel");
+    return JB_OK;
+}
+
+// Q += T/2 (with_r: + R) for one chunk from the masks (kin_masks), per-SNP lists and
+// kin_sp_kernel.
+static int32_t kin_missing_terms(const int8_t* codes, int64_t ld_codes, int64_t n, int64_t m,
+                                 const double* mu, double* RT, int64_t ldr, int64_t max_missing,
+                                 const KinCorrWs& L, uint8_t* ws, bool with_r, cudaStream_t st) {
     int* status = reinterpret_cast<int*>(ws + L.status);
     uint32_t* mask = reinterpret_cast<uint32_t*>(ws + L.mask);
     uint32_t* zb = with_r ? reinterpret_cast<uint32_t*>(ws + L.zb) : nullptr;
@@ -834,8 +939,6 @@ static int32_t kin_missing_terms(const int8_t* codes, int64_t ld_codes, const in
     int64_t* off = reinterpret_cast<int64_t*>(ws + L.off);
     uint16_t* idx = reinterpret_cast<uint16_t*>(ws + L.idx);
     const int vec = ((reinterpret_cast<uintptr_t>(codes) & 15) == 0 && ld_codes % 16 == 0) ? 1 : 0;
-    kin_missing_mask_kernel<<<(unsigned)n, 256, 0, st>>>(Cs, ldcs, m, mask, L.words);
-    JB_LAUNCH_CHECK("kin_missing_mask_kernel");
     const unsigned snp_blocks = (unsigned)ceil_div(m, 8);
     kin_sp_count_kernel<<<snp_blocks, 256, 0, st>>>(codes, ld_codes, n, m, L.wpr, L.nb, vec, zb, cnt);
     JB_LAUNCH_CHECK("kin_sp_count_kernel");
@@ -857,10 +960,10 @@ int64_t jb_kinship_i8_corrections_workspace_size(int64_t n, int64_t m, int64_t m
     return kin_corr_ws(n, m, max_missing, false).total;
 }
 
-int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes, const int8_t* Cs,
-                                  int64_t ldcs, int64_t n, int64_t m, const double* mu, double* a,
-                                  double* b, double* RT, int64_t ldr, int64_t max_missing,
-                                  void* workspace, int64_t workspace_bytes, uintptr_t stream) {
+int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes, int32_t has_missing,
+                                  int64_t n, int64_t m, const double* mu, double* a, double* b,
+                                  double* RT, int64_t ldr, int64_t max_missing, void* workspace,
+                                  int64_t workspace_bytes, uintptr_t stream) {
     JB_CHECK_ARG(n > 0 && m >= 0 && ld_codes >= n && max_missing >= 0,
                  "jb_kinship_i8_corrections: bad shape");
     if (m == 0) return JB_OK;
@@ -875,9 +978,11 @@ int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes, const i
     uint8_t* ws = static_cast<uint8_t*>(workspace);
     JB_CUDA(cudaMemsetAsync(ws + L.status, 0, sizeof(int), st));
     int32_t rc = kin_vectors(codes, ld_codes, n, m, mu, a, b, reinterpret_cast<double*>(ws + L.pa), st);
-    if (rc || !Cs) return rc;
-    JB_CHECK_ARG(RT && ldr >= n && ldcs >= m, "jb_kinship_i8_corrections: Q buffer needed");
-    return kin_missing_terms(codes, ld_codes, Cs, ldcs, n, m, mu, RT, ldr, max_missing, L, ws, true, st);
+    if (rc || !has_missing) return rc;
+    JB_CHECK_ARG(RT && ldr >= n, "jb_kinship_i8_corrections: Q buffer needed");
+    rc = kin_masks(codes, ld_codes, n, m, L, ws, st);
+    if (rc) return rc;
+    return kin_missing_terms(codes, ld_codes, n, m, mu, RT, ldr, max_missing, L, ws, true, st);
 }
 
 int64_t jb_kinship_i8_tc_workspace_size(int64_t n, int64_t m, int64_t max_missing) {
@@ -886,14 +991,14 @@ int64_t jb_kinship_i8_tc_workspace_size(int64_t n, int64_t m, int64_t max_missin
 }
 
 int32_t jb_kinship_i8_corrections_tc(const int8_t* codes, int64_t ld_codes, const int8_t* Zs,
-                                     int64_t ldz, int64_t col0, const int8_t* Cs, int64_t ldcs,
-                                     int64_t n, int64_t m, const double* mu, double* a, double* b,
-                                     double* RT, int64_t ldr, int64_t max_missing,
-                                     void* workspace, int64_t workspace_bytes, uintptr_t stream) {
-    JB_CHECK_ARG(n > 0 && m >= 0 && ld_codes >= n && ldr >= n && ldcs >= m && max_missing >= 0,
+                                     int64_t ldz, int64_t col0, int64_t n, int64_t m,
+                                     const double* mu, double* a, double* b, double* RT,
+                                     int64_t ldr, int64_t max_missing, void* workspace,
+                                     int64_t workspace_bytes, uintptr_t stream) {
+    JB_CHECK_ARG(n > 0 && m >= 0 && ld_codes >= n && ldr >= n && max_missing >= 0,
                  "jb_kinship_i8_corrections_tc: bad shape");
     if (m == 0) return JB_OK;
-    JB_CHECK_ARG(codes && Zs && Cs && mu && a && b && RT, "jb_kinship_i8_corrections_tc: null pointer");
+    JB_CHECK_ARG(codes && Zs && mu && a && b && RT, "jb_kinship_i8_corrections_tc: null pointer");
     JB_CHECK_ARG(m <= kSpMaxChunk && 4 * n < (1ll << 31), "jb_kinship_i8_corrections_tc: chunk too large");
     JB_CHECK_ARG(col0 % 16 == 0 && ldz % 16 == 0 && ldz >= col0 + m,
                  "jb_kinship_i8_corrections_tc: Zs column block must start on 16 bytes");
@@ -906,9 +1011,11 @@ int32_t jb_kinship_i8_corrections_tc(const int8_t* codes, int64_t ld_codes, cons
     int32_t rc = kin_vectors(codes, ld_codes, n, m, mu, a, b, reinterpret_cast<double*>(ws + L.pa), st);
     if (rc) return rc;
     // R on the tensor cores
+    rc = kin_masks(codes, ld_codes, n, m, L, ws, st);
+    if (rc) return rc;
     int8_t* B = reinterpret_cast<int8_t*>(ws + L.B);
     kin_rmask_kernel<<<dim3((unsigned)ceil_div(L.ldb, 256), (unsigned)n), 256, 0, st>>>(
-        Cs, ldcs, m, mu, B, L.ldb);
+        reinterpret_cast<const uint32_t*>(ws + L.mask), L.words, m, mu, B, L.ldb);
     JB_LAUNCH_CHECK("kin_rmask_kernel");
     const int MB = (int)ceil_div(n, kBM), NB = (int)ceil_div(4 * n, 256);
     Tile* tiles = reinterpret_cast<Tile*>(ws + L.tiles);
@@ -927,7 +1034,7 @@ int32_t jb_kinship_i8_corrections_tc(const int8_t* codes, int64_t ld_codes, cons
         ta, tb, tiles, n_tiles, (int)ceil_div(m, kBK), epi, status);
     JB_LAUNCH_CHECK("i8_gemm_kernel<kinship R>");
     // T/2 from the per-SNP missing lists
-    return kin_missing_terms(codes, ld_codes, Cs, ldcs, n, m, mu, RT, ldr, max_missing, L, ws, false, st);
+    return kin_missing_terms(codes, ld_codes, n, m, mu, RT, ldr, max_missing, L, ws, false, st);
 }
 
 int32_t jb_kinship_i8_finalize(const int32_t* C, int64_t ldc, int64_t n, const double* a,

@@ -134,24 +134,21 @@ class _KinshipI8:
             self._density_scale = 1.0
             return
         st = stream_handle()
-        Cs = None
-        if has_missing:
-            if self.RT is None:
-                self.RT = torch.zeros((self.n, self.n), dtype=torch.float64, device="cuda")
-            Cs = torch.empty((self.n, m), dtype=torch.int8, device="cuda")
+        if has_missing and self.RT is None:
+            self.RT = torch.zeros((self.n, self.n), dtype=torch.float64, device="cuda")
         _native.call("jb_codes_to_sample_major", ptr(codes), ld, self.n, m, ptr(self.Zs), self.ldz,
-                     self.col, ptr(Cs), m, st)
+                     self.col, None, 0, st)
         lib = _native.load()
         cap = int(n_missing) if has_missing else 0
         if has_missing and self.col % 16 == 0 and \
                 n_missing > TC_MISSING_DENSITY * self.n * m * self._density_scale:
             ws = workspace(lib.jb_kinship_i8_tc_workspace_size(self.n, m, cap))
             _native.call("jb_kinship_i8_corrections_tc", ptr(codes), ld, ptr(self.Zs), self.ldz,
-                         self.col, ptr(Cs), m, self.n, m, ptr(mu64), ptr(self.a), ptr(self.b),
+                         self.col, self.n, m, ptr(mu64), ptr(self.a), ptr(self.b),
                          ptr(self.RT), self.n, cap, ptr(ws), ws.numel(), st)
         else:
             ws = workspace(lib.jb_kinship_i8_corrections_workspace_size(self.n, m, cap))
-            _native.call("jb_kinship_i8_corrections", ptr(codes), ld, ptr(Cs), m, self.n, m,
+            _native.call("jb_kinship_i8_corrections", ptr(codes), ld, int(has_missing), self.n, m,
                          ptr(mu64), ptr(self.a), ptr(self.b), ptr(self.RT), self.n, cap, ptr(ws),
                          ws.numel(), st)
         if has_missing:
