@@ -51,6 +51,9 @@ class GwasJob:
     maf_threshold: float = 0.01
     miss_threshold: float = 0.05
     arrival: float = 0.0
+    admitted: float = 0.0  # left the queue (HBM budget and a slot free)
+    ready: float = 0.0  # set-up done (statistics, cohort, chunk graph)
+    new_cohort: bool = False  # this job built its cohort's kinship + eigendecomposition
     done: float = 0.0
     results: dict = field(default_factory=dict)
     snp_indices: np.ndarray | None = None
@@ -157,6 +160,8 @@ class GwasServer:
                 else:
                     self._building[job.cohort_id] = _Building()
                     build = True
+            job.admitted = time.perf_counter()
+            job.new_cohort = bool(build)
             act = _Active(job, torch.cuda.Stream())
             act.bytes = need
             self.used += need
@@ -275,6 +280,7 @@ class GwasServer:
             if fut.done():
                 self.preparing.remove(item)
                 fut.result()  # re-raises a set-up failure here
+                act.job.ready = time.perf_counter()
                 self.active.append(act)
                 busy = True
         for act in list(self.active):
@@ -312,8 +318,23 @@ class GwasServer:
         return self.finished
 
     def latency_summary(self) -> dict:
-        lat = np.array([j.done - j.arrival for j in self.finished])
-        span = max(j.done for j in self.finished) - min(j.arrival for j in self.finished)
-        return {"jobs": len(self.finished), "p50_s": float(np.percentile(lat, 50)),
+        jobs = self.finished
+        lat = np.array([j.done - j.arrival for j in jobs])
+        span = max(j.done for j in jobs) - min(j.arrival for j in jobs)
+
+        def pct(v):
+            v = np.asarray(v, dtype=np.float64)
+            return {"p50_s": float(np.percentile(v, 50)), "p99_s": float(np.percentile(v, 99))} \
+                if v.size else None
+
+        # where latency goes: queue wait, set-up (split by whether the job built its
+        # cohort), and chunk execution after set-up
+        phases = {
+            "queue": pct([j.admitted - j.arrival for j in jobs]),
+            "setup_new_cohort": pct([j.ready - j.admitted for j in jobs if j.new_cohort]),
+            "setup_resident_cohort": pct([j.ready - j.admitted for j in jobs if not j.new_cohort]),
+            "run": pct([j.done - j.ready for j in jobs]),
+        }
+        return {"jobs": len(jobs), "p50_s": float(np.percentile(lat, 50)),
                 "p99_s": float(np.percentile(lat, 99)), "mean_s": float(lat.mean()),
-                "snps_per_s": self.snps_done / span if span > 0 else None}
+                "snps_per_s": self.snps_done / span if span > 0 else None, "phases": phases}
