@@ -121,12 +121,10 @@ int32_t jb_kinship_finalize(double* K, int64_t n, int64_t ldk, double scale,
  * jb_kinship_i8_corrections: accumulate a, b (n doubles each) and, when has_missing
  *   is non-zero (the chunk has missing calls), Q = R + T/2 into RT (column-major n x n, ld ldr;
  *   T is symmetric, so R + R^T + T = Q + Q^T).  At most 16384 SNPs per call.  R runs as
- *   FP64 multiply-adds over each sample's missing SNPs (n per missing call), T/2 from
- *   per-SNP lists of missing samples in exact 2^-44 fixed point.  max_missing: capacity
- *   for the chunk's missing calls (the sum over its SNPs of n - n_obs, known from pass-1
- *   counts); workspace: jb_kinship_i8_corrections_workspace_size(n, m, max_missing)
- *   bytes, its first int32 a status word read with jb_gram_status (non-zero after an
- *   exceeded capacity).  Every sum runs in a fixed order: results are bit-reproducible.
+ *   FP64 multiply-adds over each sample's missing SNPs (n per missing call); the same walk
+ *   finds the samples missing at those SNPs and adds T/2.  workspace:
+ *   jb_kinship_i8_corrections_workspace_size(n, m) bytes.  Every sum runs in a fixed
+ *   order: results are bit-reproducible.
  * jb_kinship_i8_finalize: K (n x n, ldk) = symmetric combination above / p_kept.
  */
 /*
@@ -136,20 +134,19 @@ int32_t jb_kinship_finalize(double* K, int64_t n, int64_t ldk, double scale,
  * dense part R = Z diag(mu) M^T on the INT8 tensor cores: mu_j as four base-254 digits
  * (|error| <= 4.8e-10 per mu_j, mu_j in [0, 2]) interleaved along N of one GEMM per chunk
  * whose A operand is the chunk's columns col0..col0+m of the sample-major Gram operand Zs
- * (col0 and ldz multiples of 16); T/2 = M diag(mu^2/2) M^T from per-SNP missing-sample
- * lists.  Faster than the FP64 walk of jb_kinship_i8_corrections only when several
- * per cent of the calls are missing (the dense GEMM costs the same at any density).
- * max_missing: capacity for the chunk's missing calls (the sum over its SNPs of n - n_obs,
- * known from pass-1 counts); workspace: jb_kinship_i8_tc_workspace_size(n, m,
- * max_missing) bytes, first int32 a status word read with jb_gram_status (non-zero after a
- * pipeline timeout or an exceeded capacity).
+ * (col0 and ldz multiples of 16); T/2 = M diag(mu^2/2) M^T from the same dosage-word walk
+ * as jb_kinship_i8_corrections without its FMAs.  Faster than the FP64 walk of
+ * jb_kinship_i8_corrections only when several per cent of the calls are missing (the
+ * dense GEMM costs the same at any density).  workspace: jb_kinship_i8_tc_workspace_size(n,
+ * m) bytes, first int32 a status word read with jb_gram_status (non-zero after a pipeline
+ * timeout).
  */
-int64_t jb_kinship_i8_tc_workspace_size(int64_t n, int64_t m, int64_t max_missing);
+int64_t jb_kinship_i8_tc_workspace_size(int64_t n, int64_t m);
 int32_t jb_kinship_i8_corrections_tc(const int8_t* codes, int64_t ld_codes, const int8_t* Zs,
                                      int64_t ldz, int64_t col0, int64_t n, int64_t m,
                                      const double* mu, double* a, double* b, double* RT,
-                                     int64_t ldr, int64_t max_missing, void* workspace,
-                                     int64_t workspace_bytes, uintptr_t stream);
+                                     int64_t ldr, void* workspace, int64_t workspace_bytes,
+                                     uintptr_t stream);
 
 int64_t jb_gram_i8_workspace_size(int64_t n);
 int32_t jb_gram_i8(const int8_t* Zs, int64_t n, int64_t p, int64_t ldz, int32_t* C,
@@ -174,11 +171,11 @@ int32_t jb_gram_i8_noalloc(const int8_t* Zs, int64_t n, int64_t p, int64_t ldz, 
 int32_t jb_codes_to_sample_major(const int8_t* codes, int64_t ld_codes, int64_t n,
                                  int64_t m, int8_t* Zs, int64_t ldz, int64_t col0,
                                  int8_t* Cs, int64_t ldcs, uintptr_t stream);
-int64_t jb_kinship_i8_corrections_workspace_size(int64_t n, int64_t m, int64_t max_missing);
+int64_t jb_kinship_i8_corrections_workspace_size(int64_t n, int64_t m);
 int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes, int32_t has_missing,
                                   int64_t n, int64_t m, const double* mu, double* a, double* b,
-                                  double* RT, int64_t ldr, int64_t max_missing,
-                                  void* workspace, int64_t workspace_bytes, uintptr_t stream);
+                                  double* RT, int64_t ldr, void* workspace,
+                                  int64_t workspace_bytes, uintptr_t stream);
 int32_t jb_kinship_i8_finalize(const int32_t* C, int64_t ldc, int64_t n, const double* a,
                                const double* b, double sum_mu2, const double* RT,
                                int64_t ldr, int64_t p_kept, double* K, int64_t ldk,

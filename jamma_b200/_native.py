@@ -80,12 +80,12 @@ SIGNATURES: dict[str, tuple] = {
         _i32, [_p, _p, _i64, _i64, _p, _p, _p, _p, _f64, _p, _p, _i64, _i64, _p, _i64, _u]),
     "jb_kinship_loco_f64": (_i32, [_p, _p, _i64, _i64, _i64, _p, _i64, _u]),
     "jb_codes_to_sample_major": (_i32, [_p, _i64, _i64, _i64, _p, _i64, _i64, _p, _i64, _u]),
-    "jb_kinship_i8_corrections_workspace_size": (_i64, [_i64, _i64, _i64]),
-    "jb_kinship_i8_tc_workspace_size": (_i64, [_i64, _i64, _i64]),
+    "jb_kinship_i8_corrections_workspace_size": (_i64, [_i64, _i64]),
+    "jb_kinship_i8_tc_workspace_size": (_i64, [_i64, _i64]),
     "jb_kinship_i8_corrections_tc": (
-        _i32, [_p, _i64, _p, _i64, _i64, _i64, _i64, _p, _p, _p, _p, _i64, _i64, _p, _i64, _u]),
+        _i32, [_p, _i64, _p, _i64, _i64, _i64, _i64, _p, _p, _p, _p, _i64, _p, _i64, _u]),
     "jb_kinship_i8_corrections": (
-        _i32, [_p, _i64, _i32, _i64, _i64, _p, _p, _p, _p, _i64, _i64, _p, _i64, _u]),
+        _i32, [_p, _i64, _i32, _i64, _i64, _p, _p, _p, _p, _i64, _p, _i64, _u]),
     "jb_kinship_i8_finalize": (_i32, [_p, _i64, _i64, _p, _p, _f64, _p, _i64, _i64, _p, _i64, _u]),
     "jb_ozaki_workspace_size": (_i64, [_i64]),
     "jb_ozaki_prepare": (_i32, [_p, _i64, _i64, _p, _i64, _u]),

@@ -247,30 +247,28 @@ __global__ void kin_vectors_reduce_kernel(int64_t n, int64_t nblk, const double*
 //                                 T_ik = sum_{j in miss(k) and miss(i)} mu_j^2
 // (z_ij the 0/1/2 call, 0 where missing).  R is n x nnz(M) multiply-adds: with 1 % of calls
 // missing that is 1 % of a dense Z diag(mu) M^T, so it runs on the FP64 pipe from
-// registers rather than densely on the tensor cores.  T has n nnz(M) p terms (p the
-// missing fraction) and comes from per-SNP lists of missing samples.
+// registers rather than densely on the tensor cores.
 //
-// kin_sp_count_kernel / kin_sp_fill_kernel (one warp per SNP): the chunk's calls as
-// "dosage words" (16 samples per uint32, 2 bits each: the call, 0 where missing) and, per
-// (SNP j, block b of kSpBlock samples), the block-local indices of j's missing samples
-// (CSR, rows j * nb + b, offsets from kin_scan_kernel).
+// kin_sp_words_kernel (one warp per SNP): the chunk's calls as "dosage words", 16 samples
+// per uint32, 2 bits each: the call 0/1/2, or 3 where it is missing.
 //
 // kin_sp_kernel: one CTA per (sample k, block b of 4096 samples i).  The CTA turns k's
-// missing-SNP bitmask into an increasing list in shared memory, adds T/2 for its block
-// from the per-SNP lists (exact: mu_j^2/2 in 2^-44 fixed point, int64 shared atomics, so
-// the order of the adds does not matter), then walks the list once for R with every
-// thread owning 16 consecutive samples in registers (one dosage word per SNP).
+// missing-SNP bitmask into an increasing list in shared memory, then walks it once with
+// every thread owning 16 consecutive samples i: per SNP j one dosage word, and per sample
+// one FMA of mu_j with the word's 2-bit value c as the double 4 + c.  A missing call
+// (c = 3) adds 3 mu_j more than R wants; it also marks the (i, k, j) triple of T.  Two
+// bit operations per word find the missing calls, and for each of them a rare branch adds
+// mu_j^2/2 - 3 mu_j into the sample's slot in shared memory (thread-private, summed in SNP
+// order).  So R + T/2 comes out of one walk with no per-SNP lists and no atomics.
 constexpr int kSpThreads = 256;
 constexpr int kSpSpt = 16;                      // samples per thread = one dosage word
 constexpr int kSpBlock = kSpThreads * kSpSpt;  // samples per CTA
 constexpr int kSpWords = kSpBlock / 16;        // dosage words per CTA
 constexpr int kSpMaxChunk = 16384;             // SNPs per call (list in shared memory)
-constexpr double kSpTScale = 17592186044416.0; // 2^44
-constexpr double kSpTInv = 1.0 / 17592186044416.0;
 
 struct SpSmem {
-    unsigned long long acc[kSpBlock];  // T/2 of the block, fixed point
-    uint16_t jl[kSpMaxChunk];          // k's missing SNPs, increasing
+    double corr[kSpSpt][kSpThreads];  // per-thread missing-call terms, [sample][thread]
+    uint16_t jl[kSpMaxChunk];         // k's missing SNPs, increasing
     int warp_sum[kSpThreads / 32];
 };
 
@@ -303,71 +301,18 @@ __device__ __forceinline__ void sp_load16(const int8_t* __restrict__ row, int64_
     }
 }
 
-__device__ __forceinline__ int warp_sum_i(int v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-__global__ void __launch_bounds__(256) kin_sp_count_kernel(const int8_t* __restrict__ codes,
+__global__ void __launch_bounds__(256) kin_sp_words_kernel(const int8_t* __restrict__ codes,
                                                            int64_t ldc, int64_t n, int64_t m,
-                                                           int64_t wpr, int nb, int vec,
-                                                           uint32_t* __restrict__ zb,
-                                                           int32_t* __restrict__ cnt) {
+                                                           int64_t wpr, int vec,
+                                                           uint32_t* __restrict__ zb) {
     const int64_t j = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (j >= m) return;  // warp-uniform
     const int8_t* row = codes + j * ldc;
-    for (int bb = 0; bb < nb; ++bb) {
-        int c = 0;
-        const int64_t w1 = (int64_t)(bb + 1) * kSpWords < wpr ? (int64_t)(bb + 1) * kSpWords : wpr;
-        for (int64_t wi = (int64_t)bb * kSpWords + lane; wi < w1; wi += 32) {
-            uint32_t z, miss;
-            sp_load16(row, wi * 16, n, vec != 0, z, miss);
-            if (zb) zb[j * wpr + wi] = z;
-            c += __popc(miss);
-        }
-        c = warp_sum_i(c);
-        if (lane == 0) cnt[j * nb + bb] = c;
-    }
-}
-
-__global__ void __launch_bounds__(256) kin_sp_fill_kernel(const int8_t* __restrict__ codes,
-                                                          int64_t ldc, int64_t n, int64_t m,
-                                                          int64_t wpr, int nb, int vec,
-                                                          const int64_t* __restrict__ off,
-                                                          uint16_t* __restrict__ idx, int64_t cap,
-                                                          int* __restrict__ err) {
-    const int64_t j = (int64_t)blockIdx.x * 8 + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    if (j >= m) return;  // warp-uniform
-    const int8_t* row = codes + j * ldc;
-    for (int bb = 0; bb < nb; ++bb) {
-        int64_t pos = off[j * nb + bb];
-#pragma unroll 1
-        for (int it = 0; it < kSpWords / 32; ++it) {
-            const int64_t wl = (int64_t)it * 32 + lane, wi = (int64_t)bb * kSpWords + wl;
-            uint32_t z = 0u, miss = 0u;
-            if (wi < wpr) sp_load16(row, wi * 16, n, vec != 0, z, miss);
-            const int c = __popc(miss);
-            int incl = c;
-#pragma unroll
-            for (int o = 1; o < 32; o <<= 1) {
-                const int t = __shfl_up_sync(0xffffffffu, incl, o);
-                if (lane >= o) incl += t;
-            }
-            int64_t e = pos + incl - c;
-            while (miss) {
-                const int bit = __ffs(miss) - 1;
-                miss &= miss - 1u;
-                if (e < cap)
-                    idx[e] = (uint16_t)(wl * 16 + (bit >> 1));
-                else
-                    atomicCAS(err, 0, 300);  // list capacity exceeded: entry skipped
-                ++e;
-            }
-            pos += __shfl_sync(0xffffffffu, incl, 31);
-        }
+    for (int64_t wi = lane; wi < wpr; wi += 32) {
+        uint32_t z, miss;
+        sp_load16(row, wi * 16, n, vec != 0, z, miss);
+        zb[j * wpr + wi] = z | miss | (miss << 1);  // missing -> 3
     }
 }
 
@@ -408,8 +353,8 @@ __global__ void __launch_bounds__(256) kin_mask_kernel(const int8_t* __restrict_
     if (s0 + lane < n) mask[(s0 + lane) * words + jt] = out;
 }
 
-// One SNP for a thread's 16 samples.  A call z becomes the double 4 + z built in one
-// 64-bit integer multiply-add: the call's two bits, masked at bit position pos (20..30) of
+// One SNP for a thread's 16 samples.  A word value c (0..3) becomes the double 4 + c built
+// in one 64-bit integer multiply-add: the two bits, masked at bit position pos (20..30) of
 // w or of w shifted by 10 or 20, times 2^(50 - pos) land at bits 50-51 -- the top two
 // mantissa bits -- of the bit pattern of 4.0 (exponent 2, so they weigh 1 and 2), and the
 // result is already the register pair the FMA with mu_j reads.  The offset 4 sum_j mu_j is
@@ -434,8 +379,7 @@ __device__ __forceinline__ void sp_word(uint32_t w, double u, double (&r)[kSpSpt
 template <bool kR>
 __global__ void __launch_bounds__(kSpThreads, 3) kin_sp_kernel(
     const uint32_t* __restrict__ zb, int64_t wpr, const uint32_t* __restrict__ mask,
-    int64_t words, const int64_t* __restrict__ off, const uint16_t* __restrict__ idx,
-    int64_t cap, int nb, const double* __restrict__ mu, int64_t n, double* __restrict__ Q,
+    int64_t words, const double* __restrict__ mu, int64_t n, double* __restrict__ Q,
     int64_t ldq) {
     extern __shared__ __align__(16) unsigned char sp_smem_raw[];
     SpSmem& S = *reinterpret_cast<SpSmem*>(sp_smem_raw);
@@ -454,7 +398,8 @@ __global__ void __launch_bounds__(kSpThreads, 3) kin_sp_kernel(
         if (lane >= o) incl += t;
     }
     if (lane == 31) S.warp_sum[warp] = incl;
-    for (int e = tid; e < kSpBlock; e += kSpThreads) S.acc[e] = 0ull;
+#pragma unroll
+    for (int q = 0; q < kSpSpt; ++q) S.corr[q][tid] = 0.0;  // this thread's own slots
     __syncthreads();
     int pos = incl - c, cnt = 0;
 #pragma unroll
@@ -471,75 +416,63 @@ __global__ void __launch_bounds__(kSpThreads, 3) kin_sp_kernel(
         m1 &= m1 - 1u;
     }
     __syncthreads();
-    // T/2 for this block: every sample of the block missing at one of k's missing SNPs.
-    // Lane l of warp w takes list entries 8 l + w (+ 256 r): a short list spreads over all
-    // eight warps, which then reach the R walk and the final barrier together.  Each entry
-    // is one SNP's list, read four entries at a time so the loads overlap.
-    for (int p = lane * (kSpThreads / 32) + warp; p < cnt; p += kSpThreads) {
-        const int64_t j = S.jl[p];
-        const int64_t e0 = off[j * nb + b];
-        int64_t e1 = off[j * nb + b + 1];
-        e1 = e1 < cap ? e1 : cap;  // filled entries only
-        const double u = __ldg(mu + j);
-        const unsigned long long h = (unsigned long long)__double2ll_rn(0.5 * u * u * kSpTScale);
-        for (int64_t e = e0; e < e1; e += 4) {
-            int v[4];
-#pragma unroll
-            for (int x = 0; x < 4; ++x) v[x] = e + x < e1 ? (int)__ldg(idx + e + x) : -1;
-#pragma unroll
-            for (int x = 0; x < 4; ++x)
-                if (v[x] >= 0) atomicAdd(&S.acc[v[x]], h);
-        }
-    }
     double r[kSpSpt];
 #pragma unroll
     for (int q = 0; q < kSpSpt; ++q) r[q] = 0.0;
     double s = 0.0;
     const int64_t wi = (int64_t)b * kSpWords + tid;
-    if (kR) {
-        const bool act = wi < wpr;
-        const uint32_t* __restrict__ zc = zb + (act ? wi : 0);
-        uint32_t wn[4];
-        double un[4];
-        auto fetch = [&](int p0) {
+    const bool act = wi < wpr;
+    const uint32_t* __restrict__ zc = zb + (act ? wi : 0);
+    uint32_t wn[4];
+    double un[4];
+    auto fetch = [&](int p0) {
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                const int p = p0 + e;
-                if (p < cnt) {
-                    const int64_t j = S.jl[p];
-                    un[e] = __ldg(mu + j);
-                    wn[e] = act ? __ldg(zc + j * wpr) : 0u;
-                } else {
-                    un[e] = 0.0;
-                    wn[e] = 0u;
-                }
+        for (int e = 0; e < 4; ++e) {
+            const int p = p0 + e;
+            if (p < cnt) {
+                const int64_t j = S.jl[p];
+                un[e] = __ldg(mu + j);
+                wn[e] = act ? __ldg(zc + j * wpr) : 0u;
+            } else {
+                un[e] = 0.0;
+                wn[e] = 0u;
             }
-        };
-        fetch(0);
+        }
+    };
+    fetch(0);
 #pragma unroll 1
-        for (int p0 = 0; p0 < cnt; p0 += 4) {
-            uint32_t w[4];
-            double u[4];
+    for (int p0 = 0; p0 < cnt; p0 += 4) {
+        uint32_t w[4];
+        double u[4];
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
-                w[e] = wn[e];
-                u[e] = un[e];
-            }
-            fetch(p0 + 4);
+        for (int e = 0; e < 4; ++e) {
+            w[e] = wn[e];
+            u[e] = un[e];
+        }
+        fetch(p0 + 4);
 #pragma unroll
-            for (int e = 0; e < 4; ++e) {
+        for (int e = 0; e < 4; ++e) {
+            if (kR) {
                 s += u[e];
                 sp_word(w[e], u[e], r);
             }
+            uint32_t mm = w[e] & (w[e] >> 1) & 0x55555555u;  // bit 2q: sample q missing
+            if (mm) {
+                const double h = kR ? fma(0.5 * u[e], u[e], -3.0 * u[e]) : 0.5 * u[e] * u[e];
+                do {
+                    const int q = (__ffs(mm) - 1) >> 1;
+                    S.corr[q][tid] += h;
+                    mm &= mm - 1u;
+                } while (mm);
+            }
         }
     }
-    __syncthreads();  // T/2 complete
     const double s4 = 4.0 * s;
     const int64_t i0 = (int64_t)b * kSpBlock + (int64_t)tid * kSpSpt;
 #pragma unroll
     for (int q = 0; q < kSpSpt; ++q) {
         const int64_t i = i0 + q;
-        double v = (double)(long long)S.acc[tid * kSpSpt + q] * kSpTInv;
+        double v = S.corr[q][tid];
         if (kR) v += r[q] - s4;
         if (i < n && v != 0.0) Q[k * ldq + i] += v;  // Q[i, k] (column-major, column k)
     }
@@ -554,7 +487,7 @@ __global__ void __launch_bounds__(kSpThreads, 3) kin_sp_kernel(
 // is B_t's row k -- so one GEMM per chunk (M = n samples i, N = 4n, K = m SNPs) leaves
 // every (i, k) with its four planes in one tile, and the epilogue adds
 // (2/127) (((C3 w3 + C2 w2) + C1 w1) + C0) to Q[i, k].  The missing x missing term
-// T/2 = M diag(mu^2/2) M^T stays sparse (kin_mm_kernel).
+// T/2 = M diag(mu^2/2) M^T comes from the dosage-word walk (kin_sp_kernel<false>).
 constexpr double kMuScale = 2.0 / 127.0;
 __device__ __constant__ double kPlaneW[4] = {1.0, 1.0 / 254.0, 1.0 / (254.0 * 254.0),
                                              1.0 / (254.0 * 254.0 * 254.0)};
@@ -613,33 +546,6 @@ struct KinREpi {
         }
     }
 };
-
-// offsets[0..m] = exclusive scan of cnt (one CTA of 1024 threads, contiguous segments).
-__global__ void kin_scan_kernel(const int32_t* __restrict__ cnt, int64_t m,
-                                int64_t* __restrict__ offsets) {
-    __shared__ int64_t part[1024];
-    const int t = threadIdx.x;
-    const int64_t per = (m + 1023) / 1024, s0 = t * per, s1 = s0 + per < m ? s0 + per : m;
-    int64_t sum = 0;
-    for (int64_t j = s0; j < s1; ++j) sum += cnt[j];
-    part[t] = sum;
-    __syncthreads();
-    if (t == 0) {
-        int64_t acc = 0;
-        for (int w = 0; w < 1024; ++w) {
-            const int64_t v = part[w];
-            part[w] = acc;
-            acc += v;
-        }
-        offsets[m] = acc;
-    }
-    __syncthreads();
-    int64_t acc = part[t];
-    for (int64_t j = s0; j < s1; ++j) {
-        offsets[j] = acc;
-        acc += cnt[j];
-    }
-}
 
 // K = (C - a_i - a_j + s - b_i - b_j + Q_ij + Q_ji) / p, symmetric, column-major.
 __global__ void kin_finalize_i8_kernel(const int32_t* __restrict__ C, int64_t ldc, int64_t n,
@@ -866,10 +772,10 @@ int32_t jb_codes_to_sample_major(const int8_t* codes, int64_t ld_codes, int64_t 
 
 // Workspace of the correction entry points (tc: with the tensor-core R operand).
 struct KinCorrWs {
-    int64_t status, pa, mask, zb, cnt, off, idx, tiles, B, ldb, total, wpr, words;
+    int64_t status, pa, mask, zb, tiles, B, ldb, total, wpr, words;
     int nb;
 };
-static KinCorrWs kin_corr_ws(int64_t n, int64_t m, int64_t max_missing, bool tc) {
+static KinCorrWs kin_corr_ws(int64_t n, int64_t m, bool tc) {
     KinCorrWs w;
     const int64_t mm = m > 0 ? m : 1;
     const int64_t nblk = ceil_div(mm, 256);
@@ -885,13 +791,7 @@ static KinCorrWs kin_corr_ws(int64_t n, int64_t m, int64_t max_missing, bool tc)
     w.mask = off;
     off += a256(n * w.words * 4);
     w.zb = off;
-    off += tc ? 0 : a256(mm * w.wpr * 4);
-    w.cnt = off;
-    off += a256(mm * w.nb * 4);
-    w.off = off;
-    off += a256((mm * w.nb + 1) * 8);
-    w.idx = off;
-    off += a256((max_missing > 0 ? max_missing : 1) * 2);
+    off += a256(mm * w.wpr * 4);
     w.ldb = (mm + 127) / 128 * 128;
     w.tiles = off;
     off += tc ? a256(ceil_div(n, kBM) * ceil_div(4 * n, 256) * (int64_t)sizeof(Tile)) : 0;
@@ -927,51 +827,39 @@ static int32_t kin_masks(const int8_t* codes, int64_t ld_codes, int64_t n, int64
     return JB_OK;
 }
 
-// Q += T/2 (with_r: + R) for one chunk from the masks (kin_masks), per-SNP lists and
-// kin_sp_kernel.
+// Q += T/2 (with_r: + R) for one chunk from the masks (kin_masks) and the dosage words.
 static int32_t kin_missing_terms(const int8_t* codes, int64_t ld_codes, int64_t n, int64_t m,
-                                 const double* mu, double* RT, int64_t ldr, int64_t max_missing,
-                                 const KinCorrWs& L, uint8_t* ws, bool with_r, cudaStream_t st) {
-    int* status = reinterpret_cast<int*>(ws + L.status);
-    uint32_t* mask = reinterpret_cast<uint32_t*>(ws + L.mask);
-    uint32_t* zb = with_r ? reinterpret_cast<uint32_t*>(ws + L.zb) : nullptr;
-    int32_t* cnt = reinterpret_cast<int32_t*>(ws + L.cnt);
-    int64_t* off = reinterpret_cast<int64_t*>(ws + L.off);
-    uint16_t* idx = reinterpret_cast<uint16_t*>(ws + L.idx);
+                                 const double* mu, double* RT, int64_t ldr, const KinCorrWs& L,
+                                 uint8_t* ws, bool with_r, cudaStream_t st) {
+    const uint32_t* mask = reinterpret_cast<const uint32_t*>(ws + L.mask);
+    uint32_t* zb = reinterpret_cast<uint32_t*>(ws + L.zb);
     const int vec = ((reinterpret_cast<uintptr_t>(codes) & 15) == 0 && ld_codes % 16 == 0) ? 1 : 0;
-    const unsigned snp_blocks = (unsigned)ceil_div(m, 8);
-    kin_sp_count_kernel<<<snp_blocks, 256, 0, st>>>(codes, ld_codes, n, m, L.wpr, L.nb, vec, zb, cnt);
-    JB_LAUNCH_CHECK("kin_sp_count_kernel");
-    kin_scan_kernel<<<1, 1024, 0, st>>>(cnt, m * L.nb, off);
-    JB_LAUNCH_CHECK("kin_scan_kernel");
-    kin_sp_fill_kernel<<<snp_blocks, 256, 0, st>>>(codes, ld_codes, n, m, L.wpr, L.nb, vec, off, idx,
-                                                   max_missing, status);
-    JB_LAUNCH_CHECK("kin_sp_fill_kernel");
+    kin_sp_words_kernel<<<(unsigned)ceil_div(m, 8), 256, 0, st>>>(codes, ld_codes, n, m, L.wpr, vec, zb);
+    JB_LAUNCH_CHECK("kin_sp_words_kernel");
     auto kern = with_r ? kin_sp_kernel<true> : kin_sp_kernel<false>;
     JB_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SpSmem)));
     kern<<<dim3((unsigned)n, (unsigned)L.nb), kSpThreads, sizeof(SpSmem), st>>>(
-        zb, L.wpr, mask, L.words, off, idx, max_missing, L.nb, mu, n, RT, ldr);
+        zb, L.wpr, mask, L.words, mu, n, RT, ldr);
     JB_LAUNCH_CHECK("kin_sp_kernel");
     return JB_OK;
 }
 
-int64_t jb_kinship_i8_corrections_workspace_size(int64_t n, int64_t m, int64_t max_missing) {
-    if (n <= 0 || m < 0 || max_missing < 0) return -1;
-    return kin_corr_ws(n, m, max_missing, false).total;
+int64_t jb_kinship_i8_corrections_workspace_size(int64_t n, int64_t m) {
+    if (n <= 0 || m < 0) return -1;
+    return kin_corr_ws(n, m, false).total;
 }
 
 int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes, int32_t has_missing,
                                   int64_t n, int64_t m, const double* mu, double* a, double* b,
-                                  double* RT, int64_t ldr, int64_t max_missing, void* workspace,
+                                  double* RT, int64_t ldr, void* workspace,
                                   int64_t workspace_bytes, uintptr_t stream) {
-    JB_CHECK_ARG(n > 0 && m >= 0 && ld_codes >= n && max_missing >= 0,
-                 "jb_kinship_i8_corrections: bad shape");
+    JB_CHECK_ARG(n > 0 && m >= 0 && ld_codes >= n, "jb_kinship_i8_corrections: bad shape");
     if (m == 0) return JB_OK;
     JB_CHECK_ARG(m <= kSpMaxChunk, "jb_kinship_i8_corrections: at most %d SNPs per call", kSpMaxChunk);
     JB_CHECK_ARG(codes && mu && a && b, "jb_kinship_i8_corrections: null pointer");
     JB_CHECK_ARG(n * ceil_div(n, kSpBlock) < (1ll << 31) && n < (1ll << 31),
                  "jb_kinship_i8_corrections: n too large");
-    const KinCorrWs L = kin_corr_ws(n, m, max_missing, false);
+    const KinCorrWs L = kin_corr_ws(n, m, false);
     JB_CHECK_ARG(workspace && workspace_bytes >= L.total,
                  "jb_kinship_i8_corrections: workspace too small");
     cudaStream_t st = as_stream(stream);
@@ -982,27 +870,27 @@ int32_t jb_kinship_i8_corrections(const int8_t* codes, int64_t ld_codes, int32_t
     JB_CHECK_ARG(RT && ldr >= n, "jb_kinship_i8_corrections: Q buffer needed");
     rc = kin_masks(codes, ld_codes, n, m, L, ws, st);
     if (rc) return rc;
-    return kin_missing_terms(codes, ld_codes, n, m, mu, RT, ldr, max_missing, L, ws, true, st);
+    return kin_missing_terms(codes, ld_codes, n, m, mu, RT, ldr, L, ws, true, st);
 }
 
-int64_t jb_kinship_i8_tc_workspace_size(int64_t n, int64_t m, int64_t max_missing) {
-    if (n <= 0 || m < 0 || max_missing < 0) return -1;
-    return kin_corr_ws(n, m, max_missing, true).total;
+int64_t jb_kinship_i8_tc_workspace_size(int64_t n, int64_t m) {
+    if (n <= 0 || m < 0) return -1;
+    return kin_corr_ws(n, m, true).total;
 }
 
 int32_t jb_kinship_i8_corrections_tc(const int8_t* codes, int64_t ld_codes, const int8_t* Zs,
                                      int64_t ldz, int64_t col0, int64_t n, int64_t m,
                                      const double* mu, double* a, double* b, double* RT,
-                                     int64_t ldr, int64_t max_missing, void* workspace,
-                                     int64_t workspace_bytes, uintptr_t stream) {
-    JB_CHECK_ARG(n > 0 && m >= 0 && ld_codes >= n && ldr >= n && max_missing >= 0,
+                                     int64_t ldr, void* workspace, int64_t workspace_bytes,
+                                     uintptr_t stream) {
+    JB_CHECK_ARG(n > 0 && m >= 0 && ld_codes >= n && ldr >= n,
                  "jb_kinship_i8_corrections_tc: bad shape");
     if (m == 0) return JB_OK;
     JB_CHECK_ARG(codes && Zs && mu && a && b && RT, "jb_kinship_i8_corrections_tc: null pointer");
     JB_CHECK_ARG(m <= kSpMaxChunk && 4 * n < (1ll << 31), "jb_kinship_i8_corrections_tc: chunk too large");
     JB_CHECK_ARG(col0 % 16 == 0 && ldz % 16 == 0 && ldz >= col0 + m,
                  "jb_kinship_i8_corrections_tc: Zs column block must start on 16 bytes");
-    const KinCorrWs L = kin_corr_ws(n, m, max_missing, true);
+    const KinCorrWs L = kin_corr_ws(n, m, true);
     JB_CHECK_ARG(workspace && workspace_bytes >= L.total, "jb_kinship_i8_corrections_tc: workspace too small");
     cudaStream_t st = as_stream(stream);
     uint8_t* ws = static_cast<uint8_t*>(workspace);
@@ -1034,7 +922,7 @@ int32_t jb_kinship_i8_corrections_tc(const int8_t* codes, int64_t ld_codes, cons
         ta, tb, tiles, n_tiles, (int)ceil_div(m, kBK), epi, status);
     JB_LAUNCH_CHECK("i8_gemm_kernel<kinship R>");
     // T/2 from the per-SNP missing lists
-    return kin_missing_terms(codes, ld_codes, n, m, mu, RT, ldr, max_missing, L, ws, false, st);
+    return kin_missing_terms(codes, ld_codes, n, m, mu, RT, ldr, L, ws, false, st);
 }
 
 int32_t jb_kinship_i8_finalize(const int32_t* C, int64_t ldc, int64_t n, const double* a,

@@ -118,17 +118,15 @@ class _KinshipI8:
     def add(self, codes: torch.Tensor, mu64: torch.Tensor, has_missing: bool,
             n_missing: int | None = None) -> None:
         """Add a chunk of decoded codes (m, ld).  ``n_missing``: the chunk's number of
-        missing calls (from pass-1 counts; counted on the device when not given), the
-        capacity of its per-SNP missing lists; chunks whose missing calls exceed
-        TC_MISSING_DENSITY take the tensor-core correction."""
+        missing calls (from pass-1 counts; counted on the device when not given); chunks
+        whose missing calls exceed TC_MISSING_DENSITY take the tensor-core correction."""
         m, ld = codes.shape
         if has_missing and n_missing is None:
             n_missing = int((codes[:, : self.n] == 3).sum())
         if m > self.MAX_CHUNK:  # the correction kernels take at most MAX_CHUNK SNPs per call
             for s in range(0, m, self.MAX_CHUNK):
                 e = min(s + self.MAX_CHUNK, m)
-                # the whole chunk's count bounds every part's list capacity; the density
-                # test uses the chunk's average
+                # the density test uses the whole chunk's average
                 self._density_scale = m / (e - s)
                 self.add(codes[s:e], mu64[s:e], has_missing, n_missing)
             self._density_scale = 1.0
@@ -139,17 +137,16 @@ class _KinshipI8:
         _native.call("jb_codes_to_sample_major", ptr(codes), ld, self.n, m, ptr(self.Zs), self.ldz,
                      self.col, None, 0, st)
         lib = _native.load()
-        cap = int(n_missing) if has_missing else 0
         if has_missing and self.col % 16 == 0 and \
                 n_missing > TC_MISSING_DENSITY * self.n * m * self._density_scale:
-            ws = workspace(lib.jb_kinship_i8_tc_workspace_size(self.n, m, cap))
+            ws = workspace(lib.jb_kinship_i8_tc_workspace_size(self.n, m))
             _native.call("jb_kinship_i8_corrections_tc", ptr(codes), ld, ptr(self.Zs), self.ldz,
                          self.col, self.n, m, ptr(mu64), ptr(self.a), ptr(self.b),
-                         ptr(self.RT), self.n, cap, ptr(ws), ws.numel(), st)
+                         ptr(self.RT), self.n, ptr(ws), ws.numel(), st)
         else:
-            ws = workspace(lib.jb_kinship_i8_corrections_workspace_size(self.n, m, cap))
+            ws = workspace(lib.jb_kinship_i8_corrections_workspace_size(self.n, m))
             _native.call("jb_kinship_i8_corrections", ptr(codes), ld, int(has_missing), self.n, m,
-                         ptr(mu64), ptr(self.a), ptr(self.b), ptr(self.RT), self.n, cap, ptr(ws),
+                         ptr(mu64), ptr(self.a), ptr(self.b), ptr(self.RT), self.n, ptr(ws),
                          ws.numel(), st)
         if has_missing:
             self._status.append(ws[:4].clone())  # status word, checked in finish()
