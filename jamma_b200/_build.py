@@ -56,7 +56,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
         objs.append(str(obj))
     tmp = LIB.with_suffix(".so.tmp")
     link = [nvcc, "-shared", "-o", str(tmp)] + ARCH + objs + [
-        "-L", str(cuda / "lib64"), "-lcublas", "-lcusolver",
+        "-L", str(cuda / "lib64"), "-lcublas", "-lcusolver", "-ldl",
         "-Xlinker", f"-rpath,{cuda / 'lib64'}",
     ]
     if verbose:

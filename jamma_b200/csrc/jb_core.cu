@@ -1,5 +1,10 @@
 // libjamma_b200 core: error plumbing, PLINK decode, imputation, plain FP64 kinship,
 // FP64 eigendecomposition (cuSOLVER) and plain FP64 rotation (cuBLAS).
+#include <cusolverMg.h>
+#include <dlfcn.h>
+
+#include <mutex>
+#include <string>
 #include "jb_common.cuh"
 
 #include <mutex>
@@ -333,23 +338,181 @@ int32_t jb_kinship_finalize(double* K, int64_t n, int64_t ldk, double scale, uin
     return JB_OK;
 }
 
-int64_t jb_eigh_workspace_size(int64_t n) {
+// The single-GPU divide-and-conquer solver (cusolverDnXsyevd) rejects matrices whose
+// workspace, about 4 n^2 doubles, passes 2^31 elements (n above ~23 000).  Larger n go to
+// the cusolverMg solver on a one-device grid, whose workspace size is 64-bit: with one
+// device its 1-D column block-cyclic layout is the plain column-major matrix (ld = n).
+namespace {
+constexpr int64_t kMgColBlock = 256;
+
+// cusolverMg is loaded at its first use, from the directory of the libcusolver the process
+// already runs (in a PyTorch process that is PyTorch's own copy), so it pairs with the
+// cuBLAS that is loaded; linking it at build time could pair it with another cuBLAS.
+struct MgApi {
+    decltype(&cusolverMgCreate) create;
+    decltype(&cusolverMgDestroy) destroy;
+    decltype(&cusolverMgDeviceSelect) device_select;
+    decltype(&cusolverMgCreateDeviceGrid) create_grid;
+    decltype(&cusolverMgDestroyGrid) destroy_grid;
+    decltype(&cusolverMgCreateMatrixDesc) create_desc;
+    decltype(&cusolverMgDestroyMatrixDesc) destroy_desc;
+    decltype(&cusolverMgSyevd_bufferSize) syevd_buffer_size;
+    decltype(&cusolverMgSyevd) syevd;
+};
+
+const MgApi* mg_api() {
+    static MgApi api;
+    static bool ok = false;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* lib = nullptr;
+        Dl_info info;
+        if (dladdr(reinterpret_cast<void*>(&cusolverDnCreate), &info) && info.dli_fname) {
+            std::string path(info.dli_fname);
+            const size_t slash = path.rfind('/');
+            if (slash != std::string::npos) {
+                path = path.substr(0, slash + 1) + "libcusolverMg.so.11";
+                lib = dlopen(path.c_str(), RTLD_NOW | RTLD_LOCAL);
+            }
+        }
+        if (!lib) lib = dlopen("libcusolverMg.so.11", RTLD_NOW | RTLD_LOCAL);
+        if (!lib) return;
+        auto sym = [&](const char* name) { return dlsym(lib, name); };
+        api.create = reinterpret_cast<decltype(api.create)>(sym("cusolverMgCreate"));
+        api.destroy = reinterpret_cast<decltype(api.destroy)>(sym("cusolverMgDestroy"));
+        api.device_select = reinterpret_cast<decltype(api.device_select)>(sym("cusolverMgDeviceSelect"));
+        api.create_grid = reinterpret_cast<decltype(api.create_grid)>(sym("cusolverMgCreateDeviceGrid"));
+        api.destroy_grid = reinterpret_cast<decltype(api.destroy_grid)>(sym("cusolverMgDestroyGrid"));
+        api.create_desc = reinterpret_cast<decltype(api.create_desc)>(sym("cusolverMgCreateMatrixDesc"));
+        api.destroy_desc = reinterpret_cast<decltype(api.destroy_desc)>(sym("cusolverMgDestroyMatrixDesc"));
+        api.syevd_buffer_size =
+            reinterpret_cast<decltype(api.syevd_buffer_size)>(sym("cusolverMgSyevd_bufferSize"));
+        api.syevd = reinterpret_cast<decltype(api.syevd)>(sym("cusolverMgSyevd"));
+        ok = api.create && api.destroy && api.device_select && api.create_grid && api.destroy_grid &&
+             api.create_desc && api.destroy_desc && api.syevd_buffer_size && api.syevd;
+    });
+    return ok ? &api : nullptr;
+}
+
+struct MgSolver {
+    const MgApi* api = mg_api();
+    cusolverMgHandle_t h = nullptr;
+    cudaLibMgGrid_t grid = nullptr;
+    cudaLibMgMatrixDesc_t desc = nullptr;
+    ~MgSolver() {
+        if (desc) api->destroy_desc(desc);
+        if (grid) api->destroy_grid(grid);
+        if (h) api->destroy(h);
+    }
+    cusolverStatus_t init(int64_t n) {
+        if (!api) return CUSOLVER_STATUS_NOT_INITIALIZED;  // libcusolverMg not found
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess) return CUSOLVER_STATUS_INTERNAL_ERROR;
+        cusolverStatus_t s = api->create(&h);
+        if (s != CUSOLVER_STATUS_SUCCESS) return s;
+        int ids[1] = {dev};
+        s = api->device_select(h, 1, ids);
+        if (s != CUSOLVER_STATUS_SUCCESS) return s;
+        int32_t gids[1] = {dev};
+        s = api->create_grid(&grid, 1, 1, gids, CUDALIBMG_GRID_MAPPING_COL_MAJOR);
+        if (s != CUSOLVER_STATUS_SUCCESS) return s;
+        return api->create_desc(&desc, n, n, n, kMgColBlock, CUDA_R_64F, grid);
+    }
+    // workspace in doubles; A may be null for the query, W is a host array of n doubles
+    cusolverStatus_t query(int64_t n, double* A, double* w_host, int64_t* lwork) {
+        void* arr[1] = {A};
+        return api->syevd_buffer_size(h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)n,
+                                      arr, 1, 1, desc, w_host, CUDA_R_64F, CUDA_R_64F, lwork);
+    }
+};
+
+// true when cusolverDnXsyevd takes n; dev_bytes: its device workspace
+bool dn_syevd_fits(int64_t n, size_t* dev_bytes) {
     cusolverDnHandle_t h = cusolver_handle();
-    if (!h || n <= 0) return -1;
     cusolverDnParams_t params;
-    if (cusolverDnCreateParams(&params) != CUSOLVER_STATUS_SUCCESS) return -1;
-    size_t dev_bytes = 0, host_bytes = 0;
-    cusolverStatus_t s = cusolverDnXsyevd_bufferSize(
+    if (!h || cusolverDnCreateParams(&params) != CUSOLVER_STATUS_SUCCESS) return false;
+    size_t host_bytes = 0;
+    const cusolverStatus_t s = cusolverDnXsyevd_bufferSize(
         h, params, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, n, CUDA_R_64F, nullptr, n,
-        CUDA_R_64F, nullptr, CUDA_R_64F, &dev_bytes, &host_bytes);
+        CUDA_R_64F, nullptr, CUDA_R_64F, dev_bytes, &host_bytes);
     cusolverDnDestroyParams(params);
-    if (s != CUSOLVER_STATUS_SUCCESS) return -1;
-    return (int64_t)(((dev_bytes + 255) / 256) * 256) + 256;  // + device info word
+    return s == CUSOLVER_STATUS_SUCCESS;
+}
+}  // namespace
+
+int64_t jb_eigh_workspace_size(int64_t n) {
+    if (n <= 0) return -1;
+    size_t dev_bytes = 0;
+    if (dn_syevd_fits(n, &dev_bytes))
+        return (int64_t)(((dev_bytes + 255) / 256) * 256) + 256;  // + device info word
+    if (n > 2147483647ll) return -1;
+    MgSolver mg;
+    std::vector<double> w_host((size_t)n);
+    int64_t lwork = 0;
+    cusolverStatus_t s = mg.init(n);
+    if (s == CUSOLVER_STATUS_SUCCESS) s = mg.query(n, nullptr, w_host.data(), &lwork);
+    if (s != CUSOLVER_STATUS_SUCCESS) {
+        set_error("eigendecomposition workspace query failed for n = %lld (cusolverMg status %d%s)",
+                  (long long)n, (int)s, mg_api() ? "" : "; libcusolverMg.so.11 not found");
+        return -1;
+    }
+    return ((lwork * 8 + 255) / 256) * 256;
+}
+
+// Large-n path of jb_eigh_f64 (lda == n): blocking cusolverMgSyevd on this device.
+static int32_t eigh_f64_mg(double* A, int64_t n, double* w, double threshold, void* workspace,
+                           int64_t workspace_bytes, cudaStream_t st) {
+    MgSolver mg;
+    double* w_host = nullptr;  // pinned: valid for the solver as a host or a device address
+    JB_CUDA(cudaMallocHost(&w_host, (size_t)n * sizeof(double)));
+    int64_t lwork = 0;
+    cusolverStatus_t s = mg.init(n);
+    if (s == CUSOLVER_STATUS_SUCCESS) s = mg.query(n, A, w_host, &lwork);
+    if (s != CUSOLVER_STATUS_SUCCESS) {
+        cudaFreeHost(w_host);
+        return cusolver_status(s, "cusolverMgSyevd_bufferSize");
+    }
+    if (workspace_bytes < lwork * 8) {
+        cudaFreeHost(w_host);
+        set_error("jb_eigh_f64: workspace %lld < required %lld", (long long)workspace_bytes,
+                  (long long)(lwork * 8));
+        return JB_E_INVALID;
+    }
+    cudaError_t e = cudaStreamSynchronize(st);  // the solver runs on its own streams
+    int info = 0;
+    if (e == cudaSuccess) {
+        void* arr_a[1] = {A};
+        void* arr_w[1] = {workspace};
+        s = mg.api->syevd(mg.h, CUSOLVER_EIG_MODE_VECTOR, CUBLAS_FILL_MODE_LOWER, (int)n, arr_a, 1,
+                          1, mg.desc, w_host, CUDA_R_64F, CUDA_R_64F, arr_w, lwork, &info);
+        e = cudaDeviceSynchronize();
+    }
+    if (e == cudaSuccess && s == CUSOLVER_STATUS_SUCCESS && info == 0)
+        e = cudaMemcpyAsync(w, w_host, (size_t)n * sizeof(double), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && s == CUSOLVER_STATUS_SUCCESS && info == 0) e = cudaStreamSynchronize(st);
+    cudaFreeHost(w_host);
+    if (e != cudaSuccess) return cuda_status(e, "cusolverMg eigendecomposition");
+    if (s != CUSOLVER_STATUS_SUCCESS) return cusolver_status(s, "cusolverMgSyevd");
+    if (info != 0) {
+        set_error("cusolverMgSyevd: info = %d (no convergence or bad argument)", info);
+        return JB_E_NUMERIC;
+    }
+    threshold_kernel<<<64, 256, 0, st>>>(w, n, threshold);
+    JB_LAUNCH_CHECK("threshold_kernel");
+    return JB_OK;
 }
 
 int32_t jb_eigh_f64(double* A, int64_t n, int64_t lda, double* w, double threshold,
                     void* workspace, int64_t workspace_bytes, uintptr_t stream) {
     JB_CHECK_ARG(n > 0 && lda >= n && A && w, "jb_eigh_f64: bad arguments");
+    {
+        size_t dn_bytes = 0;
+        if (!dn_syevd_fits(n, &dn_bytes)) {
+            JB_CHECK_ARG(lda == n && n <= 2147483647ll, "jb_eigh_f64: n = %lld needs lda == n",
+                         (long long)n);
+            return eigh_f64_mg(A, n, w, threshold, workspace, workspace_bytes, as_stream(stream));
+        }
+    }
     cusolverDnHandle_t h = cusolver_handle();
     if (!h) {
         set_error("cuSOLVER handle creation failed");

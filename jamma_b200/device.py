@@ -62,5 +62,7 @@ def empty(shape, dtype=torch.float64) -> torch.Tensor:
 def workspace(nbytes: int) -> torch.Tensor:
     """Byte buffer for a library workspace (256-byte aligned by the caching allocator)."""
     if nbytes < 0:
-        raise RuntimeError("workspace size query failed")
+        from jamma_b200 import _native
+
+        raise RuntimeError(f"workspace size query failed: {_native.last_error()}")
     return torch.empty(max(int(nbytes), 1), dtype=torch.uint8, device="cuda")
