@@ -542,6 +542,13 @@ def run_ours(args) -> None:
 
     serving = None
     if rank == 0 and not args.no_serving:
+        # start the server from a clean allocator: the earlier legs' freed buffers go back
+        # to the device instead of fragmenting the jobs' allocations
+        import gc
+
+        gc.collect()
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
         serving = run_serving(args)
 
     if rank == 0:
