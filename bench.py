@@ -528,11 +528,15 @@ def run_ours(args) -> None:
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ps = max(1, min(args.steps, 3))
+        if args.profile_phase == "multi":  # the multi-phenotype steps are the profiler range
+            torch.cuda.profiler.start()
         a.record(st)
         for s in range(args.warmup, args.warmup + ps):
             pstep(s)
         b.record(st)
         torch.cuda.synchronize()
+        if args.profile_phase == "multi":
+            torch.cuda.profiler.stop()
         pms = a.elapsed_time(b) / ps
         multi = {"phenotypes": phi, "lmm_mode": args.pheno_mode, "snps_per_step": mp,
                  "ms_per_step": pms, "snp_phenotype_pairs_per_s": mp * phi / (pms / 1e3),
@@ -773,7 +777,7 @@ def main():
     ap.add_argument("--pheno-chunk", type=int, default=2048)
     ap.add_argument("--pheno-mode", type=int, default=4)
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--profile-phase", choices=["assoc", "kinship"], default="assoc",
+    ap.add_argument("--profile-phase", choices=["assoc", "kinship", "multi"], default="assoc",
                     help="which phase torch.cuda.profiler.start/stop brackets")
     ap.add_argument("--rot-kernel", type=int, choices=[0, 1], default=None,
                     help="fix the INT8 rotation kernel (0 one CTA per tile, 1 CTA pairs)")

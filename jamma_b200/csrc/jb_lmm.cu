@@ -216,13 +216,13 @@ __device__ __forceinline__ PabOut<C> pab_reduce(const double (&row0)[Lay<C>::NI]
 
 // REML log-likelihood (_reml_with_precomputed_iab, likelihood_jax.py:280-339).
 template <int C>
-__device__ __forceinline__ double reml_logl(const PabOut<C>& pb, const double (&iab_diag)[C + 1],
+__device__ __forceinline__ double reml_logl(const PabOut<C>& pb, const double (&log_iab)[C + 1],
                                             double logdet_h, const Params& p) {
     double ldw = 0.0;
 #pragma unroll
     for (int i = 0; i <= C; ++i) {
         ldw = __dadd_rn(ldw, pb.diag[i] > 0 ? log(pb.diag[i]) : 0.0);
-        ldw = __dsub_rn(ldw, iab_diag[i] > 0 ? log(iab_diag[i]) : 0.0);
+        ldw = __dsub_rn(ldw, log_iab[i]);
     }
     const double pyy = clamp_pyy(pb.yy1);
     double f = __dsub_rn(p.c_reml, __dmul_rn(0.5, logdet_h));
@@ -320,14 +320,14 @@ __device__ __forceinline__ void eval_full(const Params& p, const double* __restr
 
 template <int C, bool REML>
 __device__ __forceinline__ double eval_logl(const Params& p, const double* x, const double* y,
-                                            double log_lam, const double (&iab_diag)[C + 1],
+                                            double log_lam, const double (&log_iab)[C + 1],
                                             PabOut<C>* keep) {
     double row0[Lay<C>::NI];
     double logdet;
     eval_full<C>(p, x, y, exp(log_lam), row0, logdet);
     const PabOut<C> pb = pab_reduce<C>(row0);
     if (keep) *keep = pb;
-    return REML ? reml_logl<C>(pb, iab_diag, logdet, p) : mle_logl<C>(pb, logdet, p);
+    return REML ? reml_logl<C>(pb, log_iab, logdet, p) : mle_logl<C>(pb, logdet, p);
 }
 
 // Chebyshev series sum_j c_j T_j(t) by Clenshaw's recurrence.
@@ -498,7 +498,7 @@ __device__ __forceinline__ void coop_shared(const BracketCoef<C>& b, double s, d
 template <int C, bool REML>
 __device__ __forceinline__ double coop_logl(const Params& p, const GlobalCoef<C>& g,
                                             const BracketCoef<C>& b, double s,
-                                            const double (&iab_diag)[C + 1]) {
+                                            const double (&log_iab)[C + 1]) {
     using L = Lay<C>;
     double xs[L::NX], shared[L::NS], logdet;
     coop_xsums<C>(p, g, s, xs);
@@ -506,7 +506,7 @@ __device__ __forceinline__ double coop_logl(const Params& p, const GlobalCoef<C>
     double row0[L::NI];
     assemble<C>(row0, shared, xs);
     const PabOut<C> pb = pab_reduce<C>(row0);
-    return REML ? reml_logl<C>(pb, iab_diag, logdet, p) : mle_logl<C>(pb, logdet, p);
+    return REML ? reml_logl<C>(pb, log_iab, logdet, p) : mle_logl<C>(pb, logdet, p);
 }
 
 // Golden-section refinement (_golden_section_refine, likelihood_jax.py:419-488) on the
@@ -514,11 +514,11 @@ __device__ __forceinline__ double coop_logl(const Params& p, const GlobalCoef<C>
 // expansions for the final evaluation.
 template <int C, bool REML>
 __device__ double golden_coop(const Params& p, const GlobalCoef<C>& g, int best, int f,
-                              const double (&iab_diag)[C + 1], BracketCoef<C>& bc) {
+                              const double (&log_iab)[C + 1], BracketCoef<C>& bc) {
     const int lo = best - 1 > 0 ? best - 1 : 0;
     const int hi = best + 1 < p.n_grid - 1 ? best + 1 : p.n_grid - 1;
     bc = load_bracket_coef<C>(p, best, f);
-    auto probe = [&](double s) { return coop_logl<C, REML>(p, g, bc, s, iab_diag); };
+    auto probe = [&](double s) { return coop_logl<C, REML>(p, g, bc, s, log_iab); };
     double a = p.loglam[lo], b = p.loglam[hi];
     double c = __dsub_rn(b, __dmul_rn(kPhi, __dsub_rn(b, a)));
     double d = __dadd_rn(a, __dmul_rn(kPhi, __dsub_rn(b, a)));
@@ -597,24 +597,24 @@ __device__ __forceinline__ void direct_xsums2(const Params& p, const double* __r
 template <int C, bool REML>
 __device__ __forceinline__ double final_logl(const Params& p, const double (&xs)[Lay<C>::NX],
                                              const BracketCoef<C>& bc, double s,
-                                             const double (&iab_diag)[C + 1], PabOut<C>& pb) {
+                                             const double (&log_iab)[C + 1], PabOut<C>& pb) {
     using L = Lay<C>;
     double shared[L::NS], logdet;
     coop_shared<C>(bc, s, logdet, shared);
     double row0[L::NI];
     assemble<C>(row0, shared, xs);
     pb = pab_reduce<C>(row0);
-    return REML ? reml_logl<C>(pb, iab_diag, logdet, p) : mle_logl<C>(pb, logdet, p);
+    return REML ? reml_logl<C>(pb, log_iab, logdet, p) : mle_logl<C>(pb, logdet, p);
 }
 
 // Grid bracket + golden section (_golden_section_refine, likelihood_jax.py:419-488).
 template <int C, bool REML>
 __device__ void golden(const Params& p, const double* x, const double* y, int best,
-                       const double (&iab_diag)[C + 1], double& lam_out, double& logl_out,
+                       const double (&log_iab)[C + 1], double& lam_out, double& logl_out,
                        PabOut<C>& pb_out) {
     const int lo = best - 1 > 0 ? best - 1 : 0;
     const int hi = best + 1 < p.n_grid - 1 ? best + 1 : p.n_grid - 1;
-    auto probe = [&](double s) { return eval_logl<C, REML>(p, x, y, s, iab_diag, nullptr); };
+    auto probe = [&](double s) { return eval_logl<C, REML>(p, x, y, s, log_iab, nullptr); };
     double a = p.loglam[lo], b = p.loglam[hi];
     double c = __dsub_rn(b, __dmul_rn(kPhi, __dsub_rn(b, a)));
     double d = __dadd_rn(a, __dmul_rn(kPhi, __dsub_rn(b, a)));
@@ -633,7 +633,7 @@ __device__ void golden(const Params& p, const double* x, const double* y, int be
     }
     const double log_opt = __dmul_rn(__dadd_rn(a, b), 0.5);
     lam_out = exp(log_opt);
-    logl_out = eval_logl<C, REML>(p, x, y, log_opt, iab_diag, &pb_out);
+    logl_out = eval_logl<C, REML>(p, x, y, log_opt, log_iab, &pb_out);
 }
 
 // jnp.argmax semantics: first maximum, NaN wins (first NaN).
@@ -720,16 +720,16 @@ __global__ void __launch_bounds__(kPairsThreads, PairsOccupancy<C>::kMinBlocks)
     if (INTERP) gc = load_global_coef<C>(p, j, f);
 
     // ---------------- phase 1: H = 1 (Iab) and H = H0 (score)
-    double iab_diag[C + 1];
+    double log_iab[C + 1];
 #pragma unroll
-    for (int i = 0; i <= C; ++i) iab_diag[i] = 0.0;
+    for (int i = 0; i <= C; ++i) log_iab[i] = 0.0;
     if (need_reml) {
         double xs[L::NX], row0[L::NI];
         row_xsums(INTERP ? 0 : p.n_grid, xs);
         assemble<C>(row0, p.S + (int64_t)p.n_grid * srow + (int64_t)f * L::NS, xs);
         const PabOut<C> pb = pab_reduce<C>(row0);
 #pragma unroll
-        for (int i = 0; i <= C; ++i) iab_diag[i] = pb.diag[i];
+        for (int i = 0; i <= C; ++i) log_iab[i] = pb.diag[i] > 0 ? log(pb.diag[i]) : 0.0;
     }
     if (need_score) {
         double xs[L::NX], row0[L::NI];
@@ -766,7 +766,7 @@ __global__ void __launch_bounds__(kPairsThreads, PairsOccupancy<C>::kMinBlocks)
         assemble<C>(row0, p.S + (int64_t)g * srow + (int64_t)f * L::NS, xs);
         const PabOut<C> pb = pab_reduce<C>(row0);
         const double ldh = p.logdet[g];
-        if (need_reml) best_reml.push(g, reml_logl<C>(pb, iab_diag, ldh, p));
+        if (need_reml) best_reml.push(g, reml_logl<C>(pb, log_iab, ldh, p));
         if (need_mle) best_mle.push(g, mle_logl<C>(pb, ldh, p));
     }
     if (INTERP) {
@@ -781,8 +781,8 @@ __global__ void __launch_bounds__(kPairsThreads, PairsOccupancy<C>::kMinBlocks)
         // both searches first, then one direct pass over x for the two final evaluations
         BracketCoef<C> bm, br;
         double s_m = 0.0, s_r = 0.0;
-        if (need_mle) s_m = golden_coop<C, false>(p, gc, best_mle.idx, f, iab_diag, bm);
-        if (need_reml) s_r = golden_coop<C, true>(p, gc, best_reml.idx, f, iab_diag, br);
+        if (need_mle) s_m = golden_coop<C, false>(p, gc, best_mle.idx, f, log_iab, bm);
+        if (need_reml) s_r = golden_coop<C, true>(p, gc, best_reml.idx, f, log_iab, br);
         lam_m = exp(s_m);
         lam_r = exp(s_r);
         double xm[L::NX], xr[L::NX];
@@ -795,15 +795,15 @@ __global__ void __launch_bounds__(kPairsThreads, PairsOccupancy<C>::kMinBlocks)
         }
         if (need_mle) {
             PabOut<C> pb;
-            logl_m = final_logl<C, false>(p, xm, bm, s_m, iab_diag, pb);
+            logl_m = final_logl<C, false>(p, xm, bm, s_m, log_iab, pb);
         }
-        if (need_reml) logl_r = final_logl<C, true>(p, xr, br, s_r, iab_diag, pb_r);
+        if (need_reml) logl_r = final_logl<C, true>(p, xr, br, s_r, log_iab, pb_r);
     } else {
         if (need_mle) {
             PabOut<C> pb;
-            golden<C, false>(p, x, y, best_mle.idx, iab_diag, lam_m, logl_m, pb);
+            golden<C, false>(p, x, y, best_mle.idx, log_iab, lam_m, logl_m, pb);
         }
-        if (need_reml) golden<C, true>(p, x, y, best_reml.idx, iab_diag, lam_r, logl_r, pb_r);
+        if (need_reml) golden<C, true>(p, x, y, best_reml.idx, log_iab, lam_r, logl_r, pb_r);
     }
     if (need_mle && lane == 0) {
         if (p.out.lambda_mle) p.out.lambda_mle[o] = lam_m;
