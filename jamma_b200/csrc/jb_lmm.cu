@@ -686,7 +686,7 @@ __device__ __forceinline__ void beta_se(const PabOut<C>& pb, double px_yy, doubl
 constexpr int kPairsThreads = 128;
 template <int C>
 struct PairsOccupancy {
-    static constexpr int kMinBlocks = C == 1 ? 5 : (C == 2 ? 3 : 2);
+    static constexpr int kMinBlocks = C == 1 ? 4 : (C == 2 ? 3 : 2);  // C = 1: 125 registers, no spill
 };
 
 template <int C, bool INTERP>
