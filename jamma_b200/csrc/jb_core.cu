@@ -81,7 +81,36 @@ __global__ void decode_bed_kernel(const uint8_t* __restrict__ packed, int64_t bp
     int obs = 0, sum = 0, het = 0, hom2 = 0;
     // count-A1: 00 -> 2, 01 -> missing (3), 10 -> 1, 11 -> 0
     auto code_of = [](int c) { return c == 0 ? 2 : (c == 1 ? 3 : (c == 2 ? 1 : 0)); };
-    if (!sidx && (ld & 3) == 0) {
+    if (!sidx && (ld & 15) == 0 && (bps & 3) == 0 &&
+        (reinterpret_cast<uintptr_t>(packed) & 3) == 0 && (reinterpret_cast<uintptr_t>(codes) & 15) == 0) {
+        // 16 samples per thread: one 32-bit record word (sample e at bits 2e, 2e+1 = l, h)
+        // to 16 code bytes.  count-A1 code = (~h, l ^ h) per field; the per-SNP counts come
+        // from popcounts of the code bit-planes.  bps % 4 == 0 keeps every word in the record.
+        for (int64_t q = threadIdx.x; q < ld / 16; q += blockDim.x) {
+            const int64_t s0 = 16 * q;
+            uint4 o = make_uint4(0u, 0u, 0u, 0u);
+            if (s0 < n) {
+                const uint32_t w = __ldg(reinterpret_cast<const uint32_t*>(rec) + q);
+                const int64_t nv = n - s0 < 16 ? n - s0 : 16;
+                const uint32_t vm = (nv >= 16 ? 0xffffffffu : ((1u << (2 * nv)) - 1u)) & 0x55555555u;
+                const uint32_t h = (w >> 1) & 0x55555555u, l = w & 0x55555555u;
+                const uint32_t c0 = (l ^ h) & vm, c1 = ~h & vm;
+                const uint32_t vo = vm & ~(l & ~h);  // observed (not code 3)
+                obs += __popc(vo);
+                sum += 2 * __popc(c1 & vo) + __popc(c0 & vo);
+                het += __popc(~c1 & c0 & vo);
+                hom2 += __popc(c1 & ~c0 & vo);
+                const uint32_t code = c0 | (c1 << 1);
+                auto spread4 = [](uint32_t x) {  // four 2-bit fields -> four bytes
+                    x &= 0xffu;
+                    x = (x | (x << 12)) & 0x000f000fu;
+                    return (x | (x << 6)) & 0x03030303u;
+                };
+                o = make_uint4(spread4(code), spread4(code >> 8), spread4(code >> 16), spread4(code >> 24));
+            }
+            *reinterpret_cast<uint4*>(out + s0) = o;
+        }
+    } else if (!sidx && (ld & 3) == 0) {
         for (int64_t q = threadIdx.x; q < ld / 4; q += blockDim.x) {
             const int64_t s0 = 4 * q;
             uint32_t word = 0;
