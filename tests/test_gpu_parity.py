@@ -97,6 +97,26 @@ def test_decode_bed_matches_oracle():
     np.testing.assert_array_equal(counts[:, 3], (gs == 2).sum(0))
 
 
+# all samples, no subset: 16 samples per thread from one record word (n = 29 with a partial
+# last word, n = 208), 4 samples per thread (ld a multiple of 4), one sample per thread
+@pytest.mark.parametrize("n,ld", [(29, 32), (208, 208), (203, 204), (201, 201)])
+def test_decode_bed_all_samples_matches_oracle(n, ld):
+    from jamma_b200.engine import decode_packed
+
+    g = synth.genotypes(n, 131, 0.05, seed=n)
+    packed = OP.encode_genotypes(g)
+    codes, counts = decode_packed(torch.from_numpy(packed).cuda(), n, None, n, ld=ld)
+    codes = codes.cpu().numpy()
+    counts = counts.cpu().numpy()
+    exp = np.where(np.isnan(g), 3, np.nan_to_num(g)).T.astype(np.int8)
+    np.testing.assert_array_equal(codes[:, :n], exp)
+    assert np.all(codes[:, n:] == 0)
+    np.testing.assert_array_equal(counts[:, 0], (~np.isnan(g)).sum(0))
+    np.testing.assert_array_equal(counts[:, 1], np.nansum(g, 0))
+    np.testing.assert_array_equal(counts[:, 2], (g == 1).sum(0))
+    np.testing.assert_array_equal(counts[:, 3], (g == 2).sum(0))
+
+
 # ------------------------------------------------------------------ kinship
 def test_kinship_gemma_fixture(gemma, gemma_geno):
     from jamma_b200 import compute_centered_kinship
