@@ -185,6 +185,20 @@ def _int8_gemm_peak(size: int = 8192, reps: int = 10) -> float:
     return 2.0 * size ** 3 / (best / 1e3) / 1e12
 
 
+def _kinship_phases(ev, n: int, p: int, i8_peak: float) -> dict | None:
+    """Device time of the INT8 kinship's two phases: the per-chunk layout + correction
+    kernels, and the Gram + finalisation (one tcgen05 GEMM of n(n+1)p int8 ops)."""
+    if ev is None:
+        return None
+    chunks_ms, gram_ms = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
+    tops = n * (n + 1.0) * p / (gram_ms / 1e3) / 1e12
+    return {"chunks_ms": chunks_ms, "gram_and_finalize_ms": gram_ms,
+            "gram_tops": tops, "gram_frac_of_int8_peak": tops / i8_peak,
+            "note": "chunks: transpose into the Gram operand, bitmasks, dosage words, the "
+                    "missing-call walk and the correction vectors for every chunk; "
+                    "gram_tops counts n(n+1)p int8 ops against the whole second phase"}
+
+
 def _accuracy(got: dict, ref: dict) -> dict:
     """Errors of one form's statistics against another's on the same SNPs: max / median
     relative error per field; for p-values also the fraction within 1e-6 relative, the
@@ -305,8 +319,12 @@ def run_ours(args) -> None:
     poly = snp_stats_from_counts(kin_counts, n)[2]
     keep = np.where(poly)[0]
 
+    kin_events = {}
+
     def kinship(form: str):
         acc = _KinshipI8(n, keep.size) if form == "int8" else _KinshipAccumulator(n, 4096)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record(st)
         for s in range(0, keep.size, kc):
             sub = keep[s:s + kc]
             rec_k = kin_rec.index_select(0, torch.from_numpy(sub).cuda())
@@ -318,7 +336,11 @@ def run_ours(args) -> None:
                 acc.add_sum_mu2(cc[:, 1] / np.maximum(cc[:, 0], 1))
             else:
                 acc.add(codes_k, mu)
-        return acc.finish()
+        ev[1].record(st)
+        K_out = acc.finish()
+        ev[2].record(st)
+        kin_events[form] = ev
+        return K_out
 
     # one small INT8 kinship first, so the timed one excludes one-time costs (kernel
     # module loads, allocator growth); it covers the first chunk's SNPs only
@@ -586,6 +608,7 @@ def run_ours(args) -> None:
             "fp64_form": {"value": value64, "unit": "SNPs/s", "steps": fp64_steps,
                           "kernel_ms_per_step": kern64, "speedup_mixed_vs_fp64": value / value64},
             "kinship_s": kinship_s, "kinship_form": "int8 tcgen05 Gram + FP64 corrections",
+            "kinship_phases": _kinship_phases(kin_events.get("int8"), n, int(keep.size), i8_measured),
             "kinship_fp64_s": kinship_fp64_s, "kinship_snps": int(keep.size),
             "kinship_int8_vs_fp64_max_rel_diff": kin_maxdiff, "eigh_s": eigh_s,
             "roofline": {"kernel": "i8_gemm_kernel<rotate> (tcgen05 kind::i8, 4 digit planes)",
