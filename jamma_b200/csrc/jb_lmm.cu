@@ -636,6 +636,259 @@ __device__ void golden(const Params& p, const double* x, const double* y, int be
     logl_out = eval_logl<C, REML>(p, x, y, log_opt, log_iab, &pb_out);
 }
 
+// ---------------------------------------------------------------- two pairs per warp
+// The mixed-form search with one (SNP, phenotype) pair per half-warp and exactly the values
+// of the one-pair-per-warp form above: lane l (< 16) of a half stands in for that form's
+// lanes l ("v0") and l + 16 ("v1").  It holds both lanes' Chebyshev values, coefficients
+// and partial sums, built by the same formulas from the same inputs, and folds them with
+// the first (offset-16) step of the warp butterfly; the other four steps run across the
+// half.  Every value and the order of every sum match, so results are bit-identical, while
+// the per-probe scalar work (Pab recursion, logs, golden-section bookkeeping) that every
+// lane repeats now serves two pairs per instruction.
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ double fold_sum(double p0, double p1) {
+    double v = __dadd_rn(p0, p1);  // offset 16: v_l + v_{l^16} (never contracted into an FMA)
+#pragma unroll
+    for (int o = 8; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+    return v;
+}
+
+// lane_cheb's T_l and T_{l+16} (32-lane doubling rounds) and T_32.
+__device__ __forceinline__ void lane_cheb_v(double x, double& t0, double& t1, double& t32) {
+    const int lane = threadIdx.x & 15;
+    double tl = lane == 0 ? 1.0 : x;
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {  // a = 1, 2, 4, 8 (lanes above 16 are idle in these rounds)
+        const int a = 1 << r;
+        const bool act = lane > a && lane <= 2 * a;
+        const double ta = __shfl_sync(kFull, tl, a, 16);
+        const double tb = __shfl_sync(kFull, tl, act ? lane - a : 0, 16);
+        const double tc = __shfl_sync(kFull, tl, act ? 2 * a - lane : 0, 16);
+        if (act) tl = fma(2.0 * ta, tb, -tc);
+    }
+    const double t8 = __shfl_sync(kFull, tl, 8, 16);
+    const double t16 = fma(2.0 * t8, t8, -1.0);  // lane 16 at a = 8: 2 T_8 T_8 - T_0
+    const double tmir = __shfl_sync(kFull, tl, (16 - lane) & 15, 16);  // T_{16-l}
+    t0 = tl;
+    t1 = lane == 0 ? t16 : fma(2.0 * t16, tl, -tmir);  // lanes 17..31 at a = 16
+    t32 = fma(2.0 * t16, t16, -1.0);
+}
+
+struct LaneTV {
+    double t0[kCoefPerLane], t1[kCoefPerLane];
+};
+__device__ __forceinline__ LaneTV lane_cheb_global_v(double x) {
+    const int lane = threadIdx.x & 15;
+    double t0, t1, t32;
+    lane_cheb_v(x, t0, t1, t32);
+    const double a = __shfl_sync(kFull, t0, (16 - lane) & 15, 16);  // T_{16-l}
+    const double b = __shfl_sync(kFull, t1, (16 - lane) & 15, 16);  // T_{32-l}
+    LaneTV r;
+    r.t0[0] = t0;
+    r.t1[0] = t1;
+    r.t0[1] = fma(2.0 * t32, t0, -(lane == 0 ? t32 : b));  // T_{l+32}
+    r.t1[1] = fma(2.0 * t32, t1, -(lane == 0 ? t1 : a));   // T_{l+48}
+#pragma unroll
+    for (int i = 2; i < kCoefPerLane; ++i) {
+        r.t0[i] = fma(2.0 * t32, r.t0[i - 1], -r.t0[i - 2]);
+        r.t1[i] = fma(2.0 * t32, r.t1[i - 1], -r.t1[i - 2]);
+    }
+    return r;
+}
+
+template <int C>
+struct GlobalCoefV {
+    GlobalCoef<C> v0, v1;
+};
+template <int C>
+__device__ __forceinline__ GlobalCoefV<C> load_global_coef_v(const Params& p, int64_t j, int f) {
+    const int lane = threadIdx.x & 15;
+    const int64_t cp = C + p.phi;
+    GlobalCoefV<C> g;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        GlobalCoef<C>& gg = h ? g.v1 : g.v0;
+#pragma unroll
+        for (int i = 0; i < kCoefPerLane; ++i) {
+            const int64_t r = 1 + lane + 16 * h + 32 * i;
+            const double* rl = p.CL + j * p.ldcl + r * cp;
+#pragma unroll
+            for (int a = 0; a < C; ++a) gg.c[a][i] = __ldg(rl + a);
+            gg.c[C][i] = __ldg(p.CQ + j * p.ldcq + r);
+            gg.c[C + 1][i] = __ldg(rl + C + f);
+        }
+    }
+    return g;
+}
+
+template <int C>
+__device__ __forceinline__ void coop_xsums_v(const Params& p, const GlobalCoefV<C>& g, double s,
+                                             double (&xs)[Lay<C>::NX]) {
+    const LaneTV T = lane_cheb_global_v((s - p.gmid) * p.ginv);
+#pragma unroll
+    for (int q = 0; q < Lay<C>::NX; ++q) {
+        double v0 = g.v0.c[q][0] * T.t0[0], v1 = g.v1.c[q][0] * T.t1[0];
+#pragma unroll
+        for (int i = 1; i < kCoefPerLane; ++i) {
+            v0 = fma(g.v0.c[q][i], T.t0[i], v0);
+            v1 = fma(g.v1.c[q][i], T.t1[i], v1);
+        }
+        xs[q] = fold_sum(v0, v1);
+    }
+}
+
+template <int C>
+struct BracketCoefV {
+    BracketCoef<C> v0, v1;
+};
+template <int C>
+__device__ __forceinline__ BracketCoefV<C> load_bracket_coef_v(const Params& p, int best, int f) {
+    using L = Lay<C>;
+    const int lane = threadIdx.x & 15;
+    const int nf = 1 + p.phi * L::NS;
+    const double* cb = p.cheb + (int64_t)best * nf * kChebN;
+    BracketCoefV<C> b;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        BracketCoef<C>& bb = h ? b.v1 : b.v0;
+        const int jj = lane + 16 * h;
+        bb.c[0] = jj < kChebN ? __ldg(cb + jj) : 0.0;
+#pragma unroll
+        for (int k = 0; k < L::NS; ++k)
+            bb.c[1 + k] = jj < kChebN ? __ldg(cb + (1 + f * L::NS + k) * kChebN + jj) : 0.0;
+        bb.mid = p.cheb_mid[best];
+        bb.inv_half = 1.0 / p.cheb_half[best];
+    }
+    return b;
+}
+
+template <int C>
+__device__ __forceinline__ void coop_shared_v(const BracketCoefV<C>& b, double s, double& logdet,
+                                              double (&shared)[Lay<C>::NS]) {
+    double t0, t1, t32;
+    lane_cheb_v((s - b.v0.mid) * b.v0.inv_half, t0, t1, t32);
+    logdet = fold_sum(b.v0.c[0] * t0, b.v1.c[0] * t1);
+#pragma unroll
+    for (int k = 0; k < Lay<C>::NS; ++k) shared[k] = fold_sum(b.v0.c[1 + k] * t0, b.v1.c[1 + k] * t1);
+}
+
+template <int C, bool REML>
+__device__ __forceinline__ double coop_logl_v(const Params& p, const GlobalCoefV<C>& g,
+                                              const BracketCoefV<C>& b, double s,
+                                              const double (&log_iab)[C + 1]) {
+    using L = Lay<C>;
+    double xs[L::NX], shared[L::NS], logdet;
+    coop_xsums_v<C>(p, g, s, xs);
+    coop_shared_v<C>(b, s, logdet, shared);
+    double row0[L::NI];
+    assemble<C>(row0, shared, xs);
+    const PabOut<C> pb = pab_reduce<C>(row0);
+    return REML ? reml_logl<C>(pb, log_iab, logdet, p) : mle_logl<C>(pb, logdet, p);
+}
+
+template <int C, bool REML>
+__device__ double golden_coop_v(const Params& p, const GlobalCoefV<C>& g, int best, int f,
+                                const double (&log_iab)[C + 1], BracketCoefV<C>& bc) {
+    const int lo = best - 1 > 0 ? best - 1 : 0;
+    const int hi = best + 1 < p.n_grid - 1 ? best + 1 : p.n_grid - 1;
+    bc = load_bracket_coef_v<C>(p, best, f);
+    auto probe = [&](double s) { return coop_logl_v<C, REML>(p, g, bc, s, log_iab); };
+    double a = p.loglam[lo], b = p.loglam[hi];
+    double c = __dsub_rn(b, __dmul_rn(kPhi, __dsub_rn(b, a)));
+    double d = __dadd_rn(a, __dmul_rn(kPhi, __dsub_rn(b, a)));
+    double fc = probe(c);
+    double fd = probe(d);
+    for (int it = 0; it < p.n_iter; ++it) {
+        const bool keep_left = fc > fd;
+        const double na = keep_left ? a : c;
+        const double nb = keep_left ? d : b;
+        const double nc = __dsub_rn(nb, __dmul_rn(kPhi, __dsub_rn(nb, na)));
+        const double nd = __dadd_rn(na, __dmul_rn(kPhi, __dsub_rn(nb, na)));
+        const double nl = probe(keep_left ? nc : nd);
+        const double nfc = keep_left ? nl : fd;
+        const double nfd = keep_left ? fc : nl;
+        a = na; b = nb; c = nc; d = nd; fc = nfc; fd = nfd;
+    }
+    return __dmul_rn(__dadd_rn(a, b), 0.5);
+}
+
+// direct_xsums2 with lanes l and l + 16 of the 32-lane form in one lane: each virtual lane
+// keeps its own accumulators and visits its samples (l + 32 t, l + 16 + 32 t) in order.
+template <int C>
+__device__ __forceinline__ void direct_xsums2_v(const Params& p, const double* __restrict__ x,
+                                                const double* __restrict__ y, double lam0,
+                                                double lam1, bool two,
+                                                double (&xs0)[Lay<C>::NX],
+                                                double (&xs1)[Lay<C>::NX]) {
+    using L = Lay<C>;
+    double a0[2][L::NX], a1[2][L::NX];
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+#pragma unroll
+        for (int k = 0; k < L::NX; ++k) a0[h][k] = a1[h][k] = 0.0;
+    const int lane = threadIdx.x & 15;
+    auto step = [&](int h, double ev, double xv, double yv, const double* w) {
+        const double t0 = __drcp_rn(__dadd_rn(__dmul_rn(lam0, ev), 1.0)) * xv;
+#pragma unroll
+        for (int a = 0; a < C; ++a) a0[h][a] = fma(t0, w[a], a0[h][a]);
+        a0[h][C] = fma(t0, xv, a0[h][C]);
+        a0[h][C + 1] = fma(t0, yv, a0[h][C + 1]);
+        if (two) {
+            const double t1 = __drcp_rn(__dadd_rn(__dmul_rn(lam1, ev), 1.0)) * xv;
+#pragma unroll
+            for (int a = 0; a < C; ++a) a1[h][a] = fma(t1, w[a], a1[h][a]);
+            a1[h][C] = fma(t1, xv, a1[h][C]);
+            a1[h][C + 1] = fma(t1, yv, a1[h][C + 1]);
+        }
+    };
+    int64_t i = lane;  // virtual lane 0 at i, virtual lane 1 at i + 16
+    for (; i + 32 * (UNR - 1) + 16 < p.n; i += 32 * UNR) {
+        double ev[2 * UNR], xv[2 * UNR], yv[2 * UNR], w[2 * UNR][C > 0 ? C : 1];
+#pragma unroll
+        for (int u = 0; u < 2 * UNR; ++u) {
+            const int64_t ii = i + 32 * (u >> 1) + 16 * (u & 1);
+            ev[u] = __ldg(p.evals + ii);
+            xv[u] = x[ii];
+            yv[u] = __ldg(y + ii);
+#pragma unroll
+            for (int a = 0; a < C; ++a) w[u][a] = __ldg(p.W + a * p.ldw + ii);
+        }
+#pragma unroll
+        for (int u = 0; u < 2 * UNR; ++u) step(u & 1, ev[u], xv[u], yv[u], w[u]);
+    }
+    for (; i < p.n; i += 32) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int64_t ii = i + 16 * h;
+            if (ii < p.n) {
+                double w[C > 0 ? C : 1];
+#pragma unroll
+                for (int a = 0; a < C; ++a) w[a] = __ldg(p.W + a * p.ldw + ii);
+                step(h, __ldg(p.evals + ii), x[ii], __ldg(y + ii), w);
+            }
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < L::NX; ++k) {
+        xs0[k] = fold_sum(a0[0][k], a0[1][k]);
+        xs1[k] = two ? fold_sum(a1[0][k], a1[1][k]) : 0.0;
+    }
+}
+
+template <int C, bool REML>
+__device__ __forceinline__ double final_logl_v(const Params& p, const double (&xs)[Lay<C>::NX],
+                                               const BracketCoefV<C>& bc, double s,
+                                               const double (&log_iab)[C + 1], PabOut<C>& pb) {
+    using L = Lay<C>;
+    double shared[L::NS], logdet;
+    coop_shared_v<C>(bc, s, logdet, shared);
+    double row0[L::NI];
+    assemble<C>(row0, shared, xs);
+    pb = pab_reduce<C>(row0);
+    return REML ? reml_logl<C>(pb, log_iab, logdet, p) : mle_logl<C>(pb, logdet, p);
+}
+
 // jnp.argmax semantics: first maximum, NaN wins (first NaN).
 struct ArgMax {
     int idx = -1;
@@ -658,9 +911,10 @@ struct ArgMax {
         }
         if (x > v || (x == v && i < idx)) { idx = i; v = x; }
     }
-    __device__ void warp_reduce() {
+    template <int GW = 32>
+    __device__ void warp_reduce() {  // over groups of GW lanes
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
+        for (int o = GW / 2; o > 0; o >>= 1) {
             const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
             const double ov = __shfl_xor_sync(0xffffffffu, v, o);
             merge(oi, ov);
@@ -687,15 +941,27 @@ constexpr int kPairsThreads = 128;
 template <int C>
 struct PairsOccupancy {
     static constexpr int kMinBlocks = C == 1 ? 4 : (C == 2 ? 3 : 2);  // C = 1: 125 registers, no spill
+    // two pairs per warp: each lane holds two virtual lanes' state (C = 1: 168 registers;
+    // 3 blocks measured 2% faster than 2 blocks at 180 registers and no spill)
+    static constexpr int kMinBlocksHalf = 3;
 };
 
-template <int C, bool INTERP>
-__global__ void __launch_bounds__(kPairsThreads, PairsOccupancy<C>::kMinBlocks)
+// One (SNP, phenotype) pair per group of GW lanes: a warp (GW = 32), or a half-warp in the
+// mixed form with one covariate column (GW = 16, the bit-identical two-pairs-per-warp
+// helpers above).  Every lane of a warp runs the same control flow: a group past the last
+// pair repeats the last pair and writes nothing.
+template <int C, bool INTERP, int GW>
+__global__ void __launch_bounds__(kPairsThreads, GW == 16 ? PairsOccupancy<C>::kMinBlocksHalf
+                                                            : PairsOccupancy<C>::kMinBlocks)
     lmm_pairs_kernel(const Params p) {
     using L = Lay<C>;
-    const int64_t wid = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (wid >= p.m * p.phi) return;
-    const int lane = threadIdx.x & 31;
+    static_assert(GW == 32 || (INTERP && GW == 16), "half-warp pairs are a mixed-form path");
+    const int64_t npairs = p.m * p.phi;
+    const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if ((tid & ~31ll) / GW >= npairs) return;  // the whole warp is idle
+    const bool valid_pair = tid / GW < npairs;
+    const int64_t wid = valid_pair ? tid / GW : npairs - 1;
+    const int lane = threadIdx.x & (GW - 1);
     const int64_t j = wid / p.phi;
     const int f = (int)(wid % p.phi);
     const double* __restrict__ x = p.G + j * p.ldg;
@@ -717,7 +983,11 @@ __global__ void __launch_bounds__(kPairsThreads, PairsOccupancy<C>::kMinBlocks)
 
     // mixed form: this SNP's global series coefficients, spread over the warp
     GlobalCoef<C> gc;
-    if (INTERP) gc = load_global_coef<C>(p, j, f);
+    GlobalCoefV<C> gcv;
+    if constexpr (INTERP && GW == 16)
+        gcv = load_global_coef_v<C>(p, j, f);
+    else if (INTERP)
+        gc = load_global_coef<C>(p, j, f);
 
     // ---------------- phase 1: H = 1 (Iab) and H = H0 (score)
     double log_iab[C + 1];
@@ -733,7 +1003,9 @@ __global__ void __launch_bounds__(kPairsThreads, PairsOccupancy<C>::kMinBlocks)
     }
     if (need_score) {
         double xs[L::NX], row0[L::NI];
-        if (INTERP)
+        if constexpr (INTERP && GW == 16)
+            coop_xsums_v<C>(p, gcv, log(p.lam0[f]), xs);
+        else if (INTERP)
             coop_xsums<C>(p, gc, log(p.lam0[f]), xs);
         else
             row_xsums(p.n_grid + 1 + f, xs);
@@ -744,7 +1016,7 @@ __global__ void __launch_bounds__(kPairsThreads, PairsOccupancy<C>::kMinBlocks)
         beta_se<C>(pb, clamp_pyy(pb.yy1), p.df, valid, beta, tau, se);
         const double fstat = p.n_d * (pb.xy * pb.xy) / (pb.yy * (valid ? pb.xx : 1.0));
         const double pv = f_pvalue(fstat, p.df, valid);
-        if (lane == 0) {
+        if (lane == 0 && valid_pair) {
             if (p.out.p_score) p.out.p_score[o] = pv;
             if (p.mode == 3) {
                 if (p.out.beta) p.out.beta[o] = beta;
@@ -756,8 +1028,8 @@ __global__ void __launch_bounds__(kPairsThreads, PairsOccupancy<C>::kMinBlocks)
 
     // ---------------- phase 2: shared lambda grid
     ArgMax best_reml, best_mle;
-    // mixed form: lanes take grid points lane, lane+32, ... from the series, then merge
-    for (int g = INTERP ? lane : 0; g < p.n_grid; g += INTERP ? 32 : 1) {
+    // mixed form: lanes take grid points lane, lane+GW, ... from the series, then merge
+    for (int g = INTERP ? lane : 0; g < p.n_grid; g += INTERP ? GW : 1) {
         double xs[L::NX], row0[L::NI];
         if (INTERP)
             series_xsums<C>(p, j, f, p.loglam[g], xs);
@@ -770,14 +1042,34 @@ __global__ void __launch_bounds__(kPairsThreads, PairsOccupancy<C>::kMinBlocks)
         if (need_mle) best_mle.push(g, mle_logl<C>(pb, ldh, p));
     }
     if (INTERP) {
-        best_reml.warp_reduce();
-        best_mle.warp_reduce();
+        best_reml.warp_reduce<GW>();
+        best_mle.warp_reduce<GW>();
     }
 
     // ---------------- phase 3: golden sections + statistics
     double lam_m = 0.0, logl_m = 0.0, lam_r = 0.0, logl_r = 0.0;
     PabOut<C> pb_r;
-    if (INTERP) {
+    if constexpr (INTERP && GW == 16) {
+        BracketCoefV<C> bm, br;
+        double s_m = 0.0, s_r = 0.0;
+        if (need_mle) s_m = golden_coop_v<C, false>(p, gcv, best_mle.idx, f, log_iab, bm);
+        if (need_reml) s_r = golden_coop_v<C, true>(p, gcv, best_reml.idx, f, log_iab, br);
+        lam_m = exp(s_m);
+        lam_r = exp(s_r);
+        double xm[L::NX], xr[L::NX];
+        if (need_mle && need_reml) {
+            direct_xsums2_v<C>(p, x, y, lam_m, lam_r, true, xm, xr);
+        } else if (need_mle) {
+            direct_xsums2_v<C>(p, x, y, lam_m, lam_m, false, xm, xr);
+        } else {
+            direct_xsums2_v<C>(p, x, y, lam_r, lam_r, false, xr, xm);
+        }
+        if (need_mle) {
+            PabOut<C> pb;
+            logl_m = final_logl_v<C, false>(p, xm, bm, s_m, log_iab, pb);
+        }
+        if (need_reml) logl_r = final_logl_v<C, true>(p, xr, br, s_r, log_iab, pb_r);
+    } else if (INTERP) {
         // both searches first, then one direct pass over x for the two final evaluations
         BracketCoef<C> bm, br;
         double s_m = 0.0, s_r = 0.0;
@@ -805,7 +1097,7 @@ __global__ void __launch_bounds__(kPairsThreads, PairsOccupancy<C>::kMinBlocks)
         }
         if (need_reml) golden<C, true>(p, x, y, best_reml.idx, log_iab, lam_r, logl_r, pb_r);
     }
-    if (need_mle && lane == 0) {
+    if (need_mle && lane == 0 && valid_pair) {
         if (p.out.lambda_mle) p.out.lambda_mle[o] = lam_m;
         if (p.out.logl_mle) p.out.logl_mle[o] = logl_m;
         const double stat = jmax(2.0 * (logl_m - p.logl0[f]), 0.0);
@@ -818,7 +1110,7 @@ __global__ void __launch_bounds__(kPairsThreads, PairsOccupancy<C>::kMinBlocks)
         beta_se<C>(pb_r, px_yy, p.df, valid, beta, tau, se);
         const double fstat = (pb_r.yy - px_yy) * tau;
         const double pv = f_pvalue(fstat, p.df, valid);
-        if (lane == 0) {
+        if (lane == 0 && valid_pair) {
             if (p.out.lambda_remle) p.out.lambda_remle[o] = lam_r;
             if (p.out.logl_h1) p.out.logl_h1[o] = logl_r;
             if (p.out.beta) p.out.beta[o] = beta;
@@ -1274,12 +1566,14 @@ __global__ void linspace_kernel(double* out, double start, double stop, int num)
 
 template <int C>
 int32_t launch_pairs(const Params& p, cudaStream_t st) {
-    const int64_t warps = p.m * p.phi;
-    const int64_t blocks = ceil_div(warps * 32, kPairsThreads);
-    if (p.cheb)
-        lmm_pairs_kernel<C, true><<<(unsigned)blocks, kPairsThreads, 0, st>>>(p);
+    const int64_t pairs = p.m * p.phi;
+    if (p.cheb && C == 1)  // two pairs per warp (bit-identical to one per warp)
+        lmm_pairs_kernel<C, true, (C == 1 ? 16 : 32)>
+            <<<(unsigned)ceil_div(pairs * 16, kPairsThreads), kPairsThreads, 0, st>>>(p);
+    else if (p.cheb)
+        lmm_pairs_kernel<C, true, 32><<<(unsigned)ceil_div(pairs * 32, kPairsThreads), kPairsThreads, 0, st>>>(p);
     else
-        lmm_pairs_kernel<C, false><<<(unsigned)blocks, kPairsThreads, 0, st>>>(p);
+        lmm_pairs_kernel<C, false, 32><<<(unsigned)ceil_div(pairs * 32, kPairsThreads), kPairsThreads, 0, st>>>(p);
     JB_LAUNCH_CHECK("lmm_pairs_kernel");
     return JB_OK;
 }
