@@ -61,7 +61,9 @@ class BedFile:
             n_samples, n_snps = meta["n_samples"], meta["n_snps"]
         self.n_samples, self.n_snps = int(n_samples), int(n_snps)
         self.bytes_per_snp = (self.n_samples + 3) // 4
-        raw = np.memmap(self.path, dtype=np.uint8, mode="r")
+        # copy-on-write: the views handed to torch.from_numpy are writable, the file is never
+        # written
+        raw = np.memmap(self.path, dtype=np.uint8, mode="c")
         if raw.size < 3 or bytes(raw[:3]) != BED_MAGIC:
             raise ValueError(f"{self.path}: not a SNP-major PLINK .bed file")
         expect = 3 + self.bytes_per_snp * self.n_snps

@@ -1,0 +1,69 @@
+"""Comparison helpers for the GPU parity tests (device results against the CPU oracle).
+
+Plain FP64 form: lambda 1e-9 relative and other fields 1e-8 relative for at least
+``min_frac`` of SNPs, lambda always within the golden section's final bracket (1e-4),
+every p-value within 1e-6 relative or 1e-12 absolute, identical calls at 0.05 / 1e-3 /
+5e-8.  Mixed form: identical NaN pattern, every |log10 p| error below 1e-4 and identical
+calls (lambda is not compared: a golden-section step on a flat likelihood may resolve
+differently).
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+FIELDS = {"l_remle": "lambda_remle", "logl_H1": "logl_h1", "beta": "beta", "se": "se",
+          "p_wald": "p_wald", "l_mle": "lambda_mle", "p_lrt": "p_lrt", "p_score": "p_score"}
+
+
+def _arrays(results):
+    out = {}
+    for field, key in FIELDS.items():
+        vals = [getattr(r, field) for r in results]
+        if all(v is not None for v in vals):
+            out[key] = np.array(vals, dtype=float)
+    return out
+
+
+def _rel(a, b):
+    with np.errstate(invalid="ignore", divide="ignore"):
+        return np.abs(a - b) / np.maximum(np.abs(b), 1e-300)
+
+
+def _finite_pair(got, ref, k):
+    a, b = np.asarray(got[k], float), np.asarray(ref[k], float)
+    assert a.shape == b.shape, k
+    nan_a, nan_b = np.isnan(a), np.isnan(b)
+    np.testing.assert_array_equal(nan_a, nan_b, err_msg=f"{k}: NaN pattern")
+    return a[~nan_a], b[~nan_b]
+
+
+def assert_assoc_parity(got: dict, ref: dict, keys, min_frac: float = 0.99):
+    for k in keys:
+        a, b = _finite_pair(got, ref, k)
+        if a.size == 0:
+            continue
+        r = _rel(a, b)
+        tight = 1e-9 if k.startswith("lambda") else 1e-8
+        frac = np.mean(r <= tight)
+        assert frac >= min_frac, f"{k}: only {frac:.4f} within {tight}; worst {r.max():.3e}"
+        if k.startswith("lambda"):
+            assert r.max() <= 1e-4, f"{k}: worst {r.max():.3e}"
+        if k.startswith("p_"):
+            ok = (r <= 1e-6) | (np.abs(a - b) <= 1e-12)
+            assert ok.mean() >= 0.999, f"{k}: worst {r.max():.3e}"
+            for t in (0.05, 1e-3, 5e-8):
+                np.testing.assert_array_equal(a < t, b < t, err_msg=f"{k}: calls at {t}")
+
+
+def assert_mixed_parity(got: dict, ref: dict, keys):
+    for k in keys:
+        a, b = _finite_pair(got, ref, k)
+        if a.size == 0 or not k.startswith("p_"):
+            continue
+        with np.errstate(divide="ignore", invalid="ignore"):  # p = 0 on both sides
+            dlog = np.abs(np.log10(a) - np.log10(b))
+        dlog = np.where(a == b, 0.0, dlog)
+        assert dlog.max() < 1e-4, f"{k}: |dlog10 p| {dlog.max():.2e}"
+        for t in (0.05, 1e-3, 5e-8):
+            np.testing.assert_array_equal(a < t, b < t, err_msg=f"{k}: calls at {t}")

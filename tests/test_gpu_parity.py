@@ -25,47 +25,9 @@ from oracle import kinship as OK
 from oracle import lmm as OL
 from oracle import plink as OP
 
+from _parity import _arrays, assert_assoc_parity
+
 pytestmark = pytest.mark.gpu
-
-FIELDS = {"l_remle": "lambda_remle", "logl_H1": "logl_h1", "beta": "beta", "se": "se",
-          "p_wald": "p_wald", "l_mle": "lambda_mle", "p_lrt": "p_lrt", "p_score": "p_score"}
-
-
-def _arrays(results):
-    out = {}
-    for field, key in FIELDS.items():
-        vals = [getattr(r, field) for r in results]
-        if all(v is not None for v in vals):
-            out[key] = np.array(vals, dtype=float)
-    return out
-
-
-def _rel(a, b):
-    with np.errstate(invalid="ignore", divide="ignore"):
-        return np.abs(a - b) / np.maximum(np.abs(b), 1e-300)
-
-
-def assert_assoc_parity(got: dict, ref: dict, keys):
-    for k in keys:
-        a, b = np.asarray(got[k], float), np.asarray(ref[k], float)
-        assert a.shape == b.shape, k
-        nan_a, nan_b = np.isnan(a), np.isnan(b)
-        np.testing.assert_array_equal(nan_a, nan_b, err_msg=f"{k}: NaN pattern")
-        a, b = a[~nan_a], b[~nan_b]
-        if a.size == 0:
-            continue
-        r = _rel(a, b)
-        tight = 1e-9 if k.startswith("lambda") else 1e-8
-        frac = np.mean(r <= tight)
-        assert frac >= 0.99, f"{k}: only {frac:.4f} within {tight}; worst {r.max():.3e}"
-        if k.startswith("lambda"):
-            assert r.max() <= 1e-4, f"{k}: worst {r.max():.3e}"
-        if k.startswith("p_"):
-            ok = (r <= 1e-6) | (np.abs(a - b) <= 1e-12)
-            assert ok.mean() >= 0.999, f"{k}: worst {r.max():.3e}"
-            for t in (0.05, 1e-3, 5e-8):
-                np.testing.assert_array_equal(a < t, b < t, err_msg=f"{k}: calls at {t}")
-
 
 @pytest.fixture(scope="module", autouse=True)
 def _cuda():
