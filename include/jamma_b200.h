@@ -303,8 +303,8 @@ typedef struct jb_lmm_out {
  * log lambda over [1e-5, 1e5] whose coefficients come from the chunk DGEMMs; log|H^-1|
  * and the genotype-free sums come from per-bracket degree-24 expansions of exact FP64
  * node values (both built by jb_lmm_prepare with precision 1); grid points and golden
- * probes read these series, the final evaluation at each optimum reduces the genotype
- * sums directly in FP64.  Needs 1e-5 <= l_min < l_max <= 1e5 and
+ * probes and the final evaluation at each optimum read these series (no pass over the
+ * genotypes).  Needs 1e-5 <= l_min < l_max <= 1e5 and
  * 1 + 1e5 * min(eval) > 0.5 (no pole of 1/(lambda eval + 1) near the domain);
  * 2 = as 1, with the linear series sums already placed in chunk_workspace by
  * jb_lmm_chunk_series_i8 for the same chunk (only the squared sums use a DGEMM).

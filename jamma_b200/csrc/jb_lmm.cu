@@ -13,6 +13,11 @@
 //   phase 3  JAX-style golden-section refinement for MLE and REML, per-SNP lambda;
 //   epilogue Wald (from the final REML evaluation), LRT and score statistics.
 //
+// Mixed form (precision >= 1): no likelihood evaluation streams x.  The x-dependent sums
+// come from the SNP's global Chebyshev series in log lambda (chunk GEMM rows), log|H^-1|
+// and the x-free sums from per-bracket expansions; the final evaluation at each optimum
+// is one more such probe.
+//
 // The sequence of evaluations, bracket rules and NaN behaviour follow
 // src/jamma/lmm/likelihood_jax.py (148-339 likelihoods, 419-598 search, 601-798
 // statistics) exactly; only the summation order of the length-n reductions differs.
@@ -493,20 +498,30 @@ __device__ __forceinline__ void coop_shared(const BracketCoef<C>& b, double s, d
     for (int k = 0; k < Lay<C>::NS; ++k) shared[k] = warp_sum(b.c[1 + k] * tl);
 }
 
-// Mixed-form log-likelihood at log-lambda s: no length-n pass (series for the x-dependent
-// sums, bracket expansions for the rest).
+// Mixed-form log-likelihood at log-lambda s with no length-n pass: the x-dependent sums
+// from the SNP's global series, log|H^-1| and the x-free sums from the bracket's expansions
+// (exact FP64 node values).  The golden-section probes and the final evaluation at the
+// optimum both use it; pb receives the Pab rows for the statistics.
 template <int C, bool REML>
-__device__ __forceinline__ double coop_logl(const Params& p, const GlobalCoef<C>& g,
+__device__ __forceinline__ double coop_eval(const Params& p, const GlobalCoef<C>& g,
                                             const BracketCoef<C>& b, double s,
-                                            const double (&log_iab)[C + 1]) {
+                                            const double (&log_iab)[C + 1], PabOut<C>& pb) {
     using L = Lay<C>;
     double xs[L::NX], shared[L::NS], logdet;
     coop_xsums<C>(p, g, s, xs);
     coop_shared<C>(b, s, logdet, shared);
     double row0[L::NI];
     assemble<C>(row0, shared, xs);
-    const PabOut<C> pb = pab_reduce<C>(row0);
+    pb = pab_reduce<C>(row0);
     return REML ? reml_logl<C>(pb, log_iab, logdet, p) : mle_logl<C>(pb, logdet, p);
+}
+
+template <int C, bool REML>
+__device__ __forceinline__ double coop_logl(const Params& p, const GlobalCoef<C>& g,
+                                            const BracketCoef<C>& b, double s,
+                                            const double (&log_iab)[C + 1]) {
+    PabOut<C> pb;
+    return coop_eval<C, REML>(p, g, b, s, log_iab, pb);
 }
 
 // Golden-section refinement (_golden_section_refine, likelihood_jax.py:419-488) on the
@@ -536,75 +551,6 @@ __device__ double golden_coop(const Params& p, const GlobalCoef<C>& g, int best,
         a = na; b = nb; c = nc; d = nd; fc = nfc; fd = nfd;
     }
     return __dmul_rn(__dadd_rn(a, b), 0.5);
-}
-
-// Direct FP64 x-dependent sums at two lambdas in one pass over the rotated genotype
-// (the final MLE and REML evaluations share the read of x).
-template <int C>
-__device__ __forceinline__ void direct_xsums2(const Params& p, const double* __restrict__ x,
-                                              const double* __restrict__ y, double lam0,
-                                              double lam1, bool two,
-                                              double (&xs0)[Lay<C>::NX],
-                                              double (&xs1)[Lay<C>::NX]) {
-    using L = Lay<C>;
-    double a0[L::NX], a1[L::NX];
-#pragma unroll
-    for (int k = 0; k < L::NX; ++k) a0[k] = a1[k] = 0.0;
-    const int lane = threadIdx.x & 31;
-    auto step = [&](double ev, double xv, double yv, const double* w) {
-        const double t0 = __drcp_rn(__dadd_rn(__dmul_rn(lam0, ev), 1.0)) * xv;
-#pragma unroll
-        for (int a = 0; a < C; ++a) a0[a] = fma(t0, w[a], a0[a]);
-        a0[C] = fma(t0, xv, a0[C]);
-        a0[C + 1] = fma(t0, yv, a0[C + 1]);
-        if (two) {
-            const double t1 = __drcp_rn(__dadd_rn(__dmul_rn(lam1, ev), 1.0)) * xv;
-#pragma unroll
-            for (int a = 0; a < C; ++a) a1[a] = fma(t1, w[a], a1[a]);
-            a1[C] = fma(t1, xv, a1[C]);
-            a1[C + 1] = fma(t1, yv, a1[C + 1]);
-        }
-    };
-    int64_t i = lane;
-    for (; i + 32 * (UNR - 1) < p.n; i += 32 * UNR) {
-        double ev[UNR], xv[UNR], yv[UNR], w[UNR][C > 0 ? C : 1];
-#pragma unroll
-        for (int u = 0; u < UNR; ++u) {
-            ev[u] = __ldg(p.evals + i + 32 * u);
-            xv[u] = x[i + 32 * u];
-            yv[u] = __ldg(y + i + 32 * u);
-#pragma unroll
-            for (int a = 0; a < C; ++a) w[u][a] = __ldg(p.W + a * p.ldw + i + 32 * u);
-        }
-#pragma unroll
-        for (int u = 0; u < UNR; ++u) step(ev[u], xv[u], yv[u], w[u]);
-    }
-    for (; i < p.n; i += 32) {
-        double w[C > 0 ? C : 1];
-#pragma unroll
-        for (int a = 0; a < C; ++a) w[a] = __ldg(p.W + a * p.ldw + i);
-        step(__ldg(p.evals + i), x[i], __ldg(y + i), w);
-    }
-#pragma unroll
-    for (int k = 0; k < L::NX; ++k) {
-        xs0[k] = warp_sum(a0[k]);
-        xs1[k] = two ? warp_sum(a1[k]) : 0.0;
-    }
-}
-
-// Final mixed-form evaluation at the optimum: direct x-dependent sums, x-free sums and
-// log|H^-1| from the bracket's expansions (exact FP64 node values, ~1e-16 relative).
-template <int C, bool REML>
-__device__ __forceinline__ double final_logl(const Params& p, const double (&xs)[Lay<C>::NX],
-                                             const BracketCoef<C>& bc, double s,
-                                             const double (&log_iab)[C + 1], PabOut<C>& pb) {
-    using L = Lay<C>;
-    double shared[L::NS], logdet;
-    coop_shared<C>(bc, s, logdet, shared);
-    double row0[L::NI];
-    assemble<C>(row0, shared, xs);
-    pb = pab_reduce<C>(row0);
-    return REML ? reml_logl<C>(pb, log_iab, logdet, p) : mle_logl<C>(pb, logdet, p);
 }
 
 // Grid bracket + golden section (_golden_section_refine, likelihood_jax.py:419-488).
@@ -774,17 +720,25 @@ __device__ __forceinline__ void coop_shared_v(const BracketCoefV<C>& b, double s
 }
 
 template <int C, bool REML>
-__device__ __forceinline__ double coop_logl_v(const Params& p, const GlobalCoefV<C>& g,
+__device__ __forceinline__ double coop_eval_v(const Params& p, const GlobalCoefV<C>& g,
                                               const BracketCoefV<C>& b, double s,
-                                              const double (&log_iab)[C + 1]) {
+                                              const double (&log_iab)[C + 1], PabOut<C>& pb) {
     using L = Lay<C>;
     double xs[L::NX], shared[L::NS], logdet;
     coop_xsums_v<C>(p, g, s, xs);
     coop_shared_v<C>(b, s, logdet, shared);
     double row0[L::NI];
     assemble<C>(row0, shared, xs);
-    const PabOut<C> pb = pab_reduce<C>(row0);
+    pb = pab_reduce<C>(row0);
     return REML ? reml_logl<C>(pb, log_iab, logdet, p) : mle_logl<C>(pb, logdet, p);
+}
+
+template <int C, bool REML>
+__device__ __forceinline__ double coop_logl_v(const Params& p, const GlobalCoefV<C>& g,
+                                              const BracketCoefV<C>& b, double s,
+                                              const double (&log_iab)[C + 1]) {
+    PabOut<C> pb;
+    return coop_eval_v<C, REML>(p, g, b, s, log_iab, pb);
 }
 
 template <int C, bool REML>
@@ -811,82 +765,6 @@ __device__ double golden_coop_v(const Params& p, const GlobalCoefV<C>& g, int be
         a = na; b = nb; c = nc; d = nd; fc = nfc; fd = nfd;
     }
     return __dmul_rn(__dadd_rn(a, b), 0.5);
-}
-
-// direct_xsums2 with lanes l and l + 16 of the 32-lane form in one lane: each virtual lane
-// keeps its own accumulators and visits its samples (l + 32 t, l + 16 + 32 t) in order.
-template <int C>
-__device__ __forceinline__ void direct_xsums2_v(const Params& p, const double* __restrict__ x,
-                                                const double* __restrict__ y, double lam0,
-                                                double lam1, bool two,
-                                                double (&xs0)[Lay<C>::NX],
-                                                double (&xs1)[Lay<C>::NX]) {
-    using L = Lay<C>;
-    double a0[2][L::NX], a1[2][L::NX];
-#pragma unroll
-    for (int h = 0; h < 2; ++h)
-#pragma unroll
-        for (int k = 0; k < L::NX; ++k) a0[h][k] = a1[h][k] = 0.0;
-    const int lane = threadIdx.x & 15;
-    auto step = [&](int h, double ev, double xv, double yv, const double* w) {
-        const double t0 = __drcp_rn(__dadd_rn(__dmul_rn(lam0, ev), 1.0)) * xv;
-#pragma unroll
-        for (int a = 0; a < C; ++a) a0[h][a] = fma(t0, w[a], a0[h][a]);
-        a0[h][C] = fma(t0, xv, a0[h][C]);
-        a0[h][C + 1] = fma(t0, yv, a0[h][C + 1]);
-        if (two) {
-            const double t1 = __drcp_rn(__dadd_rn(__dmul_rn(lam1, ev), 1.0)) * xv;
-#pragma unroll
-            for (int a = 0; a < C; ++a) a1[h][a] = fma(t1, w[a], a1[h][a]);
-            a1[h][C] = fma(t1, xv, a1[h][C]);
-            a1[h][C + 1] = fma(t1, yv, a1[h][C + 1]);
-        }
-    };
-    int64_t i = lane;  // virtual lane 0 at i, virtual lane 1 at i + 16
-    for (; i + 32 * (UNR - 1) + 16 < p.n; i += 32 * UNR) {
-        double ev[2 * UNR], xv[2 * UNR], yv[2 * UNR], w[2 * UNR][C > 0 ? C : 1];
-#pragma unroll
-        for (int u = 0; u < 2 * UNR; ++u) {
-            const int64_t ii = i + 32 * (u >> 1) + 16 * (u & 1);
-            ev[u] = __ldg(p.evals + ii);
-            xv[u] = x[ii];
-            yv[u] = __ldg(y + ii);
-#pragma unroll
-            for (int a = 0; a < C; ++a) w[u][a] = __ldg(p.W + a * p.ldw + ii);
-        }
-#pragma unroll
-        for (int u = 0; u < 2 * UNR; ++u) step(u & 1, ev[u], xv[u], yv[u], w[u]);
-    }
-    for (; i < p.n; i += 32) {
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int64_t ii = i + 16 * h;
-            if (ii < p.n) {
-                double w[C > 0 ? C : 1];
-#pragma unroll
-                for (int a = 0; a < C; ++a) w[a] = __ldg(p.W + a * p.ldw + ii);
-                step(h, __ldg(p.evals + ii), x[ii], __ldg(y + ii), w);
-            }
-        }
-    }
-#pragma unroll
-    for (int k = 0; k < L::NX; ++k) {
-        xs0[k] = fold_sum(a0[0][k], a0[1][k]);
-        xs1[k] = two ? fold_sum(a1[0][k], a1[1][k]) : 0.0;
-    }
-}
-
-template <int C, bool REML>
-__device__ __forceinline__ double final_logl_v(const Params& p, const double (&xs)[Lay<C>::NX],
-                                               const BracketCoefV<C>& bc, double s,
-                                               const double (&log_iab)[C + 1], PabOut<C>& pb) {
-    using L = Lay<C>;
-    double shared[L::NS], logdet;
-    coop_shared_v<C>(bc, s, logdet, shared);
-    double row0[L::NI];
-    assemble<C>(row0, shared, xs);
-    pb = pab_reduce<C>(row0);
-    return REML ? reml_logl<C>(pb, log_iab, logdet, p) : mle_logl<C>(pb, logdet, p);
 }
 
 // jnp.argmax semantics: first maximum, NaN wins (first NaN).
@@ -941,8 +819,8 @@ constexpr int kPairsThreads = 128;
 template <int C>
 struct PairsOccupancy {
     static constexpr int kMinBlocks = C == 1 ? 4 : (C == 2 ? 3 : 2);  // C = 1: 125 registers, no spill
-    // two pairs per warp: each lane holds two virtual lanes' state (C = 1: 168 registers;
-    // 3 blocks measured 2% faster than 2 blocks at 180 registers and no spill)
+    // two pairs per warp: each lane holds two virtual lanes' state (C = 1: 160 registers,
+    // no spill; 4 blocks at 128 registers measured within 0.5 %)
     static constexpr int kMinBlocksHalf = 3;
 };
 
@@ -1056,40 +934,23 @@ __global__ void __launch_bounds__(kPairsThreads, GW == 16 ? PairsOccupancy<C>::k
         if (need_reml) s_r = golden_coop_v<C, true>(p, gcv, best_reml.idx, f, log_iab, br);
         lam_m = exp(s_m);
         lam_r = exp(s_r);
-        double xm[L::NX], xr[L::NX];
-        if (need_mle && need_reml) {
-            direct_xsums2_v<C>(p, x, y, lam_m, lam_r, true, xm, xr);
-        } else if (need_mle) {
-            direct_xsums2_v<C>(p, x, y, lam_m, lam_m, false, xm, xr);
-        } else {
-            direct_xsums2_v<C>(p, x, y, lam_r, lam_r, false, xr, xm);
-        }
         if (need_mle) {
             PabOut<C> pb;
-            logl_m = final_logl_v<C, false>(p, xm, bm, s_m, log_iab, pb);
+            logl_m = coop_eval_v<C, false>(p, gcv, bm, s_m, log_iab, pb);
         }
-        if (need_reml) logl_r = final_logl_v<C, true>(p, xr, br, s_r, log_iab, pb_r);
+        if (need_reml) logl_r = coop_eval_v<C, true>(p, gcv, br, s_r, log_iab, pb_r);
     } else if (INTERP) {
-        // both searches first, then one direct pass over x for the two final evaluations
         BracketCoef<C> bm, br;
         double s_m = 0.0, s_r = 0.0;
         if (need_mle) s_m = golden_coop<C, false>(p, gc, best_mle.idx, f, log_iab, bm);
         if (need_reml) s_r = golden_coop<C, true>(p, gc, best_reml.idx, f, log_iab, br);
         lam_m = exp(s_m);
         lam_r = exp(s_r);
-        double xm[L::NX], xr[L::NX];
-        if (need_mle && need_reml) {
-            direct_xsums2<C>(p, x, y, lam_m, lam_r, true, xm, xr);
-        } else if (need_mle) {
-            direct_xsums2<C>(p, x, y, lam_m, lam_m, false, xm, xr);
-        } else {
-            direct_xsums2<C>(p, x, y, lam_r, lam_r, false, xr, xm);
-        }
         if (need_mle) {
             PabOut<C> pb;
-            logl_m = final_logl<C, false>(p, xm, bm, s_m, log_iab, pb);
+            logl_m = coop_eval<C, false>(p, gc, bm, s_m, log_iab, pb);
         }
-        if (need_reml) logl_r = final_logl<C, true>(p, xr, br, s_r, log_iab, pb_r);
+        if (need_reml) logl_r = coop_eval<C, true>(p, gc, br, s_r, log_iab, pb_r);
     } else {
         if (need_mle) {
             PabOut<C> pb;
