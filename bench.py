@@ -601,9 +601,10 @@ def run_ours(args) -> None:
             "data": "synthetic (seeded device RNG; Binomial(2,p) genotypes, p~U(0.05,0.5))",
             "config": _config(args, m),
             # own kernels per step: decode, [pack pairs], tiles + rotation GEMM, [tiles +
-            # series GEMM], square, search (the cuBLAS DGEMM is not counted)
+            # series GEMM], square, search, F-test p-values (Wald: -lmm 1/4, score: -lmm 3/4)
+            # (the cuBLAS DGEMM is not counted)
             "gpu_launches": (1 + int(has_missing) + 2 + 2 * int(cohort_mixed.series_ws is not None)
-                             + 2) * args.steps,
+                             + 2 + int(args.mode in (1, 4)) + int(args.mode in (3, 4))) * args.steps,
             "kernel_ms_per_step": kern_ms,
             "fp64_form": {"value": value64, "unit": "SNPs/s", "steps": fp64_steps,
                           "kernel_ms_per_step": kern64, "speedup_mixed_vs_fp64": value / value64},

@@ -893,9 +893,9 @@ __global__ void __launch_bounds__(kPairsThreads, GW == 16 ? PairsOccupancy<C>::k
         double beta, tau, se;
         beta_se<C>(pb, clamp_pyy(pb.yy1), p.df, valid, beta, tau, se);
         const double fstat = p.n_d * (pb.xy * pb.xy) / (pb.yy * (valid ? pb.xx : 1.0));
-        const double pv = f_pvalue(fstat, p.df, valid);
         if (lane == 0 && valid_pair) {
-            if (p.out.p_score) p.out.p_score[o] = pv;
+            // the F statistic (NaN: no test); lmm_fpvalue_kernel turns it into the p-value
+            if (p.out.p_score) p.out.p_score[o] = valid ? fstat : jnan();
             if (p.mode == 3) {
                 if (p.out.beta) p.out.beta[o] = beta;
                 if (p.out.se) p.out.se[o] = se;
@@ -970,13 +970,12 @@ __global__ void __launch_bounds__(kPairsThreads, GW == 16 ? PairsOccupancy<C>::k
         const double px_yy = clamp_pyy(pb_r.yy1);
         beta_se<C>(pb_r, px_yy, p.df, valid, beta, tau, se);
         const double fstat = (pb_r.yy - px_yy) * tau;
-        const double pv = f_pvalue(fstat, p.df, valid);
         if (lane == 0 && valid_pair) {
             if (p.out.lambda_remle) p.out.lambda_remle[o] = lam_r;
             if (p.out.logl_h1) p.out.logl_h1[o] = logl_r;
             if (p.out.beta) p.out.beta[o] = beta;
             if (p.out.se) p.out.se[o] = se;
-            if (p.out.p_wald) p.out.p_wald[o] = pv;
+            if (p.out.p_wald) p.out.p_wald[o] = valid ? fstat : jnan();  // F, as for p_score
         }
     }
 }
@@ -1425,6 +1424,16 @@ __global__ void linspace_kernel(double* out, double start, double stop, int num)
     out[i] = (i == num - 1) ? stop : __dadd_rn(__dmul_rn((double)i, step), start);
 }
 
+// F statistics (NaN where there is no test) -> F-test p-values, in place, one thread per
+// value.  The continued fraction of betainc_reg takes up to ~100 steps for F above ~3 at
+// df ~ 2e4; inside the search kernel every lane of a pair's group would repeat it, and a
+// warp would wait for the slower of its pairs.
+__global__ void lmm_fpvalue_kernel(double* __restrict__ v, int64_t count, double df) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+         i += (int64_t)gridDim.x * blockDim.x)
+        v[i] = f_pvalue(v[i], df, true);
+}
+
 template <int C>
 int32_t launch_pairs(const Params& p, cudaStream_t st) {
     const int64_t pairs = p.m * p.phi;
@@ -1436,6 +1445,15 @@ int32_t launch_pairs(const Params& p, cudaStream_t st) {
     else
         lmm_pairs_kernel<C, false, 32><<<(unsigned)ceil_div(pairs * 32, kPairsThreads), kPairsThreads, 0, st>>>(p);
     JB_LAUNCH_CHECK("lmm_pairs_kernel");
+    // p-values of the tests this mode ran (other outputs stay untouched)
+    double* const fv[2] = {(p.mode == 1 || p.mode == 4) ? p.out.p_wald : nullptr,
+                           (p.mode == 3 || p.mode == 4) ? p.out.p_score : nullptr};
+    const int64_t blocks = ceil_div(pairs, 256) < 4096 ? ceil_div(pairs, 256) : 4096;
+    for (double* v : fv) {
+        if (!v) continue;
+        lmm_fpvalue_kernel<<<(unsigned)blocks, 256, 0, st>>>(v, pairs, p.df);
+        JB_LAUNCH_CHECK("lmm_fpvalue_kernel");
+    }
     return JB_OK;
 }
 
