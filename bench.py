@@ -30,9 +30,12 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 HBM_PEAK_FALLBACK = 6650.0
-# DRAM read + write bytes of one INT8 rotation launch at n = 20 000, 8 192 SNPs with missing
-# calls, from one ncu capture (dram__bytes_read.sum 29.09 GB + dram__bytes_write.sum 1.31 GB)
-ROT_DRAM_BYTES = 30.40e9
+BF16_PEAK_FALLBACK = 1590.0
+# DRAM read + write bytes of one INT8 rotation launch, measured once with ncu
+# (dram__bytes_read.sum + dram__bytes_write.sum) for the configuration in the key:
+# (n, SNPs per launch, missing calls present, rotation kernel variant, tile schedule).
+# Any other configuration reports traffic null rather than a stale figure.
+ROT_DRAM_BYTES = {(20000, 8192, True, 0, (9, 16)): 30.40e9}
 
 
 def _peaks() -> dict:
@@ -192,27 +195,39 @@ def _kinship_phases(ev, n: int, p: int, i8_peak: float) -> dict | None:
         return None
     chunks_ms, gram_ms = ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2])
     tops = n * (n + 1.0) * p / (gram_ms / 1e3) / 1e12
-    return {"chunks_ms": chunks_ms, "gram_and_finalize_ms": gram_ms,
-            "gram_tops": tops, "gram_frac_of_int8_peak": tops / i8_peak,
-            "note": "chunks: transpose into the Gram operand, bitmasks, dosage words, the "
-                    "missing-call walk and the correction vectors for every chunk; "
-                    "gram_tops counts n(n+1)p int8 ops against the whole second phase"}
+    return {"chunks_ms": _r(chunks_ms), "gram_finalize_ms": _r(gram_ms), "gram_tops": _r(tops),
+            "gram_frac_int8_measured": _r(tops / i8_peak)}
 
 
-def _accuracy(got: dict, ref: dict) -> dict:
-    """Errors of one form's statistics against another's on the same SNPs: max / median
-    relative error per field; for p-values also the fraction within 1e-6 relative, the
-    max |log10 p| difference and the number of significance calls that differ at 5e-8."""
+def _r(x, sig: int = 3):
+    """Round to `sig` significant digits (keeps the JSON line short)."""
+    if x is None or not np.isfinite(x) or x == 0:
+        return None if x is None else (float(x) if np.isfinite(x) else None)
+    return float(f"{x:.{sig - 1}e}")
+
+
+P_FIELDS = ("p_wald", "p_lrt", "p_score")
+ACC_FIELDS = ("beta", "se", "logl_h1", "lambda_remle", "lambda_mle") + P_FIELDS
+
+
+def _accuracy(got: dict, ref: dict, rows=slice(None)) -> dict:
+    """Errors of one form's statistics against another's on the same SNPs.  Per field the
+    max / median relative error and the number of SNPs whose NaN pattern differs; for
+    p-values also the fraction within 1e-6 relative, the max |log10 p| difference and the
+    number of significance calls that differ at 5e-8."""
     out = {}
-    for k in sorted(got):
-        a, b = np.asarray(got[k]).ravel(), np.asarray(ref[k]).ravel()
+    for k in ACC_FIELDS:
+        if k not in got or k not in ref:
+            continue
+        a = np.asarray(got[k], dtype=np.float64).ravel()[rows]
+        b = np.asarray(ref[k], dtype=np.float64).ravel()[rows]
         ok = np.isfinite(a) & np.isfinite(b)
         rel = np.abs(a[ok] - b[ok]) / np.maximum(np.abs(b[ok]), 1e-300)
         e = {"max_rel": float(rel.max()) if rel.size else None,
              "median_rel": float(np.median(rel)) if rel.size else None,
              "nonfinite_mismatch": int(np.sum(np.isfinite(a) != np.isfinite(b)))}
-        if k.startswith("p_"):
-            e["frac_rel_lt_1e-6"] = float(np.mean(rel < 1e-6)) if rel.size else None
+        if k in P_FIELDS:
+            e["frac_rel_le_1e-6"] = float(np.mean(rel <= 1e-6)) if rel.size else None
             e["max_abs_dlog10"] = float(np.max(np.abs(np.log10(a[ok]) - np.log10(b[ok])))) \
                 if rel.size else None
             e["calls_differ_5e-8"] = int(np.sum((a[ok] < 5e-8) != (b[ok] < 5e-8)))
@@ -220,21 +235,99 @@ def _accuracy(got: dict, ref: dict) -> dict:
     return out
 
 
-def _cpu_baseline(args, cohort, evals_h, U_h, UtW_h, Uty_h, lam0, l0) -> dict:
-    """Oracle timed on the host over a bounded sample of the same workload."""
+def _accuracy_compact(acc: dict) -> dict:
+    """One number per non-p field (max rel) and [max rel, fraction <= 1e-6, max |dlog10 p|,
+    calls differing at 5e-8] per p-value field; NaN-pattern mismatches summed."""
+    out = {}
+    for k, e in acc.items():
+        key = {"lambda_remle": "l_remle", "lambda_mle": "l_mle"}.get(k, k)
+        if k in P_FIELDS:
+            out[key] = [_r(e["max_rel"]), _r(e["frac_rel_le_1e-6"], 4), _r(e["max_abs_dlog10"]),
+                        e["calls_differ_5e-8"]]
+        else:
+            out[key] = _r(e["max_rel"])
+    out["nan_mismatch"] = int(sum(e["nonfinite_mismatch"] for e in acc.values()))
+    return out
+
+
+def _oracle_check(args, packed_host: np.ndarray, evals_h: np.ndarray, UT: np.ndarray,
+                  W: np.ndarray, y: np.ndarray) -> tuple[dict, dict]:
+    """The oracle (jamma's path restated in NumPy/SciPy) on the first SNPs of a timed chunk:
+    the same packed records, decoded on the host, mean-imputed with the float32 pass-1
+    mean, rotated with the same eigenvectors on host BLAS, and searched.  Returns the
+    oracle's statistics and the CPU baseline: rotation + search of these SNPs timed on the
+    host cores (the null model is cohort set-up and runs before the timer)."""
     from threadpoolctl import threadpool_info
 
     from oracle import lmm as OL
+    from oracle.kinship import stream_pass1_means
+    from oracle.plink import decode_packed
 
-    m = args.cpu_snps
-    rng = np.random.default_rng(7)
-    g = rng.binomial(2, rng.uniform(0.05, 0.5, m), size=(args.n, m)).astype(np.float64)
+    n = args.n
+    g = decode_packed(packed_host, n)  # (n, m) float64, NaN = missing
+    mean32, _, _ = stream_pass1_means(g)
+    g = np.where(np.isnan(g), np.asarray(mean32, dtype=np.float64)[None, :], g)
+    UtW, Uty = UT @ W, UT @ y
+    lam0 = l0 = None
+    if args.mode in (2, 3, 4):
+        lam0, l0 = OL.null_model_mle(evals_h, UtW, Uty)
     t = time.perf_counter()
-    OL.lmm_chunk(args.mode, evals_h, UtW_h, Uty_h, U_h.T @ g, l0, lam0)
+    ref = OL.lmm_chunk(args.mode, evals_h, UtW, Uty, UT @ g, l0, lam0)
     sec = time.perf_counter() - t
-    cores = max([i.get("num_threads", 0) for i in threadpool_info() if i.get("user_api") == "blas"] or [1])
-    return {"value": m / sec, "unit": "SNPs/s", "cores": cores, "kind": "port",
-            "sample": f"{m} SNPs at n={args.n} (rotation on host BLAS + NumPy search, -lmm {args.mode})"}
+    m = g.shape[1]
+    cores = max([i.get("num_threads", 0) for i in threadpool_info() if i.get("user_api") == "blas"]
+                or [1])
+    cpu = {"value": m / sec, "unit": "SNPs/s", "cores": cores, "kind": "port",
+           "sample": f"the first {m} SNPs of a timed chunk (same records, 1 % missing calls) at "
+                     f"n={n}, -lmm {args.mode}: host-BLAS rotation + NumPy/SciPy search"}
+    return ref, cpu
+
+
+def _e2e_streaming(args, w, U, W, y, packed_host: np.ndarray) -> dict:
+    """The metric end to end through jamma's public streaming runner on a PLINK file:
+    ``run_lmm_association_streaming(bfile, ..., precision="mixed")`` with the cohort's
+    eigendecomposition.  Its association stage (every chunk's .bed read into pinned host
+    memory, host-to-device copy, the chunk's CUDA graph, device-to-host copy of the
+    results) is timed by the runner on the host wall clock; the whole call (pass-1
+    statistics over the file, cohort set-up from the eigenvectors, the result objects) is
+    reported beside it."""
+    import shutil
+    import tempfile
+
+    import torch
+
+    from jamma_b200 import run_lmm_association_streaming
+    from jamma_b200.io import write_plink_records
+
+    n, m = args.n, args.chunk
+    tmp = Path(tempfile.mkdtemp(prefix="jb_e2e_"))
+    try:
+        prefix = tmp / "cohort"
+        write_plink_records(prefix, packed_host, n)
+        timing: dict = {}
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        res = run_lmm_association_streaming(prefix, y, eigenvalues=w, eigenvectors=U,
+                                            covariates=W if W.shape[1] > 1 else None,
+                                            lmm_mode=args.mode, precision="mixed",
+                                            timing=timing)
+        call_s = time.perf_counter() - t
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    tested = timing["n_tested"]
+    bps = (n + 3) // 4
+    n_out = 9 if args.mode == 4 else 5
+    return {"value": tested / timing["association_s"], "unit": "SNPs/s",
+            "h2d_bytes_per_step": m * bps + m * 8, "d2h_bytes_per_step": n_out * m * 8,
+            "path": "jamma_b200.run_lmm_association_streaming(bfile, precision='mixed', "
+                    f"lmm_mode={args.mode}) on a written .bed: association stage (pinned "
+                    "double-buffered .bed chunks, side-stream H2D, CUDA-graph replay, async D2H) "
+                    "on the host wall clock",
+            "snps": tested, "chunk": m, "association_s": _r(timing["association_s"], 4),
+            "whole_call_snps_per_s": _r(tested / call_s, 4),
+            "whole_call_s": {"total": _r(call_s, 4), "pass1": _r(timing["stats_s"], 4),
+                             "setup": _r(timing["setup_s"], 4), "results": _r(timing["write_s"], 4)},
+            "results_returned": len(res)}
 
 
 def run_serving(args, seed: int = 7) -> dict:
@@ -400,7 +493,7 @@ def run_ours(args) -> None:
         """Warm up, then time `steps` chunks of one precision form with CUDA events."""
         c = cohort_mixed if precision == "mixed" else cohort
         outs = c.alloc_out(m)
-        ev = {k: [] for k in ("decode", "rotate", "lmm")}
+        ev = {k: [] for k in ("decode", "rotate", "rotate_gemm", "lmm")}
 
         def mark():
             e = torch.cuda.Event(enable_timing=True)
@@ -412,8 +505,10 @@ def run_ours(args) -> None:
             _native.call("jb_decode_bed", ptr(rec[s * m:(s + 1) * m]), bps, m, None, n, ptr(codes),
                          ld, ptr(counts), stream_handle())
             e1 = mark()
+            er = []
             if precision == "mixed":
-                c.rotate_codes_i8(codes, means[s], has_missing, out=UtG)
+                c.rotate_codes_i8(codes, means[s], has_missing, out=UtG,
+                                  after_rotation=lambda: er.append(mark()))
             else:
                 _native.call("jb_impute_f64", ptr(codes), ld, n, m, ptr(means[s]), ptr(G), n,
                              stream_handle())
@@ -424,6 +519,8 @@ def run_ours(args) -> None:
             if record:
                 for k, a, b in (("decode", e0, e1), ("rotate", e1, e2), ("lmm", e2, e3)):
                     ev[k].append((a, b))
+                if er:
+                    ev["rotate_gemm"].append((e1, er[0]))
 
         for s in range(args.warmup):
             step(s, False)
@@ -450,7 +547,7 @@ def run_ours(args) -> None:
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             ms = float(tt.item())
             dist.barrier()
-        kern = {k: float(np.mean([x.elapsed_time(y) for x, y in v])) for k, v in ev.items()}
+        kern = {k: float(np.mean([x.elapsed_time(y) for x, y in v])) for k, v in ev.items() if v}
         return ms, kern, clk.summary(), outs
 
     cohort_mixed = eng.DeviceCohort(w, U, W, y, lmm_mode=args.mode, precision="mixed")
@@ -468,7 +565,10 @@ def run_ours(args) -> None:
     ms64, kern64, _, _ = run_form("fp64", fp64_steps)
     value64 = fp64_steps * m * world / (ms64 / 1e3)
 
-    # ---------------- accuracy: mixed form vs the plain FP64 form on the same chunk (untimed)
+    # ---------------- accuracy on one timed chunk (untimed): both GPU forms on the whole
+    # chunk, and the oracle on its first SNPs (same records, eigendecomposition and phenotype)
+    s_acc = args.warmup
+
     def one_chunk(precision: str, s: int) -> dict:
         c = cohort_mixed if precision == "mixed" else cohort
         o = c.alloc_out(m)
@@ -481,54 +581,26 @@ def run_ours(args) -> None:
                          stream_handle())
             eng.rotate(c.U, G, out=UtG)
         c.associate_rotated(UtG, o)
-        return {k: v.cpu().numpy() for k, v in o.items()}
+        return {k: v.cpu().numpy()[0] for k, v in o.items()}
 
-    accuracy = _accuracy(one_chunk("mixed", args.warmup), one_chunk("fp64", args.warmup))
+    got_mixed, got_fp64 = one_chunk("mixed", s_acc), one_chunk("fp64", s_acc)
+    acc_mixed_fp64 = _accuracy(got_mixed, got_fp64)
+    acc_oracle = cpu = None
+    if rank == 0 and not args.no_cpu:
+        k = min(args.oracle_snps, m)
+        UT = U.cpu().numpy()  # row j = eigenvector j
+        ref, cpu = _oracle_check(args, rec[s_acc * m:s_acc * m + k].cpu().numpy(), w.cpu().numpy(),
+                                 UT, W, y)
+        del UT
+        acc_oracle = {"snps": k, "mixed": _accuracy(got_mixed, ref, slice(0, k)),
+                      "fp64": _accuracy(got_fp64, ref, slice(0, k))}
 
-    # ---------------- end to end through the public chunk API with host buffers (mixed form)
-    # Each step: pinned-host packed records + means -> device, the chunk's captured CUDA
-    # graph (decode, rotation, series sums, search, statistics), results -> pinned host.
-    rec_h = rec[:m].cpu().pin_memory()
-    mean_h = means[0].cpu().pin_memory()
-    res_h = {k: torch.empty((1, m), dtype=torch.float64).pin_memory() for k in outs}
-    graph = eng.ChunkGraph(cohort_mixed, m, has_missing=has_missing)
-    bufs = {"UtG": UtG}
-
-    def e2e_graph_step():
-        graph.packed.copy_(rec_h, non_blocking=True)
-        graph.means.copy_(mean_h, non_blocking=True)
-        for k, v in graph.replay().items():
-            res_h[k].copy_(v, non_blocking=True)
-
-    def e2e_eager_step():
-        rd = rec_h.to("cuda", non_blocking=True)
-        md = mean_h.to("cuda", non_blocking=True)
-        cd, _ = eng.decode_packed(rd, n, None, n, ld=ld)
-        o = cohort_mixed.associate_codes(cd, md, out=outs, bufs=bufs, has_missing=has_missing)
-        for k, v in o.items():
-            res_h[k].copy_(v, non_blocking=True)
-
-    def time_e2e(fn):
-        for _ in range(2):
-            fn()
-        torch.cuda.synchronize()
-        k = max(2, min(args.steps, 5))
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(st)
-        for _ in range(k):
-            fn()
-        b.record(st)
-        torch.cuda.synchronize()
-        t = a.elapsed_time(b) / k
-        if world > 1:
-            tt = torch.tensor([t], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t = float(tt.item())
-        return t
-
-    e2e_ms = time_e2e(e2e_graph_step)
-    e2e_eager_ms = time_e2e(e2e_eager_step)
-    del graph
+    # ---------------- end to end through the public streaming runner on a .bed file
+    e2e = None
+    if rank == 0 and not args.no_e2e:
+        del G
+        e2e = _e2e_streaming(args, w, U, W, y, rec.cpu().numpy())
+        G = eng.empty((m, n))
 
     # ---------------- many phenotypes per cohort (one SNP chunk, all phenotypes per warp set)
     multi = None
@@ -561,8 +633,8 @@ def run_ours(args) -> None:
             torch.cuda.profiler.stop()
         pms = a.elapsed_time(b) / ps
         multi = {"phenotypes": phi, "lmm_mode": args.pheno_mode, "snps_per_step": mp,
-                 "ms_per_step": pms, "snp_phenotype_pairs_per_s": mp * phi / (pms / 1e3),
-                 "snps_per_s_all_phenotypes": mp / (pms / 1e3), "steps": ps,
+                 "ms_per_step": _r(pms, 4), "snp_phenotype_pairs_per_s": _r(mp * phi / (pms / 1e3), 4),
+                 "snps_per_s_all_phenotypes": _r(mp / (pms / 1e3), 4), "steps": ps,
                  "series_from_int8_calls": coh_p.series_ws is not None}
         del coh_p, outs_p
 
@@ -579,73 +651,75 @@ def run_ours(args) -> None:
 
     if rank == 0:
         peaks = _peaks()
-        # dominant kernel of the mixed form: the INT8 tcgen05 rotation, 4 digit planes x
-        # (calls + missing masks) -> 2 * n^2 * m * 4 * (2 if missing) int8 ops per step
+        bf16 = peaks.get("bf16_tflops")
+        bf16_src = "measured (MEASURED_PEAKS.json bf16_tflops, burst)" if bf16 else "fallback"
+        bf16 = bf16 or BF16_PEAK_FALLBACK
+        # dominant kernel of the mixed form: the INT8 tcgen05 rotation GEMM.  Algorithmic
+        # work of one launch: one rotation U^T G, 2 n^2 m flops (independent of how the
+        # product is split); the implementation issues 4 digit planes x (calls [+ masks])
+        # int8 products.
+        rot_ms = kern_ms.get("rotate_gemm", kern_ms["rotate"])
+        alg_flops = 2.0 * n * n * m
         planes = 4 * (2 if has_missing else 1)
-        rot_ops = 2.0 * n * n * m * planes
-        i8_nominal = args.int8_peak_tops
         i8_measured = _int8_gemm_peak()
-        achieved = rot_ops / (kern_ms["rotate"] / 1e3) / 1e12
-        evals_h = w.cpu().numpy()
-        U_h = U.cpu().numpy().T
-        lam0, l0 = cohort.null_model()
-        cpu = None
-        if not args.no_cpu:
-            cpu = _cpu_baseline(args, cohort, evals_h, U_h, U_h.T @ W, U_h.T @ y,
-                                float(lam0[0]) if lam0 is not None else None,
-                                float(l0[0]) if l0 is not None else None)
+        achieved = alg_flops / (rot_ms / 1e3) / 1e12
+        impl_tops = alg_flops * planes / (rot_ms / 1e3) / 1e12
+        variant = int(_native.load().jb_rotate_get_kernel())
+        gm, gn = np.zeros(1, np.int32), np.zeros(1, np.int32)
+        _native.call("jb_rotate_get_schedule", gm.ctypes.data, gn.ctypes.data)
+        traffic = ROT_DRAM_BYTES.get((n, m, has_missing, variant, (int(gm[0]), int(gn[0]))))
+        roofline = {
+            "kernel": "i8_gemm_kernel<RotEpi> (tcgen05 kind::i8, digit-plane rotation U^T G)",
+            "bound": "tensor", "achieved": achieved, "peak": bf16, "unit": "TFLOP/s",
+            "frac": achieved / bf16, "traffic": traffic,
+            "peak_source": f"{bf16_src}: dense bf16 cuBLAS GEMM, the tensor-pipe roofline",
+            "algorithmic": "2 n^2 m flops per launch (one rotation; n samples, m SNPs)",
+            "launch_ms": _r(rot_ms, 4),
+            "impl_int8_ops_per_launch": alg_flops * planes,
+            "impl_tops": _r(impl_tops, 4), "int8_measured_tops": _r(i8_measured, 4),
+            "impl_frac_of_int8_measured": _r(impl_tops / i8_measured, 4),
+            "algorithmic_bytes": 4 * n * n + 2 * n * m + 8 * n * m,
+        }
+        n_tests_f = int(args.mode in (1, 4)) + int(args.mode in (3, 4))
+        series = cohort_mixed.series_ws is not None
+        # own kernels per step: decode, [pack pairs], tiles + rotation GEMM, [tiles + series
+        # GEMM], square, search, F-test p-values (the cuBLAS DGEMM is not counted)
+        launches = (1 + int(has_missing) + 2 + 2 * int(series) + 2 + n_tests_f) * args.steps
         line = {
             "metric": "lmm_assoc_snps_per_s", "value": value, "unit": "SNPs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8+f64",
             "data": "synthetic (seeded device RNG; Binomial(2,p) genotypes, p~U(0.05,0.5))",
             "config": _config(args, m),
-            # own kernels per step: decode, [pack pairs], tiles + rotation GEMM, [tiles +
-            # series GEMM], square, search, F-test p-values (Wald: -lmm 1/4, score: -lmm 3/4)
-            # (the cuBLAS DGEMM is not counted)
-            "gpu_launches": (1 + int(has_missing) + 2 + 2 * int(cohort_mixed.series_ws is not None)
-                             + 2 + int(args.mode in (1, 4)) + int(args.mode in (3, 4))) * args.steps,
-            "kernel_ms_per_step": kern_ms,
-            "fp64_form": {"value": value64, "unit": "SNPs/s", "steps": fp64_steps,
-                          "kernel_ms_per_step": kern64, "speedup_mixed_vs_fp64": value / value64},
+            "gpu_launches": launches,
+            "kernel_ms_per_step": {k: _r(v, 4) for k, v in kern_ms.items()},
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "clocks": clocks,
             "kinship_s": kinship_s, "kinship_form": "int8 tcgen05 Gram + FP64 corrections",
-            "kinship_phases": _kinship_phases(kin_events.get("int8"), n, int(keep.size), i8_measured),
             "kinship_fp64_s": kinship_fp64_s, "kinship_snps": int(keep.size),
             "kinship_int8_vs_fp64_max_rel_diff": kin_maxdiff, "eigh_s": eigh_s,
-            "roofline": {"kernel": "i8_gemm_kernel<rotate> (tcgen05 kind::i8, 4 digit planes)",
-                         "bound": "tensor", "achieved": achieved, "peak": i8_measured,
-                         "unit": "TOP/s", "frac": achieved / i8_measured,
-                         "peak_source": "measured in this run: cuBLASLt INT8 GEMM 8192^3 "
-                                        "(torch._int_mm), best of 10 (MEASURED_PEAKS.json "
-                                        "holds HBM and BF16 only)",
-                         "nominal_peak": i8_nominal, "frac_of_nominal": achieved / i8_nominal,
-                         # DRAM bytes of one launch, one ncu capture of this workload
-                         "traffic": ROT_DRAM_BYTES if (n, m, has_missing) == (20000, 8192, True) else None,
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
-                                           "rotation launch, n=20000, 8192 SNPs, schedule 9x16 "
-                                           "(profiles/rotate_i8_RotEpi_n20000_chunk8192_dram.md)",
-                         "algorithmic_bytes": 4 * n * n + 2 * n * m + 8 * n * m,
-                         "nominal_peak_source": args.int8_peak_source},
-            "accuracy_mixed_vs_fp64_form": {"snps": m, "fields": accuracy},
-            "search_kernel": {"kernel": "lmm_pairs_kernel (FP64 search + statistics)",
-                              "ms_per_step": kern_ms["lmm"]},
-            "cpu_baseline": cpu,
-            "e2e": {"value": m / (e2e_ms / 1e3) * world, "unit": "SNPs/s",
-                    "h2d_bytes_per_step": m * bps + m * 8,
-                    "d2h_bytes_per_step": len(outs) * m * 8,
-                    "path": "engine.ChunkGraph replay (CUDA graph of the chunk) with pinned-host "
-                            "copies in the timed region",
-                    "eager_value": m / (e2e_eager_ms / 1e3) * world},
-            "clocks": clocks,
+            "accuracy_detail": {"mixed_vs_fp64_form": acc_mixed_fp64,
+                                "vs_oracle": acc_oracle},
             "serving": serving,
             "multi_phenotype": multi,
             "autotune": None if tuned is None else {
                 "kernel": ["one CTA per tile", "CTA pairs (cta_group::2)"][tuned["kernel"]],
                 "schedule": tuned["schedule"], "best_chunk": tuned["chunk"],
-                "best_chunk_snps_per_s": tuned["snps_per_s"],
-                "trials": [{k: t[k] for k in ("chunk", "kernel", "schedule", "ms")}
-                           for t in tuned["trials"]]},
+                "best_chunk_snps_per_s": _r(tuned["snps_per_s"], 4), "trials": len(tuned["trials"])},
             "hbm_peak_gbs": peaks.get("hbm_gbs", HBM_PEAK_FALLBACK),
+            # ---- north-star evidence last (read from the end of the line)
+            "kinship_phases": _kinship_phases(kin_events.get("int8"), n, int(keep.size), i8_measured),
+            "accuracy_mixed_vs_fp64_form": dict(snps=m, **_accuracy_compact(acc_mixed_fp64)),
+            "accuracy_vs_oracle": None if acc_oracle is None else {
+                "snps": acc_oracle["snps"], "n": n,
+                "key": "non-p: max rel; p: [max rel, frac <= 1e-6, max |dlog10 p|, calls differ 5e-8]",
+                "mixed": _accuracy_compact(acc_oracle["mixed"]),
+                "fp64": _accuracy_compact(acc_oracle["fp64"])},
+            "fp64_form": {"value": _r(value64, 4), "unit": "SNPs/s", "steps": fp64_steps,
+                          "kernel_ms_per_step": {k: _r(v, 4) for k, v in kern64.items()}},
+            "speedup_mixed_vs_fp64": _r(value / value64, 4),
         }
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -789,7 +863,10 @@ def main():
     ap.add_argument("--int8-peak-tops", type=float, default=4500.0)
     ap.add_argument("--int8-peak-source", default="nominal B200 dense INT8 (4.5 POP/s); "
                     "MEASURED_PEAKS.json has no INT8 figure")
-    ap.add_argument("--cpu-snps", type=int, default=64)
+    ap.add_argument("--oracle-snps", type=int, default=64,
+                    help="SNPs of a timed chunk checked against the CPU oracle (also the CPU baseline)")
+    ap.add_argument("--no-e2e", action="store_true",
+                    help="skip the end-to-end run through run_lmm_association_streaming")
     ap.add_argument("--ref-snps", type=int, default=64)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serving", action="store_true")

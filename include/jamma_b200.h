@@ -162,12 +162,20 @@ int32_t jb_gram_status(const void* workspace, int32_t* out, uintptr_t stream);
  * that loads the library keeps until the process exits; n <= 65408 fits, larger n is
  * rejected with JB_E_INVALID and a message.  The first call on a device looks up that
  * array's device address (cudaGetSymbolAddress), so make it before any stream capture.
+ * The looked-up address is kept for the life of the process, so the device's primary
+ * context must not be reset (cudaDeviceReset) after that first call.
  * Every call reuses the one array (the status word is cleared on each call), so calls
  * that overlap on the GPU -- on different streams, or from different host threads --
  * race: serialise them.  No counterpart in the jamma reference.
+ *
+ * jb_gram_i8_noalloc_status: after jb_gram_i8_noalloc calls on `stream`, copy the
+ * pipeline status word of the static scratch to *out (host memory) and synchronise the
+ * stream: 0 = OK, non-zero = a bounded tensor-core pipeline wait ran out and C is
+ * incomplete.  Allocates nothing.  No counterpart in the jamma reference.
  */
 int32_t jb_gram_i8_noalloc(const int8_t* Zs, int64_t n, int64_t p, int64_t ldz, int32_t* C,
                            int64_t ldc, uintptr_t stream);
+int32_t jb_gram_i8_noalloc_status(int32_t* out, uintptr_t stream);
 int32_t jb_codes_to_sample_major(const int8_t* codes, int64_t ld_codes, int64_t n,
                                  int64_t m, int8_t* Zs, int64_t ldz, int64_t col0,
                                  int8_t* Cs, int64_t ldcs, uintptr_t stream);

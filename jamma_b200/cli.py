@@ -1,10 +1,15 @@
 """Command line with jamma's GEMMA-style flags (src/jamma/cli.py:54-524).
 
     python -m jamma_b200.cli [-outdir D] [-o P] gk -bfile B [-gk 1|2] [-maf M] [-miss R]
-                             [-loco] [-eigen] [-n N] [-ksnps FILE]
+                             [-loco] [-eigen] [-n N] [-ksnps FILE] [-precision fp64|mixed]
     python -m jamma_b200.cli [-outdir D] [-o P] lmm -bfile B [-k K | -d D -u U | -loco]
                              [-c C] [-lmm 1-4] [-maf M] [-miss R] [-eigen] [-n N]
-                             [-snps FILE] [-ksnps FILE] [-hwe P]
+                             [-snps FILE] [-ksnps FILE] [-hwe P] [-precision fp64|mixed]
+
+``-precision`` (not a GEMMA flag) selects the form of the device steps: ``fp64`` (the
+default) reproduces jamma's FP64 results; ``mixed`` runs the INT8 tensor-core kinship
+Gram, the INT8 digit-plane rotation and the series-interpolated lambda search (-gk 1 only;
+-gk 2 stays FP64).
 
 Both commands write ``{outdir}/{prefix}.log.txt`` in GEMMA's ``##`` layout.  Errors are
 reported as ``Error: ...`` with exit status 1 (cli.py:485-487).
@@ -37,6 +42,9 @@ def _gk(a, command_line: str) -> None:
     out = Path(a.outdir)
     meta = get_plink_metadata(a.bfile)
     ks = _snp_indices(a.ksnps, meta["sid"]) if a.ksnps else None
+    kin_precision = "int8" if a.precision == "mixed" else "fp64"
+    if a.gk == 2 and a.precision == "mixed":
+        raise ValueError("-gk 2 (standardized) is computed in FP64 only; drop -precision mixed")
     if a.loco:
         if a.gk == 2:
             raise ValueError("-gk 2 (standardized) is not supported with -loco; LOCO kinship "
@@ -45,7 +53,8 @@ def _gk(a, command_line: str) -> None:
         from jamma_b200.loco import compute_loco_kinship
 
         n_chr = 0
-        for chrom, K in compute_loco_kinship(a.bfile, a.maf, a.miss, ksnps_indices=ks):
+        for chrom, K in compute_loco_kinship(a.bfile, a.maf, a.miss, ksnps_indices=ks,
+                                             precision=kin_precision):
             _w(K.cpu().numpy(), out / f"{a.prefix}.loco.cXX.chr{chrom}.txt")
             n_chr += 1
         elapsed = time.perf_counter() - t0
@@ -54,7 +63,8 @@ def _gk(a, command_line: str) -> None:
                         {"total": elapsed, "kinship": elapsed}, command_line)
         print(f"wrote {n_chr} LOCO kinship matrices to {out}")
         return
-    K = compute_kinship_from_bed(a.bfile, a.maf, a.miss, kinship_mode=a.gk, ksnps_indices=ks)
+    K = compute_kinship_from_bed(a.bfile, a.maf, a.miss, kinship_mode=a.gk, ksnps_indices=ks,
+                                 precision=kin_precision)
     t_k = time.perf_counter() - t0
     kpath = out / f"{a.prefix}.cXX.txt"
     write_kinship_matrix(K, kpath)
@@ -83,10 +93,10 @@ def _lmm(a, command_line: str) -> None:
              maf=a.maf, miss=a.miss, output_dir=a.outdir, output_prefix=a.prefix,
              loco=a.loco, eigenvalue_file=a.eigenD, eigenvector_file=a.eigenU,
              write_eigen=a.eigen, phenotype_column=a.pheno_col, snps_file=a.snps,
-             ksnps_file=a.ksnps, hwe=a.hwe)
+             ksnps_file=a.ksnps, hwe=a.hwe, precision=a.precision)
     write_gemma_log(a.outdir, a.prefix, {"n_samples": r.n_samples, "n_snps": r.n_snps_tested,
                                          "lmm_mode": a.mode, "maf_threshold": a.maf,
-                                         "miss_threshold": a.miss},
+                                         "miss_threshold": a.miss, "precision": a.precision},
                     {k.removesuffix("_s"): v for k, v in r.timing.items()}, command_line)
     print(f"{r.n_snps_tested} SNPs, {r.timing['total_s']:.2f}s -> "
           f"{Path(a.outdir) / (a.prefix + '.assoc.txt')}")
@@ -108,6 +118,7 @@ def main(argv=None) -> int:
     gk.add_argument("-eigen", action="store_true")
     gk.add_argument("-n", dest="pheno_col", type=int, default=1)
     gk.add_argument("-ksnps")
+    gk.add_argument("-precision", choices=("fp64", "mixed"), default="fp64")
     gk.add_argument("--check-memory", dest="check_memory", action="store_true", default=True)
     gk.add_argument("--no-check-memory", dest="check_memory", action="store_false")
     lm = sub.add_parser("lmm")
@@ -125,6 +136,7 @@ def main(argv=None) -> int:
     lm.add_argument("-snps")
     lm.add_argument("-ksnps")
     lm.add_argument("-hwe", type=float, default=0.0)
+    lm.add_argument("-precision", choices=("fp64", "mixed"), default="fp64")
     lm.add_argument("--check-memory", dest="check_memory", action="store_true", default=True)
     lm.add_argument("--no-check-memory", dest="check_memory", action="store_false")
     a = ap.parse_args(argv)

@@ -44,6 +44,10 @@ inline cublasStatus_t bind_cublas(cublasHandle_t h, cudaStream_t st, void* ws, i
 
 inline int64_t ceil_div(int64_t a, int64_t b) { return (a + b - 1) / b; }
 
+// grid.y for kernels that stride one matrix column per y index: the hardware caps
+// gridDim.y at 65535, so larger n loop over columns j = blockIdx.y, + gridDim.y, ...
+inline unsigned grid_y(int64_t n) { return (unsigned)(n < 65535 ? (n > 0 ? n : 1) : 65535); }
+
 }  // namespace jb
 
 #define JB_CHECK_ARG(cond, ...)                 \

@@ -221,13 +221,14 @@ __global__ void center_f64_kernel(const int8_t* __restrict__ codes, int64_t ldc,
 }
 
 __global__ void symmetrize_scale_kernel(double* K, int64_t n, int64_t ldk, double scale) {
-    const int64_t col = blockIdx.y;
-    for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n;
-         row += (int64_t)gridDim.x * blockDim.x) {
-        if (row >= col) {
-            const double v = K[col * ldk + row] * scale;
-            K[col * ldk + row] = v;
-            if (row != col) K[row * ldk + col] = v;
+    for (int64_t col = blockIdx.y; col < n; col += gridDim.y) {
+        for (int64_t row = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; row < n;
+             row += (int64_t)gridDim.x * blockDim.x) {
+            if (row >= col) {
+                const double v = K[col * ldk + row] * scale;
+                K[col * ldk + row] = v;
+                if (row != col) K[row * ldk + col] = v;
+            }
         }
     }
 }
@@ -359,9 +360,8 @@ int32_t jb_kinship_accumulate_std_f64(const int8_t* codes, int64_t ld_codes, int
 int32_t jb_kinship_finalize(double* K, int64_t n, int64_t ldk, double scale, uintptr_t stream) {
     JB_CHECK_ARG(n >= 0 && ldk >= n, "jb_kinship_finalize: bad shape");
     if (n == 0) return JB_OK;
-    JB_CHECK_ARG(n < 65536 * 4, "jb_kinship_finalize: n too large");
     const int64_t bx = ceil_div(n, 256) < 64 ? ceil_div(n, 256) : 64;
-    dim3 grid((unsigned)bx, (unsigned)n, 1);
+    dim3 grid((unsigned)bx, grid_y(n), 1);
     symmetrize_scale_kernel<<<grid, 256, 0, as_stream(stream)>>>(K, n, ldk, scale);
     JB_LAUNCH_CHECK("symmetrize_scale_kernel");
     return JB_OK;

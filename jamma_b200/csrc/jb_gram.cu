@@ -504,16 +504,17 @@ __device__ __forceinline__ void mu_digits(double mu, int8_t (&d)[4]) {
 
 // B (4n x ldb, K-major): B[(4k + t) * ldb + j] = d_t(mu_j) if sample k is missing at SNP j
 // (bit j of k's missing-SNP mask).
-__global__ void kin_rmask_kernel(const uint32_t* __restrict__ mask, int64_t words, int64_t m,
-                                 const double* __restrict__ mu, int8_t* __restrict__ B,
+__global__ void kin_rmask_kernel(const uint32_t* __restrict__ mask, int64_t words, int64_t n,
+                                 int64_t m, const double* __restrict__ mu, int8_t* __restrict__ B,
                                  int64_t ldb) {
-    const int64_t k = blockIdx.y;
-    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < ldb;
-         j += (int64_t)gridDim.x * blockDim.x) {
-        int8_t d[4] = {0, 0, 0, 0};
-        if (j < m && ((__ldg(mask + k * words + (j >> 5)) >> (j & 31)) & 1u)) mu_digits(mu[j], d);
+    for (int64_t k = blockIdx.y; k < n; k += gridDim.y) {
+        for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < ldb;
+             j += (int64_t)gridDim.x * blockDim.x) {
+            int8_t d[4] = {0, 0, 0, 0};
+            if (j < m && ((__ldg(mask + k * words + (j >> 5)) >> (j & 31)) & 1u)) mu_digits(mu[j], d);
 #pragma unroll
-        for (int t = 0; t < 4; ++t) B[(4 * k + t) * ldb + j] = d[t];
+            for (int t = 0; t < 4; ++t) B[(4 * k + t) * ldb + j] = d[t];
+        }
     }
 }
 
@@ -552,15 +553,16 @@ __global__ void kin_finalize_i8_kernel(const int32_t* __restrict__ C, int64_t ld
                                        const double* __restrict__ a, const double* __restrict__ b,
                                        double s, const double* __restrict__ RT, int64_t ldr,
                                        double inv_p, double* __restrict__ K, int64_t ldk) {
-    const int64_t j = blockIdx.y;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= j && i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        // the int32 Gram holds the upper triangle (row i <= column j) at C[j*ldc + i]
-        double v = (double)C[j * ldc + i] - a[i] - a[j] + s - b[i] - b[j];
-        if (RT) v += RT[j * ldr + i] + RT[i * ldr + j];
-        v *= inv_p;
-        K[j * ldk + i] = v;
-        K[i * ldk + j] = v;
+    for (int64_t j = blockIdx.y; j < n; j += gridDim.y) {
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= j && i < n;
+             i += (int64_t)gridDim.x * blockDim.x) {
+            // the int32 Gram holds the upper triangle (row i <= column j) at C[j*ldc + i]
+            double v = (double)C[j * ldc + i] - a[i] - a[j] + s - b[i] - b[j];
+            if (RT) v += RT[j * ldr + i] + RT[i * ldr + j];
+            v *= inv_p;
+            K[j * ldk + i] = v;
+            K[i * ldk + j] = v;
+        }
     }
 }
 
@@ -574,17 +576,18 @@ __global__ void kin_finalize_loco_kernel(const int32_t* __restrict__ Cf, const i
                                          const double* __restrict__ Qf,
                                          const double* __restrict__ Qc, int64_t ldq, double inv_p,
                                          double* __restrict__ K, int64_t ldk) {
-    const int64_t j = blockIdx.y;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= j && i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        const int32_t g = Cf[j * ldc + i] - Cc[j * ldc + i];
-        const double ai = af[i] - ac[i], aj = af[j] - ac[j];
-        const double bi = bf[i] - bc[i], bj = bf[j] - bc[j];
-        double v = (double)g - ai - aj + s - bi - bj;
-        if (Qf) v += (Qf[j * ldq + i] + Qf[i * ldq + j]) - (Qc[j * ldq + i] + Qc[i * ldq + j]);
-        v *= inv_p;
-        K[j * ldk + i] = v;
-        K[i * ldk + j] = v;
+    for (int64_t j = blockIdx.y; j < n; j += gridDim.y) {
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i <= j && i < n;
+             i += (int64_t)gridDim.x * blockDim.x) {
+            const int32_t g = Cf[j * ldc + i] - Cc[j * ldc + i];
+            const double ai = af[i] - ac[i], aj = af[j] - ac[j];
+            const double bi = bf[i] - bc[i], bj = bf[j] - bc[j];
+            double v = (double)g - ai - aj + s - bi - bj;
+            if (Qf) v += (Qf[j * ldq + i] + Qf[i * ldq + j]) - (Qc[j * ldq + i] + Qc[i * ldq + j]);
+            v *= inv_p;
+            K[j * ldk + i] = v;
+            K[i * ldk + j] = v;
+        }
     }
 }
 
@@ -592,13 +595,14 @@ __global__ void kin_finalize_loco_kernel(const int32_t* __restrict__ Cf, const i
 __global__ void kin_sub_scale_kernel(const double* __restrict__ Sf, const double* __restrict__ Sc,
                                      int64_t n, int64_t lds, double scale, double* __restrict__ K,
                                      int64_t ldk) {
-    const int64_t j = blockIdx.y;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-        if (i >= j) {
-            const double v = (Sf[j * lds + i] - Sc[j * lds + i]) * scale;
-            K[j * ldk + i] = v;
-            K[i * ldk + j] = v;
+    for (int64_t j = blockIdx.y; j < n; j += gridDim.y) {
+        for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+             i += (int64_t)gridDim.x * blockDim.x) {
+            if (i >= j) {
+                const double v = (Sf[j * lds + i] - Sc[j * lds + i]) * scale;
+                K[j * ldk + i] = v;
+                K[i * ldk + j] = v;
+            }
         }
     }
 }
@@ -702,8 +706,7 @@ int32_t jb_kinship_i8_finalize_loco(const int32_t* C_full, const int32_t* C_chr,
     JB_CHECK_ARG(n > 0 && ldc >= n && ldk >= n && p_loco > 0, "jb_kinship_i8_finalize_loco: bad shape");
     JB_CHECK_ARG((Q_full == nullptr) == (Q_chr == nullptr) && (!Q_full || ldq >= n),
                  "jb_kinship_i8_finalize_loco: Q_full and Q_chr go together");
-    JB_CHECK_ARG(n < 65536 * 4, "jb_kinship_i8_finalize_loco: n too large");
-    dim3 grid((unsigned)(ceil_div(n, 256) < 64 ? ceil_div(n, 256) : 64), (unsigned)n, 1);
+    dim3 grid((unsigned)(ceil_div(n, 256) < 64 ? ceil_div(n, 256) : 64), grid_y(n), 1);
     kin_finalize_loco_kernel<<<grid, 256, 0, as_stream(stream)>>>(
         C_full, C_chr, ldc, n, a_full, a_chr, b_full, b_chr, sum_mu2_loco, Q_full, Q_chr, ldq,
         1.0 / (double)p_loco, K, ldk);
@@ -714,8 +717,7 @@ int32_t jb_kinship_i8_finalize_loco(const int32_t* C_full, const int32_t* C_chr,
 int32_t jb_kinship_loco_f64(const double* S_full, const double* S_chr, int64_t n, int64_t lds,
                             int64_t p_loco, double* K, int64_t ldk, uintptr_t stream) {
     JB_CHECK_ARG(n > 0 && lds >= n && ldk >= n && p_loco > 0, "jb_kinship_loco_f64: bad shape");
-    JB_CHECK_ARG(n < 65536 * 4, "jb_kinship_loco_f64: n too large");
-    dim3 grid((unsigned)(ceil_div(n, 256) < 64 ? ceil_div(n, 256) : 64), (unsigned)n, 1);
+    dim3 grid((unsigned)(ceil_div(n, 256) < 64 ? ceil_div(n, 256) : 64), grid_y(n), 1);
     kin_sub_scale_kernel<<<grid, 256, 0, as_stream(stream)>>>(S_full, S_chr, n, lds,
                                                              1.0 / (double)p_loco, K, ldk);
     JB_LAUNCH_CHECK("kin_sub_scale_kernel");
@@ -734,6 +736,14 @@ int32_t jb_gram_i8_noalloc(const int8_t* Zs, int64_t n, int64_t p, int64_t ldz, 
     const int32_t rc = noalloc_scratch(&scratch);
     if (rc) return rc;
     return jb_gram_i8(Zs, n, p, ldz, C, ldc, scratch, kNoAllocScratchBytes, stream);
+}
+
+int32_t jb_gram_i8_noalloc_status(int32_t* out, uintptr_t stream) {
+    JB_CHECK_ARG(out, "jb_gram_i8_noalloc_status: null pointer");
+    void* scratch = nullptr;
+    const int32_t rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    return jb_gram_status(scratch, out, stream);
 }
 
 int32_t jb_gram_status(const void* workspace, int32_t* out, uintptr_t stream) {
@@ -902,8 +912,8 @@ int32_t jb_kinship_i8_corrections_tc(const int8_t* codes, int64_t ld_codes, cons
     rc = kin_masks(codes, ld_codes, n, m, L, ws, st);
     if (rc) return rc;
     int8_t* B = reinterpret_cast<int8_t*>(ws + L.B);
-    kin_rmask_kernel<<<dim3((unsigned)ceil_div(L.ldb, 256), (unsigned)n), 256, 0, st>>>(
-        reinterpret_cast<const uint32_t*>(ws + L.mask), L.words, m, mu, B, L.ldb);
+    kin_rmask_kernel<<<dim3((unsigned)ceil_div(L.ldb, 256), grid_y(n)), 256, 0, st>>>(
+        reinterpret_cast<const uint32_t*>(ws + L.mask), L.words, n, m, mu, B, L.ldb);
     JB_LAUNCH_CHECK("kin_rmask_kernel");
     const int MB = (int)ceil_div(n, kBM), NB = (int)ceil_div(4 * n, 256);
     Tile* tiles = reinterpret_cast<Tile*>(ws + L.tiles);
@@ -929,8 +939,7 @@ int32_t jb_kinship_i8_finalize(const int32_t* C, int64_t ldc, int64_t n, const d
                                const double* b, double sum_mu2, const double* RT, int64_t ldr,
                                int64_t p_kept, double* K, int64_t ldk, uintptr_t stream) {
     JB_CHECK_ARG(n > 0 && ldc >= n && ldk >= n && p_kept > 0, "jb_kinship_i8_finalize: bad shape");
-    JB_CHECK_ARG(n < 65536 * 4, "jb_kinship_i8_finalize: n too large");
-    dim3 grid((unsigned)(ceil_div(n, 256) < 64 ? ceil_div(n, 256) : 64), (unsigned)n, 1);
+    dim3 grid((unsigned)(ceil_div(n, 256) < 64 ? ceil_div(n, 256) : 64), grid_y(n), 1);
     kin_finalize_i8_kernel<<<grid, 256, 0, as_stream(stream)>>>(C, ldc, n, a, b, sum_mu2, RT, ldr,
                                                                1.0 / (double)p_kept, K, ldk);
     JB_LAUNCH_CHECK("kin_finalize_i8_kernel");

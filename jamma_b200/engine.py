@@ -193,8 +193,11 @@ class DeviceCohort:
         return self.associate_rotated(UtG, out)
 
     def rotate_codes_i8(self, codes: torch.Tensor, means: torch.Tensor, has_missing: bool,
-                        out: torch.Tensor | None = None) -> torch.Tensor:
-        """Mixed form: INT8 tensor-core rotation of decoded codes -> U^T G (m, n) FP64."""
+                        out: torch.Tensor | None = None, after_rotation=None) -> torch.Tensor:
+        """Mixed form: INT8 tensor-core rotation of decoded codes -> U^T G (m, n) FP64.
+
+        ``after_rotation`` (optional callable) runs between the rotation GEMM and the
+        series-sum GEMM, e.g. to record a CUDA event that times the rotation alone."""
         m, ld = codes.shape
         need = _native.load().jb_rotate_i8_workspace_size(self.n, m)
         if self._rot_ws is None or self._rot_ws.numel() < need:
@@ -203,6 +206,8 @@ class DeviceCohort:
         _native.call("jb_rotate_i8", ptr(self.ozaki), self.n, ptr(codes), ld, m, ptr(means),
                      int(bool(has_missing)), ptr(out), self.n, ptr(self._rot_ws),
                      self._rot_ws.numel(), stream_handle())
+        if after_rotation is not None:
+            after_rotation()
         self._series_for = None
         if self.series_ws is not None:
             cws = self.chunk_workspace(m)

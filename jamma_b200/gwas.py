@@ -44,7 +44,20 @@ def gwas(bfile, *, kinship_file=None, covariate_file=None, lmm_mode: int = 1, ma
          miss: float = 0.05, output_dir="output", output_prefix: str = "result",
          save_kinship: bool = False, check_memory: bool = True, show_progress: bool = True,
          loco: bool = False, eigenvalue_file=None, eigenvector_file=None, write_eigen: bool = False,
-         phenotype_column: int = 1, snps_file=None, ksnps_file=None, hwe: float = 0.0) -> GWASResult:
+         phenotype_column: int = 1, snps_file=None, ksnps_file=None, hwe: float = 0.0,
+         precision: str = "fp64") -> GWASResult:
+    """Kinship (or eigen files), then the streaming association written to
+    ``{output_dir}/{output_prefix}.assoc.txt``, with jamma's arguments and defaults.
+
+    ``precision`` picks the form of every device step: ``"fp64"`` (default) is FP64
+    throughout and reproduces jamma's results; ``"mixed"`` computes the kinship with the
+    exact INT8 tensor-core Gram plus FP64 corrections, rotates genotypes on the INT8
+    tensor cores (four base-254 digit planes of the eigenvectors, exact int32 products) and
+    runs the series-interpolated lambda search, with FP64 likelihoods and statistics.
+    """
+    if precision not in ("fp64", "mixed"):
+        raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
+    kin_precision = "int8" if precision == "mixed" else "fp64"
     if lmm_mode not in (1, 2, 3, 4):
         raise ValueError(f"lmm_mode must be 1, 2, 3 or 4, got {lmm_mode}")
     if loco and kinship_file is not None:
@@ -78,7 +91,7 @@ def gwas(bfile, *, kinship_file=None, covariate_file=None, lmm_mode: int = 1, ma
         if kinship_file is not None:
             K = read_kinship_matrix(kinship_file, n_samples=n)
         else:
-            K = compute_kinship_from_bed(bfile, ksnps_indices=ks)
+            K = compute_kinship_from_bed(bfile, ksnps_indices=ks, precision=kin_precision)
             if save_kinship:
                 write_kinship_matrix(K, Path(output_dir) / f"{output_prefix}.cXX.txt")
         if write_eigen:  # eigen files of the analysed samples (pipeline.py:549-566)
@@ -97,7 +110,8 @@ def gwas(bfile, *, kinship_file=None, covariate_file=None, lmm_mode: int = 1, ma
         res = run_lmm_loco(bfile, y, covariates=cov, maf_threshold=maf, miss_threshold=miss,
                            lmm_mode=lmm_mode, output_path=out, save_kinship=save_kinship,
                            kinship_output_dir=Path(output_dir), kinship_output_prefix=output_prefix,
-                           snps_indices=snps_idx, ksnps_indices=ks)
+                           snps_indices=snps_idx, ksnps_indices=ks, precision=precision,
+                           kinship_precision=kin_precision)
         t_end = time.perf_counter()
         n_valid = int(np.sum(~np.isnan(y) & (y != -9.0)))
         return GWASResult(res, n_valid, meta["n_snps"],
@@ -105,7 +119,7 @@ def gwas(bfile, *, kinship_file=None, covariate_file=None, lmm_mode: int = 1, ma
     res = run_lmm_association_streaming(
         bfile, y, kinship=K, covariates=cov, eigenvalues=evals, eigenvectors=evecs,
         maf_threshold=maf, miss_threshold=miss, output_path=out, lmm_mode=lmm_mode,
-        snps_indices=snps_idx, hwe_threshold=hwe, timing=timing)
+        snps_indices=snps_idx, hwe_threshold=hwe, timing=timing, precision=precision)
     t_end = time.perf_counter()
     n_valid = int(np.sum(~np.isnan(y) & (y != -9.0)))
     return GWASResult(res, n_valid, meta["n_snps"],

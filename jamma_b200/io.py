@@ -80,6 +80,32 @@ class BedFile:
     def take(self, idx: np.ndarray) -> np.ndarray:
         return np.ascontiguousarray(self.records[np.asarray(idx)])
 
+    def take_into(self, idx: np.ndarray, out: np.ndarray) -> None:
+        """Copy the records of SNPs ``idx`` into ``out`` (len(idx), bytes_per_snp), e.g. a
+        pinned staging buffer, without an intermediate array."""
+        np.take(self.records, np.asarray(idx), axis=0, out=out)
+
+
+def write_plink_records(prefix, records: np.ndarray, n_samples: int, chrom=None,
+                        phenotypes=None) -> None:
+    """Write a .bed/.bim/.fam triple from packed SNP-major records (p, ceil(n/4)) --
+    e.g. records already in the device layout -- without decoding them."""
+    records = np.ascontiguousarray(records, dtype=np.uint8)
+    p, bps = records.shape
+    if bps != (n_samples + 3) // 4:
+        raise ValueError(f"records have {bps} bytes per SNP; {n_samples} samples need "
+                         f"{(n_samples + 3) // 4}")
+    with open(f"{prefix}.bed", "wb") as f:
+        f.write(BED_MAGIC)
+        records.tofile(f)
+    with open(f"{prefix}.bim", "w") as f:
+        f.writelines(f"{chrom[j] if chrom is not None else 1}\trs{j:07d}\t0\t{1000 * (j + 1)}\tA\tG\n"
+                     for j in range(p))
+    with open(f"{prefix}.fam", "w") as f:
+        f.writelines(f"FAM{i:06d}\tIND{i:06d}\t0\t0\t0\t"
+                     f"{'-9' if phenotypes is None else repr(float(phenotypes[i]))}\n"
+                     for i in range(n_samples))
+
 
 def encode_codes(genotypes: np.ndarray) -> np.ndarray:
     """(n, p) float genotypes -> (p, n) int8 codes: 0/1/2, 3 = missing (NaN).

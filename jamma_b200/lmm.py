@@ -92,15 +92,19 @@ class _Stats:
 
 
 def _build_results(mode: int, snp_idx, af, n_miss, snp_info, arrays, f: int = 0):
+    """One AssocResult per tested SNP (``_build_results_*``, src/jamma/lmm/results.py:37-286)."""
+    cols = {field: arrays[key][f].tolist() for key, field in _FIELD.items()
+            if key in arrays and not (mode == 2 and field in ("beta", "se"))}
+    af_l, miss_l = np.asarray(af, dtype=np.float64).tolist(), np.asarray(n_miss).astype(int).tolist()
+    nan = float("nan")
     out = []
-    for k, j in enumerate(snp_idx):
+    for k, j in enumerate(np.asarray(snp_idx).tolist()):
         s = snp_info[j]
-        kw = dict(chr=s["chr"], rs=s["rs"], ps=s.get("pos", s.get("ps", 0)), n_miss=int(n_miss[k]),
+        kw = dict(chr=s["chr"], rs=s["rs"], ps=s.get("pos", s.get("ps", 0)), n_miss=miss_l[k],
                   allele1=s.get("a1", s.get("allele1", "")), allele0=s.get("a0", s.get("allele0", "")),
-                  af=float(af[k]), beta=float("nan"), se=float("nan"))
-        for key, field in _FIELD.items():
-            if key in arrays and not (mode == 2 and field in ("beta", "se")):
-                kw[field] = float(arrays[key][f, k])
+                  af=af_l[k], beta=nan, se=nan)
+        for field, v in cols.items():
+            kw[field] = v[k]
         out.append(AssocResult(**kw))
     return out
 
@@ -110,27 +114,88 @@ def associate_records(cohort: eng.DeviceCohort, records, n_file: int, sample_idx
                       n_miss: np.ndarray | None = None) -> dict[str, np.ndarray]:
     """Run the association for packed .bed records (m, bytes_per_snp) of kept SNPs.
 
-    ``records`` is a host uint8 array (or a callable ``records(s, e)`` returning rows
-    s..e); ``means`` are the per-SNP imputation values.  Returns (phi, m) arrays.
+    ``records`` is a host uint8 array, or a callable ``records(s, e, out)`` that writes
+    rows s..e into the (e - s, bytes_per_snp) uint8 array ``out``; ``means`` are the
+    per-SNP imputation values.  Returns (phi, m) arrays.
+
+    The chunks stream through the device as the device loop of
+    src/jamma/lmm/runner_streaming.py:412-586 does, with every stage overlapped:
+
+    * the chunk's whole device pipeline (decode, rotation, series sums, search and
+      statistics) is captured once as a CUDA graph (:class:`engine.ChunkGraph`) and
+      replayed per chunk on the caller's stream;
+    * the host reads chunk k+1's records into one of two pinned buffers while the GPU
+      replays chunk k, and their host-to-device copy runs on a side stream into one of two
+      device staging buffers; the replay stream takes the staged chunk with one
+      device-to-device copy into the graph's input buffers;
+    * results return by asynchronous copies into pinned buffers and are collected on the
+      host one chunk behind, so the GPU always has the next chunk queued.
     """
     m = len(means)
-    step = device_chunk or device_chunk_for(cohort.n)
+    res = {k: np.empty((cohort.phi, m)) for k in eng.MODE_KEYS[cohort.mode]}
+    if m == 0:
+        return res
+    step = min(int(device_chunk or device_chunk_for(cohort.n)), m)
+    bps = (n_file + 3) // 4
     sidx = None if sample_idx is None else torch.from_numpy(
         np.asarray(sample_idx, dtype=np.int32)).to("cuda")
-    res = {k: np.empty((cohort.phi, m)) for k in eng.MODE_KEYS[cohort.mode]}
-    bufs = {"G": eng.empty((step, cohort.n)), "UtG": eng.empty((step, cohort.n))}
-    for s in range(0, m, step):
-        e = min(s + step, m)
-        rec = records(s, e) if callable(records) else records[s:e]
-        rec_d = torch.from_numpy(np.ascontiguousarray(rec)).to("cuda", non_blocking=False)
-        codes, _ = eng.decode_packed(rec_d, n_file, sidx, cohort.n, ld=cohort.code_ld)
-        mu = torch.from_numpy(np.asarray(means[s:e], dtype=np.float64)).to("cuda")
-        miss = True if n_miss is None else bool(np.any(n_miss[s:e] > 0))
-        out = cohort.associate_codes(codes, mu, bufs=bufs, has_missing=miss)
-        for k, v in out.items():
-            res[k][:, s:e] = v.cpu().numpy()
+    means = np.asarray(means, dtype=np.float64)
+    has_missing = True if n_miss is None else bool(np.any(np.asarray(n_miss) > 0))
+    main = torch.cuda.current_stream()
+    side = torch.cuda.Stream()
+    graph = eng.ChunkGraph(cohort, step, n_file, sidx, has_missing=has_missing)
+    pin_rec = [torch.empty((step, bps), dtype=torch.uint8, pin_memory=True) for _ in range(2)]
+    pin_mu = [torch.empty((step,), dtype=torch.float64, pin_memory=True) for _ in range(2)]
+    dev_rec = [torch.empty((step, bps), dtype=torch.uint8, device="cuda") for _ in range(2)]
+    dev_mu = [torch.empty((step,), dtype=torch.float64, device="cuda") for _ in range(2)]
+    pin_out = [{k: torch.empty((cohort.phi, step), dtype=torch.float64, pin_memory=True)
+                for k in graph.out} for _ in range(2)]
+    copied = [None, None]    # side stream: pinned buffer b read, staging buffer b filled
+    consumed = [None, None]  # replay stream: staging buffer b copied into the graph inputs
+    returned = [None, None]  # replay stream: results of the chunk in buffer b are in pin_out[b]
+
+    def collect(b: int, s: int, e: int) -> None:
+        returned[b].synchronize()
+        for k, v in pin_out[b].items():
+            res[k][:, s:e] = v[:, : e - s].numpy()
         if on_chunk is not None:
             on_chunk(s, e)
+
+    pending = None
+    for ci, s in enumerate(range(0, m, step)):
+        e = min(s + step, m)
+        b, rows = ci % 2, e - s
+        if copied[b] is not None:
+            copied[b].synchronize()  # chunk ci-2's upload has read pin_rec[b]
+        if callable(records):
+            records(s, e, pin_rec[b].numpy()[:rows])
+        else:
+            pin_rec[b].numpy()[:rows] = records[s:e]
+        pin_mu[b].numpy()[:rows] = means[s:e]
+        with torch.cuda.stream(side):
+            if consumed[b] is not None:
+                side.wait_event(consumed[b])
+            dev_rec[b][:rows].copy_(pin_rec[b][:rows], non_blocking=True)
+            dev_mu[b][:rows].copy_(pin_mu[b][:rows], non_blocking=True)
+            copied[b] = torch.cuda.Event()
+            copied[b].record(side)
+        main.wait_event(copied[b])
+        graph.packed[:rows].copy_(dev_rec[b][:rows], non_blocking=True)
+        graph.means[:rows].copy_(dev_mu[b][:rows], non_blocking=True)
+        consumed[b] = torch.cuda.Event()
+        consumed[b].record(main)
+        out = graph.replay()
+        for k, v in out.items():
+            pin_out[b][k][:, :rows].copy_(v[:, :rows], non_blocking=True)
+        returned[b] = torch.cuda.Event()
+        returned[b].record(main)
+        if pending is not None:
+            collect(*pending)
+        pending = (b, s, e)
+    collect(*pending)
+    if cohort.precision == "mixed" and (status := cohort.rotate_status()):
+        raise RuntimeError(f"INT8 rotation pipeline reported status {status} (a bounded "
+                           "tensor-core pipeline wait ran out)")
     return res
 
 
@@ -202,7 +267,8 @@ def run_lmm_association_streaming(
                              n_grid, n_refine, precision)
     torch.cuda.synchronize()
     t2 = time.perf_counter()
-    res = associate_records(cohort, lambda a, b: bed.take(st.idx[a:b]), n_file, sample_idx,
+    res = associate_records(cohort, lambda a, b, out: bed.take_into(st.idx[a:b], out), n_file,
+                            sample_idx,
                             st.mean[st.idx].astype(np.float64), n_miss=st.miss[st.idx])
     t3 = time.perf_counter()
     results = _build_results(lmm_mode, st.idx, st.af[st.idx], st.miss[st.idx], snp_info, res)

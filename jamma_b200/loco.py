@@ -181,7 +181,8 @@ def run_lmm_loco(bed_path, phenotypes: np.ndarray, covariates: np.ndarray | None
                 continue
             cohort = eng.DeviceCohort(evals, U, cov, yv, lmm_mode, precision=precision)
             glob = cols[st.idx]
-            res = associate_records(cohort, lambda a, b: bed.take(glob[a:b]), n_file, sample_idx,
+            res = associate_records(cohort, lambda a, b, out: bed.take_into(glob[a:b], out), n_file,
+                                    sample_idx,
                                     st.mean[st.idx].astype(np.float64), n_miss=st.miss[st.idx])
             chr_results = _build_results(lmm_mode, glob, st.af[st.idx], st.miss[st.idx], snp_info, res)
             if writer:

@@ -279,7 +279,17 @@ class GwasServer:
             act, fut = item
             if fut.done():
                 self.preparing.remove(item)
-                fut.result()  # re-raises a set-up failure here
+                try:
+                    fut.result()  # re-raises a set-up failure here
+                except BaseException:
+                    # give back the job's reservation so that a server which catches the
+                    # error and keeps running admits and evicts as before
+                    self.used -= act.bytes
+                    with self._lock:
+                        res = self.cohorts.get(act.job.cohort_id)
+                        if res is not None:
+                            res.refs -= 1
+                    raise
                 act.job.ready = time.perf_counter()
                 self.active.append(act)
                 busy = True

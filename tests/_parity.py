@@ -67,3 +67,26 @@ def assert_mixed_parity(got: dict, ref: dict, keys):
         assert dlog.max() < 1e-4, f"{k}: |dlog10 p| {dlog.max():.2e}"
         for t in (0.05, 1e-3, 5e-8):
             np.testing.assert_array_equal(a < t, b < t, err_msg=f"{k}: calls at {t}")
+
+
+def strict_fp64_report(got: dict, ref: dict, keys=("beta", "se", "logl_h1", "p_wald"),
+                       lam_key: str = "lambda_remle", lam_tol: float = 1e-12,
+                       tol: float = 1e-10) -> dict:
+    """The plain FP64 form at the north-star tolerance: on every SNP whose REML lambda
+    matches the oracle's to ``lam_tol`` relative (every golden-section decision taken the
+    same way), each field in ``keys`` must agree to ``tol`` relative.  Returns the fraction
+    of SNPs that qualify and the worst error among them per field."""
+    la, lb = np.asarray(got[lam_key], float), np.asarray(ref[lam_key], float)
+    same = np.isfinite(la) & np.isfinite(lb) & (_rel(la, lb) <= lam_tol)
+    out = {"frac_lambda_matched": float(np.mean(same)), "n": int(same.size)}
+    for k in keys:
+        if k not in got or k not in ref:
+            continue
+        a, b = np.asarray(got[k], float)[same], np.asarray(ref[k], float)[same]
+        ok = np.isfinite(a) & np.isfinite(b)
+        np.testing.assert_array_equal(np.isfinite(a), np.isfinite(b), err_msg=f"{k}: NaN pattern")
+        r = _rel(a[ok], b[ok])
+        worst = float(r.max()) if r.size else 0.0
+        out[k] = worst
+        assert worst <= tol, f"{k}: {worst:.3e} > {tol} on a SNP whose lambda matches the oracle"
+    return out

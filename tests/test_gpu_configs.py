@@ -36,6 +36,7 @@ import torch
 from jamma_b200 import synth
 from oracle import lmm as OL
 from oracle import plink as OP
+from _parity import strict_fp64_report
 
 pytestmark = pytest.mark.gpu
 
@@ -111,16 +112,18 @@ def test_forms_against_oracle_and_each_other(name):
     cov = synth.covariates(n, c - 1, seed=seed + 3) if c > 1 else None
     mu32 = np.nanmean(g.astype(np.float32), axis=0).astype(np.float64)
     packed = OP.encode_genotypes(g)
-    forms = {}
+    forms, null = {}, {}
     for precision in ("mixed", "fp64"):
         cohort = eng.DeviceCohort(w, U, cov, Y if phi > 1 else Y[:, 0], lmm_mode=mode,
                                   precision=precision)
+        null[precision] = cohort.null_model()[0]
         assert cohort.search == (1 if precision == "mixed" else 0)
         forms[precision] = associate_records(cohort, packed, n, None, mu32, device_chunk=512,
                                              n_miss=np.isnan(g).sum(0))
         if precision == "mixed":
             assert cohort.rotate_status() == 0
     tables = {"mixed vs fp64 form": {}, "mixed vs oracle": {}, "fp64 form vs oracle": {}}
+    strict_tables: dict = {}
     for f in range(phi):
         ref = OL.lmm_association(g, Y[:, f], eigenvalues=w, eigenvectors=U, covariates=cov,
                                  lmm_mode=mode, maf_threshold=0.0, miss_threshold=1.0)
@@ -130,5 +133,26 @@ def test_forms_against_oracle_and_each_other(name):
         _compare(mixed, plain, tables["mixed vs fp64 form"], "strict", name)
         _compare(mixed, ref.stats, tables["mixed vs oracle"], "oracle", name)
         _compare(plain, ref.stats, tables["fp64 form vs oracle"], "oracle", name)
+        # the plain form at the north-star tolerance (1e-10) wherever its lambda matches
+        # the oracle's, i.e. every golden-section decision went the same way
+        strict = strict_tables.setdefault(f, {})
+        if mode in (1, 4):
+            strict["reml"] = strict_fp64_report(plain, ref.stats)
+        if mode in (2, 4):
+            strict["mle"] = strict_fp64_report(plain, ref.stats, keys=("logl_mle", "p_lrt"),
+                                               lam_key="lambda_mle")
+        if mode in (3, 4):
+            lam0 = float(null["fp64"][f])
+            strict["null_lambda_rel"] = abs(lam0 - ref.lam0) / ref.lam0
+            if strict["null_lambda_rel"] <= 1e-12:
+                a, b = np.asarray(plain["p_score"]), ref.stats["p_score"]
+                ok = np.isfinite(a) & np.isfinite(b)
+                worst = float((np.abs(a[ok] - b[ok]) / np.abs(b[ok])).max())
+                strict["p_score"] = worst
+                assert worst <= 1e-10, f"{name} p_score {worst:.2e} with the oracle's lambda0"
+    for rep in strict_tables.values():
+        for part in ("reml", "mle"):
+            if part in rep:  # most decisions must match: a near tie is the exception
+                assert rep[part]["frac_lambda_matched"] >= 0.8, f"{name} {part}: {rep[part]}"
     _TABLE[name] = {"n": n, "snps": p, "n_cvt": c, "phenotypes": phi, "lmm_mode": mode,
-                    "comparisons": tables}
+                    "comparisons": tables, "fp64_form_strict": strict_tables}

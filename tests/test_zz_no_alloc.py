@@ -49,6 +49,9 @@ def test_noalloc_gram_matches_workspace_gram_on_consecutive_calls(lib):
         lib.call("jb_gram_i8", ptr(Zd), n, p, ldz, ptr(ref), n, ptr(ws), ws.numel(), st)
         got = torch.full((n, n), -1, dtype=torch.int32, device="cuda")
         lib.call("jb_gram_i8_noalloc", ptr(Zd), n, p, ldz, ptr(got), n, st)
+        status = np.full(1, -1, dtype=np.int32)  # the pipeline status word in the static scratch
+        lib.call("jb_gram_i8_noalloc_status", status.ctypes.data, st)
+        assert status[0] == 0, f"no-alloc Gram pipeline status {status[0]}"
         torch.cuda.synchronize()
         iu = np.triu_indices(n)
         g = got.cpu().numpy().T  # column-major: (i, j), i <= j, at [j*n + i]
