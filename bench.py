@@ -333,30 +333,37 @@ def _e2e_streaming(args, w, U, W, y, packed_host: np.ndarray) -> dict:
 def run_serving(args, seed: int = 7) -> dict:
     """A Poisson stream of GWAS jobs through the continuous-batching server.
 
-    Scaled-down version of the serving configuration (200 jobs, n up to 40 000) so the
-    default bench stays within minutes: ``args.serve_jobs`` jobs, n ~ log-uniform in
-    [2 000, 8 000], SNPs ~ log-uniform in [10 000, 40 000], 1-4 phenotypes, lmm mode
-    drawn from {1, 2, 3, 4}, 30 % of jobs reusing a resident cohort's eigenvectors.
+    Default: a reduced version of the serving configuration so that the default bench
+    stays within minutes -- ``args.serve_jobs`` jobs, n ~ log-uniform in [2 000, 8 000],
+    SNPs ~ log-uniform in [10 000, 40 000], 1-4 phenotypes.  ``--serve-c4``: the serving
+    configuration itself -- 200 jobs, n ~ log-uniform in [2 000, 40 000], SNPs ~
+    log-uniform in [10 000, 200 000], 1-8 phenotypes.  Both: lmm mode drawn from
+    {1, 2, 3, 4}, 30 % of jobs reusing a resident cohort's eigenvectors, 1 % missing calls.
     """
     import torch
 
     from jamma_b200 import synth
     from jamma_b200.serve import GwasJob, GwasServer
 
+    c4 = args.serve_c4
+    n_jobs = 200 if c4 else args.serve_jobs
+    n_lo, n_hi = (2000, 40000) if c4 else (2000, 8000)
+    p_lo, p_hi = (10000, 200000) if c4 else (10000, 40000)
+    phi_hi = 8 if c4 else 4
     rng = np.random.default_rng(seed)
     cohorts = {}
     jobs = []
     t = 0.0
-    for i in range(args.serve_jobs):
+    for i in range(n_jobs):
         if cohorts and rng.random() < 0.3:
             cid = list(cohorts)[rng.integers(len(cohorts))]
         else:
             cid = f"c{i}"
-            n = int(np.exp(rng.uniform(np.log(2000), np.log(8000))))
-            p = int(np.exp(rng.uniform(np.log(10000), np.log(40000))))
+            n = int(np.exp(rng.uniform(np.log(n_lo), np.log(n_hi))))
+            p = int(np.exp(rng.uniform(np.log(p_lo), np.log(p_hi))))
             cohorts[cid] = (n, synth.packed_records_device(n, p, 0.01, seed=5000 + i).cpu().numpy())
         n, packed = cohorts[cid]
-        phi = int(rng.integers(1, 5))
+        phi = int(rng.integers(1, phi_hi + 1))
         y = rng.normal(size=(n, phi))
         cov = np.column_stack([np.ones(n), rng.normal(size=n)]) if rng.random() < 0.5 else None
         t += rng.exponential(args.serve_gap)
@@ -365,11 +372,18 @@ def run_serving(args, seed: int = 7) -> dict:
     srv = GwasServer(hbm_budget_bytes=int(args.serve_budget_gb * (1 << 30)), max_active=4,
                      chunk=4096)
     torch.cuda.synchronize()
+    t0 = time.perf_counter()
     srv.run(jobs)
+    wall = time.perf_counter() - t0
     out = srv.latency_summary()
-    out.update(workload=f"{args.serve_jobs} jobs, Poisson gaps {args.serve_gap}s, n 2k-8k, "
-                        f"SNPs 10k-40k, 1-4 phenotypes, modes 1-4, 30% cohort reuse",
-               hbm_budget_gb=args.serve_budget_gb, max_active=4)
+    total_snps = sum(j.snp_indices.size * (1 if np.ndim(j.phenotypes) == 1 else j.phenotypes.shape[1])
+                     for _, j in jobs)
+    out.update(workload=(f"{'serving configuration' if c4 else 'reduced serving mix'}: {n_jobs} jobs, "
+                         f"Poisson gaps {args.serve_gap}s, n {n_lo}-{n_hi}, SNPs {p_lo}-{p_hi}, "
+                         f"1-{phi_hi} phenotypes, modes 1-4, 30% cohort reuse"),
+               hbm_budget_gb=args.serve_budget_gb, max_active=4, wall_s=wall,
+               snp_phenotype_pairs=int(total_snps),
+               new_cohorts=int(sum(1 for _, j in jobs if j.new_cohort)))
     return out
 
 
@@ -727,6 +741,25 @@ def run_ours(args) -> None:
         dist.destroy_process_group()
 
 
+def run_serving_only(args) -> None:
+    """The serving configuration alone (``--serve-c4``): one JSON line with its latency
+    percentiles, phase split and aggregate throughput."""
+    import torch
+
+    from jamma_b200 import _build
+
+    torch.cuda.set_device(_dist()[2])
+    _build.build()
+    with ClockSampler(_dist()[2]) as clk:
+        serving = run_serving(args)
+    line = {"metric": "serving_p99_latency_s", "value": serving["p99_s"], "unit": "s",
+            "higher_is_better": False, "n_gpus": 1, "dtype": "int8+f64",
+            "data": "synthetic (seeded device RNG; Binomial(2,p) genotypes, p~U(0.05,0.5))",
+            "config": {"workload": serving["workload"]}, "clocks": clk.summary(),
+            "serving": serving}
+    print(json.dumps(line), flush=True)
+
+
 def run_loco(args) -> None:
     """LOCO at config C5's shape (n samples, `--loco-chromosomes` x `--loco-snps` SNPs):
     the INT8 LOCO kinships at full size (one full-genome Gram and one Gram per chromosome,
@@ -873,6 +906,9 @@ def main():
     ap.add_argument("--serve-jobs", type=int, default=24)
     ap.add_argument("--serve-gap", type=float, default=0.2)
     ap.add_argument("--serve-budget-gb", type=float, default=60.0)
+    ap.add_argument("--serve-c4", action="store_true",
+                    help="serve the full serving configuration (200 jobs, n up to 40 000, SNPs up "
+                         "to 200 000) and print only the serving summary")
     ap.add_argument("--phenotypes", type=int, default=64,
                     help="phenotypes of the multi-phenotype sub-measurement (1 = skip)")
     ap.add_argument("--pheno-chunk", type=int, default=2048)
@@ -889,6 +925,8 @@ def main():
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
+    elif args.serve_c4:
+        run_serving_only(args)
     elif args.loco:
         run_loco(args)
     else:

@@ -176,6 +176,19 @@ int32_t jb_gram_status(const void* workspace, int32_t* out, uintptr_t stream);
 int32_t jb_gram_i8_noalloc(const int8_t* Zs, int64_t n, int64_t p, int64_t ldz, int32_t* C,
                            int64_t ldc, uintptr_t stream);
 int32_t jb_gram_i8_noalloc_status(int32_t* out, uintptr_t stream);
+
+/*
+ * Test hook of the tensor-core pipelines (no reference counterpart).  Every wait of the
+ * INT8 GEMM kernels (jb_gram_i8, jb_gram_i8_noalloc, jb_kinship_i8_corrections_tc,
+ * jb_rotate_i8 and jb_lmm_chunk_series_i8 with the one-CTA kernel) is bounded: when its
+ * deadline passes, the kernel records 100 + (the waiting role) in its status word, winds
+ * down and frees its tensor memory, so the context stays usable.  This call sets the
+ * deadline (wait_limit_ns; the default is 2 s) for later launches and, with skip_loads
+ * non-zero, makes the producer issue no tile load, so that the first MMA wait runs out
+ * with no copy or MMA in flight -- a fault-free way to test that path.  Synchronises the
+ * device.  Restore with (0, 2000000000).  Not for production use.
+ */
+int32_t jb_test_pipeline_timeout(int32_t skip_loads, int64_t wait_limit_ns);
 int32_t jb_codes_to_sample_major(const int8_t* codes, int64_t ld_codes, int64_t n,
                                  int64_t m, int8_t* Zs, int64_t ldz, int64_t col0,
                                  int8_t* Cs, int64_t ldcs, uintptr_t stream);
@@ -303,8 +316,11 @@ typedef struct jb_lmm_out {
  * src/jamma/lmm/runner_streaming.py:469-554.
  * workspace: jb_lmm_workspace_size bytes, filled by jb_lmm_prepare.
  * chunk_workspace: jb_lmm_chunk_workspace_size(n, n_cvt, phi, n_grid, m) bytes of scratch:
- * the weighted genotype sums of all m SNPs are formed there by cuBLAS DGEMMs (or, with
- * precision 2, partly by jb_lmm_chunk_series_i8) before the per-SNP kernel runs.
+ * the weighted genotype sums of all m SNPs are formed there before the per-SNP kernel runs
+ * -- the squared sums sum_i h_i x_i^2 by one fused kernel that reads each rotated genotype
+ * once and squares it on chip (FP64, fixed summation order), the linear sums by a cuBLAS
+ * DGEMM (precision 0 and 1) or by jb_lmm_chunk_series_i8 (precision 2).  The chunk's
+ * precision must match the one its workspace was prepared with (0 with 0; 1 or 2 with 1).
  * precision: 0 = every likelihood evaluation is a direct FP64 reduction over n (plain
  * form; grid, ones and null rows by DGEMM);
  * 1 = mixed form: the c+2 genotype-dependent sums are a degree-95 Chebyshev series in

@@ -77,6 +77,7 @@ SIGNATURES: dict[str, tuple] = {
     "jb_gram_status": (_i32, [_p, _p, _u]),
     "jb_gram_i8_noalloc": (_i32, [_p, _i64, _i64, _i64, _p, _i64, _u]),
     "jb_gram_i8_noalloc_status": (_i32, [_p, _u]),
+    "jb_test_pipeline_timeout": (_i32, [_i32, _i64]),
     "jb_kinship_i8_finalize_loco": (
         _i32, [_p, _p, _i64, _i64, _p, _p, _p, _p, _f64, _p, _p, _i64, _i64, _p, _i64, _u]),
     "jb_kinship_loco_f64": (_i32, [_p, _p, _i64, _i64, _i64, _p, _i64, _u]),

@@ -24,12 +24,9 @@ from pathlib import Path
 
 
 def _snp_indices(path, sid) -> "np.ndarray":
-    import numpy as np
+    from jamma_b200.io import read_snp_list_file, resolve_snp_list_to_indices
 
-    pos = {s: i for i, s in enumerate(sid)}
-    with open(path) as f:
-        ids = [line.split()[0] for line in f if line.strip()]
-    return np.array(sorted(pos[s] for s in ids if s in pos), dtype=np.int64)
+    return resolve_snp_list_to_indices(read_snp_list_file(path), sid)
 
 
 def _gk(a, command_line: str) -> None:

@@ -24,6 +24,20 @@ constexpr int kBM = 128;
 constexpr int kBK = 128;  // bytes of K per stage (one 128B swizzle row)
 constexpr int kThreads = 192;
 
+// Test hooks of the bounded pipeline waits, one copy per translation unit that launches
+// these kernels: the deadline of every wait and a switch that makes the producer issue no
+// tile load (so the MMA thread's first wait runs out, with no copy or MMA ever in flight).
+// Each kernel reads them once at start.  Set only through pipeline_test_mode (the
+// jb_test_pipeline_timeout entry point); the defaults are a 2 s deadline and loads on.
+static __device__ unsigned long long g_pipe_wait_limit_ns = kWaitLimitNs;
+static __device__ int g_pipe_skip_loads = 0;
+
+static inline cudaError_t pipeline_test_mode(int skip_loads, unsigned long long wait_limit_ns) {
+    cudaError_t e = cudaMemcpyToSymbol(g_pipe_skip_loads, &skip_loads, sizeof(int));
+    if (e != cudaSuccess) return e;
+    return cudaMemcpyToSymbol(g_pipe_wait_limit_ns, &wait_limit_ns, sizeof(wait_limit_ns));
+}
+
 template <int BN, int STAGES, int EPI_SMEM>
 struct GemmSmem {
     static constexpr int A_BYTES = kBM * kBK;
@@ -56,6 +70,8 @@ __global__ void __launch_bounds__(kThreads, 1)
 
     const int warp = threadIdx.x >> 5;
     const int lane = threadIdx.x & 31;
+    const unsigned long long wait_ns = g_pipe_wait_limit_ns;
+    const bool skip_loads = g_pipe_skip_loads != 0;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -86,11 +102,13 @@ __global__ void __launch_bounds__(kThreads, 1)
             for (int t = blockIdx.x; t < n_tiles && !*abort; t += gridDim.x) {
                 const Tile tl = tiles[t];
                 for (int kb = 0; kb < num_kb; ++kb) {
-                    if (!mbar_wait(&empty[stage], phase ^ 1, abort, err, 1)) break;
+                    if (!mbar_wait(&empty[stage], phase ^ 1, abort, err, 1, wait_ns)) break;
                     uint8_t* sa = smem + stage * S::STAGE_BYTES;
-                    mbar_expect_tx(&full[stage], S::STAGE_BYTES);
-                    tma_load_2d(sa, &tmA, &full[stage], kb * kBK, tl.mb * kBM);
-                    tma_load_2d(sa + S::A_BYTES, &tmB, &full[stage], kb * kBK, tl.nb * BN);
+                    if (!skip_loads) {
+                        mbar_expect_tx(&full[stage], S::STAGE_BYTES);
+                        tma_load_2d(sa, &tmA, &full[stage], kb * kBK, tl.mb * kBM);
+                        tma_load_2d(sa + S::A_BYTES, &tmB, &full[stage], kb * kBK, tl.nb * BN);
+                    }
                     if (++stage == STAGES) {
                         stage = 0;
                         phase ^= 1;
@@ -106,11 +124,11 @@ __global__ void __launch_bounds__(kThreads, 1)
             int acc = 0;
             uint32_t acc_phase = 0;
             for (int t = blockIdx.x; t < n_tiles && !*abort; t += gridDim.x) {
-                if (!mbar_wait(&tempty[acc], acc_phase ^ 1, abort, err, 2)) break;
+                if (!mbar_wait(&tempty[acc], acc_phase ^ 1, abort, err, 2, wait_ns)) break;
                 tc_fence_after();
                 const uint32_t d = tmem_base + (uint32_t)(acc * BN);
                 for (int kb = 0; kb < num_kb; ++kb) {
-                    if (!mbar_wait(&full[stage], phase, abort, err, 3)) break;
+                    if (!mbar_wait(&full[stage], phase, abort, err, 3, wait_ns)) break;
                     tc_fence_after();
                     const uint32_t sa = smem_u32(smem + stage * S::STAGE_BYTES);
                     const uint32_t sb = sa + S::A_BYTES;
@@ -138,7 +156,7 @@ __global__ void __launch_bounds__(kThreads, 1)
         int acc = 0;
         uint32_t acc_phase = 0;
         for (int t = blockIdx.x; t < n_tiles; t += gridDim.x) {
-            if (threadIdx.x == 64) *go = mbar_wait(&tfull[acc], acc_phase, abort, err, 4) ? 1 : 0;
+            if (threadIdx.x == 64) *go = mbar_wait(&tfull[acc], acc_phase, abort, err, 4, wait_ns) ? 1 : 0;
             asm volatile("bar.sync 1, 128;" ::: "memory");
             const int proceed = *go;
             asm volatile("bar.sync 1, 128;" ::: "memory");

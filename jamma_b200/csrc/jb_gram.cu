@@ -746,6 +746,15 @@ int32_t jb_gram_i8_noalloc_status(int32_t* out, uintptr_t stream) {
     return jb_gram_status(scratch, out, stream);
 }
 
+int32_t jb_test_pipeline_timeout(int32_t skip_loads, int64_t wait_limit_ns) {
+    JB_CHECK_ARG(wait_limit_ns > 0, "jb_test_pipeline_timeout: wait limit must be positive");
+    JB_CUDA(cudaDeviceSynchronize());  // no kernel of the old mode still running
+    const unsigned long long lim = (unsigned long long)wait_limit_ns;
+    JB_CUDA(pipeline_test_mode(skip_loads ? 1 : 0, lim));
+    JB_CUDA(rotate_pipeline_test_mode(skip_loads ? 1 : 0, lim));
+    return JB_OK;
+}
+
 int32_t jb_gram_status(const void* workspace, int32_t* out, uintptr_t stream) {
     JB_CHECK_ARG(workspace && out, "jb_gram_status: null pointer");
     JB_CUDA(cudaMemcpyAsync(out, workspace, sizeof(int32_t), cudaMemcpyDeviceToHost,

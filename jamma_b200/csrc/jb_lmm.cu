@@ -146,11 +146,26 @@ __device__ double betacf(double a, double b, double x) {
     return h;
 }
 
+// log Gamma(a + 1/2) - log Gamma(a) for a >= 25 from the Stirling series of both terms
+// (log Gamma(z) = (z - 1/2) log z - z + log(2 pi)/2 + sum_k B_2k / (2k (2k-1) z^(2k-1)))
+// expanded in 1/a: 1/2 log a - 1/(8a) + 1/(192 a^3) - 1/(640 a^5) + 17/(14336 a^7)
+// - 31/(18432 a^9) + 691/(180224 a^11); the next term is below 1e-20 at a = 25.  The plain
+// difference of the two log-gammas cancels ~5 digits at a = df/2 ~ 1e4.
+__device__ double lgamma_ratio_half(double a) {
+    const double t = 1.0 / a, t2 = t * t;
+    const double s = t * (-1.0 / 8 + t2 * (1.0 / 192 + t2 * (-1.0 / 640 + t2 * (17.0 / 14336 +
+                     t2 * (-31.0 / 18432 + t2 * (691.0 / 180224))))));
+    return 0.5 * log(a) + s;
+}
+
 __device__ double betainc_reg(double a, double b, double x) {
     if (isnan(x)) return jnan();
     if (x <= 0.0) return 0.0;
     if (x >= 1.0) return 1.0;
-    const double lbt = lgamma(a + b) - lgamma(a) - lgamma(b) + a * log(x) + b * log1p(-x);
+    // log(1 / B(a, b)); b = 1/2 (every F test here) with large a takes the series above
+    const double lb = (b == 0.5 && a >= 25.0) ? lgamma_ratio_half(a) - 0.5723649429247001
+                                              : lgamma(a + b) - lgamma(a) - lgamma(b);
+    const double lbt = lb + a * log(x) + b * log1p(-x);
     if (x < (a + 1.0) / (a + b + 2.0)) return exp(lbt) * betacf(a, b, x) / a;
     return 1.0 - exp(lbt) * betacf(b, a, 1.0 - x) / b;
 }
@@ -1075,14 +1090,174 @@ __global__ void lmm_gemm_tables_kernel(int64_t n, int n_grid, int phi, const dou
     }
 }
 
-__global__ void square_cols_kernel(const double* __restrict__ X, int64_t ldx, int64_t n, int64_t m,
-                                   double* __restrict__ X2) {
-    const int64_t total = n * m;
+// ---------------------------------------------------------------- squared x-sums
+// CQ[j*ldcq + r] = sum_i A[i, r] x_ij^2 (r < rows) for every SNP j of a rotated chunk X
+// (column-major, ld ldx): the squared weighted sums of every table row.  One fused FP64
+// kernel reads each rotated genotype once, squares it in shared memory and forms the
+// product with the row table, so X^2 never goes to HBM.
+//   * A is held transposed, AT[i*ldt + r] (ldt a multiple of the row tile, zero for
+//     r >= rows), so a slice of kSqTK samples is one contiguous block per row tile;
+//   * a CTA owns TR rows x kSqTN SNPs for one range of samples; each thread keeps an
+//     8-row x 4-SNP block of FP64 accumulators in registers (SNPs tx, tx+16, tx+32, tx+48,
+//     conflict-free reads of the padded X slice; A rows broadcast within a half-warp);
+//   * slices are double-buffered with cp.async; out-of-range samples and SNPs read as zero;
+//   * the samples are split over kz = blockIdx.z ranges when the SNP tiles alone cannot
+//     fill the GPU; partial sums go to P[(kz*m + j)*ldt + r] and sq_reduce_kernel adds
+//     them in kz order, so every sum has a fixed order (bit-reproducible).
+constexpr int kSqTK = 32;  // samples per slice
+constexpr int kSqTN = 64;  // SNPs per CTA
+constexpr int kSqSplitTarget = 148 * 4;  // CTAs to aim for (2 waves at 2 CTAs per SM)
+
+template <int TR>
+struct SqCfg {
+    static constexpr int TY = TR / 8;              // thread rows (8 table rows each)
+    static constexpr int NT = TY * 16;             // threads: 16 thread columns x 4 SNPs
+    static constexpr int XLD = kSqTK + 1;          // padded sample stride of a slice's SNP
+    static constexpr int A_ELEMS = kSqTK * TR;
+    static constexpr int X_ELEMS = kSqTN * XLD;
+    static constexpr int STAGE = A_ELEMS + X_ELEMS;  // doubles (even: stages stay 16-byte aligned)
+    static constexpr int SMEM = 2 * STAGE * 8;
+};
+
+// Row tile for a table of `rows` rows and the matching padded leading dimension of AT.
+inline int sq_tile_rows(int64_t rows) { return rows <= 56 ? 56 : 104; }
+inline int64_t sq_ldt(int64_t rows) {
+    const int tr = sq_tile_rows(rows);
+    return ceil_div(rows, tr) * tr;
+}
+// Sample-range split: enough CTAs to fill the GPU, each range at least 8 slices long.
+inline int sq_split(int64_t n, int64_t m, int64_t rows) {
+    const int64_t tiles = ceil_div(m, kSqTN) * (sq_ldt(rows) / sq_tile_rows(rows));
+    int64_t ks = ceil_div(kSqSplitTarget, tiles);
+    const int64_t kmax = ceil_div(n, 8 * kSqTK);
+    if (ks > kmax) ks = kmax;
+    return (int)(ks < 1 ? 1 : ks);
+}
+
+__device__ __forceinline__ void cp_async16(double* dst, const double* src, bool valid) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(d), "l"(src),
+                 "r"(valid ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(d), "l"(src),
+                 "r"(valid ? 8 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+    asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+template <int TR>
+__global__ void __launch_bounds__(SqCfg<TR>::NT, 2)
+    sq_sums_kernel(const double* __restrict__ AT, int64_t ldt, const double* __restrict__ X,
+                   int64_t ldx, int64_t n, int64_t m, int64_t klen, int rows,
+                   double* __restrict__ out, int64_t ldo, int64_t zstride) {
+    using Cfg = SqCfg<TR>;
+    extern __shared__ __align__(16) double sq_smem[];
+    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int64_t j0 = (int64_t)blockIdx.x * kSqTN;
+    const int64_t r0 = (int64_t)blockIdx.y * TR;
+    const int64_t kbeg = (int64_t)blockIdx.z * klen;
+    const int64_t kend = kbeg + klen < n ? kbeg + klen : n;
+    const int nsl = kend > kbeg ? (int)((kend - kbeg + kSqTK - 1) / kSqTK) : 0;
+
+    auto issue = [&](int st, int64_t k) {
+        double* As = sq_smem + st * Cfg::STAGE;
+        double* Xs = As + Cfg::A_ELEMS;
+        for (int e = tid; e < kSqTK * (TR / 2); e += Cfg::NT) {  // A: 16-byte chunks
+            const int kk = e / (TR / 2), c = e % (TR / 2);
+            const bool ok = k + kk < kend;
+            cp_async16(As + kk * TR + 2 * c, AT + (ok ? (k + kk) * ldt : 0) + r0 + 2 * c, ok);
+        }
+        for (int e = tid; e < kSqTN * kSqTK; e += Cfg::NT) {  // X: one double per copy
+            const int jj = e / kSqTK, kk = e % kSqTK;
+            const bool ok = (k + kk < kend) && (j0 + jj < m);
+            cp_async8(Xs + jj * Cfg::XLD + kk, X + (ok ? (j0 + jj) * ldx + k + kk : 0), ok);
+        }
+        cp_async_commit();
+    };
+
+    double acc[8][4];
+#pragma unroll
+    for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[a][q] = 0.0;
+
+    if (nsl > 0) issue(0, kbeg);
+    for (int s = 0; s < nsl; ++s) {
+        if (s + 1 < nsl) {
+            issue((s + 1) & 1, kbeg + (int64_t)(s + 1) * kSqTK);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        double* As = sq_smem + (s & 1) * Cfg::STAGE;
+        double* Xs = As + Cfg::A_ELEMS;
+        // square the X elements this thread copied (its own copies have landed)
+        for (int e = tid; e < kSqTN * kSqTK; e += Cfg::NT) {
+            double* v = Xs + (e / kSqTK) * Cfg::XLD + e % kSqTK;
+            *v = *v * *v;
+        }
+        __syncthreads();
+#pragma unroll 4
+        for (int kk = 0; kk < kSqTK; ++kk) {
+            const double2* ap = reinterpret_cast<const double2*>(As + kk * TR + ty * 8);
+            double a[8];
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                const double2 v = ap[h];
+                a[2 * h] = v.x;
+                a[2 * h + 1] = v.y;
+            }
+            double x[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) x[q] = Xs[(tx + 16 * q) * Cfg::XLD + kk];
+#pragma unroll
+            for (int a2 = 0; a2 < 8; ++a2)
+#pragma unroll
+                for (int q = 0; q < 4; ++q) acc[a2][q] = fma(a[a2], x[q], acc[a2][q]);
+        }
+        __syncthreads();  // the next issue overwrites this stage
+    }
+    double* o = out + (int64_t)blockIdx.z * zstride;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int64_t j = j0 + tx + 16 * q;
+        if (j >= m) continue;
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            const int64_t r = r0 + ty * 8 + a;
+            if (r < rows) o[j * ldo + r] = acc[a][q];
+        }
+    }
+}
+
+// CQ[j*ldcq + r] = sum over kz = 0..ks-1 of P[(kz*m + j)*ldt + r], in kz order.
+__global__ void sq_reduce_kernel(const double* __restrict__ P, int64_t ldt, int64_t m, int rows,
+                                 int ks, double* __restrict__ CQ, int64_t ldcq) {
+    const int64_t total = m * rows;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
          t += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t j = t / n, i = t - j * n;
-        const double v = X[j * ldx + i];
-        X2[t] = v * v;
+        const int64_t j = t / rows, r = t - j * rows;
+        double v = 0.0;
+        for (int z = 0; z < ks; ++z) v += P[((int64_t)z * m + j) * ldt + r];
+        CQ[j * ldcq + r] = v;
+    }
+}
+
+// AT[i*ldt + r] = A[r*n + i] for r < rows, 0 for rows <= r < ldt.
+__global__ void sq_table_kernel(const double* __restrict__ A, int64_t n, int rows, int64_t ldt,
+                                double* __restrict__ AT) {
+    const int64_t total = n * ldt;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < total;
+         t += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t i = t / ldt, r = t - i * ldt;
+        AT[t] = r < rows ? A[r * n + i] : 0.0;
     }
 }
 
@@ -1322,7 +1497,7 @@ __global__ void null_mle_kernel(int64_t n, const double* W, int64_t ldw, const d
 
 // ---------------------------------------------------------------- host helpers
 struct WsLayout {
-    int64_t loglam, logdet, H, S, cheb, cmid, chalf, cvals, alin, asq, hn, ccos, blas, total;
+    int64_t loglam, logdet, H, S, cheb, cmid, chalf, cvals, alin, asq, asqt, hn, ccos, blas, total;
 };
 
 inline int64_t align256(int64_t b) { return (b + 255) / 256 * 256; }
@@ -1361,6 +1536,12 @@ inline WsLayout ws_layout(int64_t n, int c, int phi, int n_grid) {
     off += align256(8 * rows * (c + phi) * n);
     w.asq = off;
     off += align256(8 * rows * n);
+    {  // the squared-sum table transposed for sq_sums_kernel, for either form's row count
+        const int64_t r1 = (int64_t)n_grid + 1 + phi, r2 = 1 + kChebG;
+        const int64_t ldt = sq_ldt(r1) > sq_ldt(r2) ? sq_ldt(r1) : sq_ldt(r2);
+        w.asqt = off;
+        off += align256(8 * ldt * n);
+    }
     w.hn = off;
     off += align256(8 * (int64_t)kChebG * n);
     w.ccos = off;
@@ -1372,15 +1553,28 @@ inline WsLayout ws_layout(int64_t n, int c, int phi, int n_grid) {
 }
 
 struct ChunkLayout {
-    int64_t x2, cl, cq, blas, total;
+    int64_t sqp, cl, cq, blas, total;
 };
+
+// Partial squared sums of sq_sums_kernel's sample ranges: the largest over the row counts a
+// chunk can use (FP64 form with and without null rows, mixed form).
+inline int64_t sq_partial_doubles(int64_t n, int64_t m, int phi, int n_grid) {
+    const int64_t cand[3] = {(int64_t)n_grid + 1 + phi, (int64_t)n_grid + 1, 1 + (int64_t)kChebG};
+    int64_t best = 0;
+    for (int64_t r : cand) {
+        const int ks = sq_split(n, m, r);
+        const int64_t v = ks > 1 ? (int64_t)ks * m * sq_ldt(r) : 0;
+        if (v > best) best = v;
+    }
+    return best;
+}
 
 inline ChunkLayout chunk_layout(int64_t n, int c, int phi, int n_grid, int64_t m) {
     ChunkLayout L;
     const int64_t rows = table_rows(phi, n_grid);
     int64_t off = 0;
-    L.x2 = off;
-    off += align256(8 * n * m);
+    L.sqp = off;
+    off += align256(8 * sq_partial_doubles(n, m, phi, n_grid));
     L.cl = off;
     off += align256(8 * rows * (c + phi) * m);
     L.cq = off;
@@ -1425,13 +1619,55 @@ __global__ void linspace_kernel(double* out, double start, double stop, int num)
 }
 
 // F statistics (NaN where there is no test) -> F-test p-values, in place, one thread per
-// value.  The continued fraction of betainc_reg takes up to ~100 steps for F above ~3 at
-// df ~ 2e4; inside the search kernel every lane of a pair's group would repeat it, and a
-// warp would wait for the slower of its pairs.
-__global__ void lmm_fpvalue_kernel(double* __restrict__ v, int64_t count, double df) {
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
-         i += (int64_t)gridDim.x * blockDim.x)
-        v[i] = f_pvalue(v[i], df, true);
+// value, for up to two arrays of `count` values (Wald and score) in one launch.  The
+// continued fraction of betainc_reg takes up to ~100 steps for F above ~3 at df ~ 2e4;
+// inside the search kernel every lane of a pair's group would repeat it, and a warp would
+// wait for the slower of its pairs.
+__global__ void lmm_fpvalue_kernel(double* __restrict__ v0, double* __restrict__ v1,
+                                   int64_t count, double df) {
+    const int64_t total = v1 ? 2 * count : count;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        double* v = i < count ? v0 + i : v1 + (i - count);
+        *v = f_pvalue(*v, df, true);
+    }
+}
+
+// Squared x-sums of a rotated chunk: sq_sums_kernel (+ sq_reduce_kernel when the samples
+// are split into ranges).  AT: the transposed table (ld sq_ldt(rows)); P: partial sums
+// (sq_partial_doubles); CQ: rows x m, ld ldcq.
+int32_t launch_sq_sums(const double* AT, int64_t rows, const double* X, int64_t ldx, int64_t n,
+                       int64_t m, double* P, double* CQ, int64_t ldcq, cudaStream_t st) {
+    const int tr = sq_tile_rows(rows);
+    const int64_t ldt = sq_ldt(rows);
+    const int ks = sq_split(n, m, rows);
+    const int64_t klen = ceil_div(ceil_div(n, ks), kSqTK) * kSqTK;
+    const int64_t gx = ceil_div(m, kSqTN);
+    if (gx > 0x7fffffffll || ldt / tr > 65535) {
+        set_error("squared x-sums: chunk too large");
+        return JB_E_INVALID;
+    }
+    dim3 grid((unsigned)gx, (unsigned)(ldt / tr), (unsigned)ks);
+    double* out = ks > 1 ? P : CQ;
+    const int64_t ldo = ks > 1 ? ldt : ldcq;
+    if (tr == 56) {
+        JB_CUDA(cudaFuncSetAttribute(sq_sums_kernel<56>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     SqCfg<56>::SMEM));
+        sq_sums_kernel<56><<<grid, SqCfg<56>::NT, SqCfg<56>::SMEM, st>>>(
+            AT, ldt, X, ldx, n, m, klen, (int)rows, out, ldo, m * ldt);
+    } else {
+        JB_CUDA(cudaFuncSetAttribute(sq_sums_kernel<104>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     SqCfg<104>::SMEM));
+        sq_sums_kernel<104><<<grid, SqCfg<104>::NT, SqCfg<104>::SMEM, st>>>(
+            AT, ldt, X, ldx, n, m, klen, (int)rows, out, ldo, m * ldt);
+    }
+    JB_LAUNCH_CHECK("sq_sums_kernel");
+    if (ks > 1) {
+        const int64_t blocks = ceil_div(m * rows, 256) < 4096 ? ceil_div(m * rows, 256) : 4096;
+        sq_reduce_kernel<<<(unsigned)blocks, 256, 0, st>>>(P, ldt, m, (int)rows, ks, CQ, ldcq);
+        JB_LAUNCH_CHECK("sq_reduce_kernel");
+    }
+    return JB_OK;
 }
 
 template <int C>
@@ -1446,12 +1682,16 @@ int32_t launch_pairs(const Params& p, cudaStream_t st) {
         lmm_pairs_kernel<C, false, 32><<<(unsigned)ceil_div(pairs * 32, kPairsThreads), kPairsThreads, 0, st>>>(p);
     JB_LAUNCH_CHECK("lmm_pairs_kernel");
     // p-values of the tests this mode ran (other outputs stay untouched)
-    double* const fv[2] = {(p.mode == 1 || p.mode == 4) ? p.out.p_wald : nullptr,
-                           (p.mode == 3 || p.mode == 4) ? p.out.p_score : nullptr};
-    const int64_t blocks = ceil_div(pairs, 256) < 4096 ? ceil_div(pairs, 256) : 4096;
-    for (double* v : fv) {
-        if (!v) continue;
-        lmm_fpvalue_kernel<<<(unsigned)blocks, 256, 0, st>>>(v, pairs, p.df);
+    double* v0 = (p.mode == 1 || p.mode == 4) ? p.out.p_wald : nullptr;
+    double* v1 = (p.mode == 3 || p.mode == 4) ? p.out.p_score : nullptr;
+    if (!v0) {
+        v0 = v1;
+        v1 = nullptr;
+    }
+    if (v0) {
+        const int64_t total = v1 ? 2 * pairs : pairs;
+        const int64_t blocks = ceil_div(total, 128) < 8192 ? ceil_div(total, 128) : 8192;
+        lmm_fpvalue_kernel<<<(unsigned)blocks, 128, 0, st>>>(v0, v1, pairs, p.df);
         JB_LAUNCH_CHECK("lmm_fpvalue_kernel");
     }
     return JB_OK;
@@ -1507,6 +1747,14 @@ int32_t launch_prepare(int64_t n, int phi, int n_grid, const double* evals, cons
         lmm_series_tables_kernel<C><<<dim3(1 + kChebG, ny), 256, 0, st>>>(n, phi, W, ldw, Y, ldy,
                                                                          Alin, Asq);
         JB_LAUNCH_CHECK("lmm_series_tables_kernel");
+    }
+    {  // the squared-sum rows transposed for sq_sums_kernel
+        const int64_t rows_sq = interp ? 1 + kChebG : (int64_t)rows_s;
+        const int64_t ldt = sq_ldt(rows_sq);
+        const int64_t blocks = ceil_div(n * ldt, 256) < 8192 ? ceil_div(n * ldt, 256) : 8192;
+        sq_table_kernel<<<(unsigned)blocks, 256, 0, st>>>(Asq, n, (int)rows_sq, ldt,
+                                                          reinterpret_cast<double*>(ws + L.asqt));
+        JB_LAUNCH_CHECK("sq_table_kernel");
     }
     if (interp) {
         const int nf = 1 + phi * Lay<C>::NS;
@@ -1706,34 +1954,30 @@ int32_t jb_lmm_chunk(int32_t lmm_mode, int32_t precision, int64_t n, int32_t n_c
     const ChunkLayout CLy = chunk_layout(n, n_cvt, phi, n_grid, m);
     JB_CHECK_ARG(chunk_workspace && chunk_bytes >= CLy.total, "jb_lmm_chunk: chunk workspace too small");
     uint8_t* cws = static_cast<uint8_t*>(chunk_workspace);
-    double* X2 = reinterpret_cast<double*>(cws + CLy.x2);
     double* CL = reinterpret_cast<double*>(cws + CLy.cl);
     double* CQ = reinterpret_cast<double*>(cws + CLy.cq);
     // FP64 form: grid rows, ones row, null rows (only when prepared); mixed: ones + series
     const int rows = precision >= 1 ? 1 + kChebG : n_grid + 1 + (lmm_mode == 1 ? 0 : phi);
     const int rows_lin = rows * (n_cvt + phi);
-    square_cols_kernel<<<(unsigned)(ceil_div(n * m, 256) < 8192 ? ceil_div(n * m, 256) : 8192), 256, 0,
-                         st>>>(UtG, ldg, n, m, X2);
-    JB_LAUNCH_CHECK("square_cols_kernel");
     {
-        cublasHandle_t h = cublas_handle();
-        if (!h) {
-            set_error("cuBLAS handle creation failed");
-            return JB_E_LIBRARY;
-        }
-        cublasStatus_t cs = bind_cublas(h, st, cws + CLy.blas, kCublasWorkspaceBytes);
-        if (cs != CUBLAS_STATUS_SUCCESS) return cublas_status(cs, "cublasSetStream/Workspace");
-        const double one = 1.0, zero = 0.0;
         if (precision != 2) {  // precision 2: CL already formed by jb_lmm_chunk_series_i8
+            cublasHandle_t h = cublas_handle();
+            if (!h) {
+                set_error("cuBLAS handle creation failed");
+                return JB_E_LIBRARY;
+            }
+            cublasStatus_t cs = bind_cublas(h, st, cws + CLy.blas, kCublasWorkspaceBytes);
+            if (cs != CUBLAS_STATUS_SUCCESS) return cublas_status(cs, "cublasSetStream/Workspace");
+            const double one = 1.0, zero = 0.0;
             cs = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, rows_lin, (int)m, (int)n, &one,
                              reinterpret_cast<const double*>(ws + L.alin), (int)n, UtG, (int)ldg,
                              &zero, CL, rows_lin);
             if (cs != CUBLAS_STATUS_SUCCESS) return cublas_status(cs, "cublasDgemm (linear x-sums)");
         }
-        cs = cublasDgemm(h, CUBLAS_OP_T, CUBLAS_OP_N, rows, (int)m, (int)n, &one,
-                         reinterpret_cast<const double*>(ws + L.asq), (int)n, X2, (int)n, &zero, CQ,
-                         rows);
-        if (cs != CUBLAS_STATUS_SUCCESS) return cublas_status(cs, "cublasDgemm (square x-sums)");
+        const int32_t rc = launch_sq_sums(reinterpret_cast<const double*>(ws + L.asqt), rows, UtG,
+                                          ldg, n, m, reinterpret_cast<double*>(cws + CLy.sqp), CQ,
+                                          rows, st);
+        if (rc) return rc;
     }
     p.CL = CL;
     p.ldcl = rows_lin;

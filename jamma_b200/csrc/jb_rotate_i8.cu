@@ -328,6 +328,10 @@ int32_t rotate_i8_gemm(const uint8_t* ozaki_ws, int64_t n_out, int64_t n_k, cons
     return JB_OK;
 }
 
+cudaError_t rotate_pipeline_test_mode(int skip_loads, unsigned long long wait_limit_ns) {
+    return pipeline_test_mode(skip_loads, wait_limit_ns);
+}
+
 }  // namespace tc
 }  // namespace jb
 

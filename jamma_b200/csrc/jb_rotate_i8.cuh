@@ -36,5 +36,9 @@ int32_t rotate_i8_gemm(const uint8_t* ozaki_ws, int64_t n_out, int64_t n_k, cons
                        int64_t b_rows, int64_t ldb, bool paired, int64_t m, const double* mean,
                        double* X, int64_t ldx, Tile* tiles, int* status, cudaStream_t st);
 
+// Test hooks of the rotation kernels' bounded waits (this translation unit's copy of the
+// GEMM core's hooks; see jb_test_pipeline_timeout).
+cudaError_t rotate_pipeline_test_mode(int skip_loads, unsigned long long wait_limit_ns);
+
 }  // namespace tc
 }  // namespace jb

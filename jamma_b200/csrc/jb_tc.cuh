@@ -56,15 +56,19 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 // Error codes written to the caller's status word.
 enum : int { kErrNone = 0, kErrTimeout = 1 };
 
-// Bounded wait.  Returns false (and has raised *abort) if the deadline passed or another
-// role already aborted.
+// Default deadline of every bounded wait.
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s
+
+// Bounded wait.  Returns false (and has raised *abort) if the deadline (limit_ns after the
+// call) passed or another role already aborted.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, volatile int* abort,
-                                          int* err, int where) {
+                                          int* err, int where,
+                                          unsigned long long limit_ns = kWaitLimitNs) {
     const uint64_t t0 = globaltimer_ns();
     while (true) {
         if (mbar_try_wait(bar, parity)) return true;
         if (*abort) return false;
-        if (globaltimer_ns() - t0 > 2000000000ull) {  // 2 s
+        if (globaltimer_ns() - t0 > limit_ns) {
             *abort = 1;
             atomicCAS(err, 0, kErrTimeout * 100 + where);
             return false;

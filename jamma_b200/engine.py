@@ -259,11 +259,14 @@ class ChunkGraph:
     Capture runs on a private stream without synchronising the device, with thread-local
     capture rules, so other streams and threads keep working meanwhile.  The graph keeps
     the cohort's workspaces alive; capture after any eager chunk larger than ``m`` so that
-    no workspace is reallocated afterwards.
+    no workspace is reallocated afterwards.  ``prefill(graph)``, if given, fills the input
+    buffers (on the capture's private stream) before the eager warm-up run, whose results
+    are then a real chunk's, left in ``out`` when the constructor returns.
     """
 
     def __init__(self, cohort: "DeviceCohort", m: int, n_file: int | None = None,
-                 sample_idx: torch.Tensor | None = None, has_missing: bool = True):
+                 sample_idx: torch.Tensor | None = None, has_missing: bool = True,
+                 prefill=None):
         n = cohort.n
         n_file = n if n_file is None else n_file
         self.cohort, self.m, self.n_file, self.sample_idx = cohort, m, n_file, sample_idx
@@ -280,6 +283,8 @@ class ChunkGraph:
         side = torch.cuda.Stream()
         side.wait_stream(caller)
         with torch.cuda.stream(side):
+            if prefill is not None:  # the warm-up computes a real first chunk
+                prefill(self)
             self._run()  # eager warm-up: workspaces, library handles, kernel attributes
             self._keep = (cohort.ws, cohort._chunk_ws, cohort._rot_ws, cohort.series_ws,
                           cohort.ozaki)
@@ -316,3 +321,47 @@ def decode_packed(packed: torch.Tensor, n_file: int, sample_idx: torch.Tensor | 
     _native.call("jb_decode_bed", ptr(packed), bps, m, ptr(sample_idx), n, ptr(codes), ld,
                  ptr(counts), stream_handle())
     return codes, counts
+
+
+def pass1_counts(bed, sample_idx: torch.Tensor | None, n: int, chunk: int = 16384) -> np.ndarray:
+    """Per-SNP counts {n_obs, sum, n_het, n_hom2} of every SNP of a .bed file over the
+    analysed samples (jamma's pass-1 statistics loop, src/jamma/lmm/runner_streaming.py:
+    224-284), pipelined: while the device decodes chunk k, the host reads chunk k+1 into the
+    other pinned buffer; counts return by asynchronous copies collected one chunk behind."""
+    p, bps = bed.n_snps, bed.bytes_per_snp
+    out = np.empty((p, 4), dtype=np.int32)
+    if p == 0:
+        return out
+    step = min(chunk, p)
+    st = torch.cuda.current_stream()
+    pin = [torch.empty((step, bps), dtype=torch.uint8, pin_memory=True) for _ in range(2)]
+    pin_cnt = [torch.empty((step, 4), dtype=torch.int32, pin_memory=True) for _ in range(2)]
+    dev = [torch.empty((step, bps), dtype=torch.uint8, device="cuda") for _ in range(2)]
+    codes = torch.empty((step, n), dtype=torch.int8, device="cuda")
+    cnt = torch.empty((step, 4), dtype=torch.int32, device="cuda")
+    done = [None, None]   # counts of the chunk in buffer b are in pin_cnt[b]
+    rng = [None, None]    # SNP range of the chunk in buffer b, not yet collected
+
+    def collect(b: int) -> None:
+        done[b].synchronize()
+        s0, e0 = rng[b]
+        out[s0:e0] = pin_cnt[b][: e0 - s0].numpy()
+        rng[b] = None
+
+    for ci, s in enumerate(range(0, p, step)):
+        e = min(s + step, p)
+        b = ci % 2
+        if rng[b] is not None:
+            collect(b)  # chunk ci-2: its upload has read pin[b], its counts are back
+        pin[b].numpy()[: e - s] = bed.records[s:e]
+        dev[b][: e - s].copy_(pin[b][: e - s], non_blocking=True)
+        _native.call("jb_decode_bed", ptr(dev[b]), bps, e - s, ptr(sample_idx), n, ptr(codes), n,
+                     ptr(cnt), stream_handle())
+        pin_cnt[b][: e - s].copy_(cnt[: e - s], non_blocking=True)
+        done[b] = torch.cuda.Event()
+        done[b].record(st)
+        rng[b] = (s, e)
+    for b in (0, 1):
+        if rng[b] is not None:
+            collect(b)
+    return out

@@ -20,6 +20,8 @@ from jamma_b200.io import (
     read_eigen_files,
     read_kinship_matrix,
     read_phenotypes,
+    read_snp_list_file,
+    resolve_snp_list_to_indices,
     write_eigen_files,
     write_kinship_matrix,
 )
@@ -33,11 +35,6 @@ class GWASResult:
     n_samples: int
     n_snps_tested: int
     timing: dict[str, float] = field(default_factory=dict)
-
-
-def _read_snp_list(path) -> list[str]:
-    with open(path) as f:
-        return [line.split()[0] for line in f if line.strip()]
 
 
 def gwas(bfile, *, kinship_file=None, covariate_file=None, lmm_mode: int = 1, maf: float = 0.01,
@@ -70,10 +67,9 @@ def gwas(bfile, *, kinship_file=None, covariate_file=None, lmm_mode: int = 1, ma
     n = meta["n_samples"]
     y = read_phenotypes(bfile, phenotype_column)
     sid = list(meta["sid"])
-    pos = {s: i for i, s in enumerate(sid)}
     snps_idx = None
     if snps_file is not None:
-        snps_idx = np.array(sorted(pos[s] for s in _read_snp_list(snps_file) if s in pos), dtype=np.int64)
+        snps_idx = resolve_snp_list_to_indices(read_snp_list_file(snps_file), sid)
     cov = None
     if covariate_file is not None:
         cov, _ = read_covariate_file(covariate_file)
@@ -81,7 +77,7 @@ def gwas(bfile, *, kinship_file=None, covariate_file=None, lmm_mode: int = 1, ma
             raise ValueError(f"Covariate file has {cov.shape[0]} rows but .fam has {n} samples")
     ks = None
     if ksnps_file is not None:
-        ks = np.array(sorted(pos[s] for s in _read_snp_list(ksnps_file) if s in pos), dtype=np.int64)
+        ks = resolve_snp_list_to_indices(read_snp_list_file(ksnps_file), sid)
     evals = evecs = K = None
     if loco:
         pass

@@ -86,6 +86,47 @@ class BedFile:
         np.take(self.records, np.asarray(idx), axis=0, out=out)
 
 
+def read_snp_list_file(path) -> set[str]:
+    """SNP ids of a GEMMA-style list file (``read_snp_list_file``,
+    src/jamma/io/snp_list.py:13-49): the first whitespace-delimited token of every
+    non-empty line.  Raises FileNotFoundError for a missing file and ValueError when the
+    file holds no id."""
+    path = Path(path)
+    if not path.exists():
+        raise FileNotFoundError(f"SNP list file not found: {path}")
+    ids: set[str] = set()
+    with open(path) as f:
+        for line in f:
+            tok = line.split()
+            if tok:
+                ids.add(tok[0])
+    if not ids:
+        raise ValueError(f"SNP list file is empty or contains no valid IDs: {path}")
+    return ids
+
+
+def resolve_snp_list_to_indices(snp_ids, bim_sids) -> np.ndarray:
+    """Sorted .bim column indices of the listed ids, case-sensitive
+    (``resolve_snp_list_to_indices``, src/jamma/io/snp_list.py:52-88).  Ids absent from the
+    .bim are skipped; ValueError when none matches."""
+    pos = {sid: i for i, sid in enumerate(bim_sids)}
+    idx = sorted(pos[s] for s in snp_ids if s in pos)
+    if not idx:
+        raise ValueError(f"No SNPs from the list matched the BIM file (requested {len(snp_ids)} SNPs)")
+    return np.array(idx, dtype=np.intp)
+
+
+def apply_snp_list_mask(snp_mask: np.ndarray, indices, n_snps: int, label: str) -> None:
+    """AND ``snp_mask`` in place with the listed indices (``apply_snp_list_mask``,
+    src/jamma/core/snp_filter.py:15-33); ValueError for an index past the last SNP."""
+    indices = np.asarray(indices, dtype=np.int64)
+    if indices.size and indices.max() >= n_snps:
+        raise ValueError(f"{label} index {indices.max()} out of range for {n_snps} SNPs")
+    keep = np.zeros(n_snps, dtype=bool)
+    keep[indices] = True
+    snp_mask &= keep
+
+
 def write_plink_records(prefix, records: np.ndarray, n_samples: int, chrom=None,
                         phenotypes=None) -> None:
     """Write a .bed/.bim/.fam triple from packed SNP-major records (p, ceil(n/4)) --

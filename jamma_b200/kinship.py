@@ -14,8 +14,8 @@ import torch
 
 from jamma_b200 import _native
 from jamma_b200.device import empty, ptr, require_cuda, stream_handle, workspace
-from jamma_b200.engine import decode_packed
-from jamma_b200.io import BedFile, pack_genotypes
+from jamma_b200.engine import decode_packed, pass1_counts
+from jamma_b200.io import BedFile, apply_snp_list_mask, pack_genotypes
 
 
 def snp_stats_from_counts(counts: np.ndarray, n: int, dtype=np.float32):
@@ -274,18 +274,11 @@ def compute_kinship_from_bed(bfile, maf_threshold: float = 0.0, miss_threshold: 
     n = bed.n_samples if sample_idx is None else len(sample_idx)
     sidx = None if sample_idx is None else torch.from_numpy(
         np.asarray(sample_idx, dtype=np.int32)).to("cuda")
-    counts = []
-    for s in range(0, bed.n_snps, chunk_size):
-        rec = torch.from_numpy(bed.read(s, min(s + chunk_size, bed.n_snps))).to("cuda")
-        _, cnt = decode_packed(rec, bed.n_samples, sidx, n)
-        counts.append(cnt.cpu().numpy())
-    counts = np.concatenate(counts)
+    counts = pass1_counts(bed, sidx, n, max(chunk_size, 16384))
     mean, miss, poly = snp_stats_from_counts(counts, n, np.float32)
     keep, _ = filter_mask(mean, miss, poly, n, maf_threshold, miss_threshold)
     if ksnps_indices is not None:
-        sub_mask = np.zeros(bed.n_snps, dtype=bool)
-        sub_mask[np.asarray(ksnps_indices, dtype=np.int64)] = True
-        keep &= sub_mask
+        apply_snp_list_mask(keep, ksnps_indices, keep.size, "Kinship SNP list")
     idx = np.where(keep)[0]
     if idx.size == 0:
         raise ValueError("No SNPs passed filtering")

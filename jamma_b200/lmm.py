@@ -22,6 +22,7 @@ from jamma_b200.io import (
     AssocResult,
     BedFile,
     IncrementalAssocWriter,
+    apply_snp_list_mask,
     format_assoc_line,
     get_plink_metadata,
     pack_genotypes,
@@ -82,9 +83,7 @@ class _Stats:
         self.mean, self.miss, poly = snp_stats_from_counts(counts, n, mean_dtype)
         keep, self.af = filter_mask(self.mean, self.miss, poly, n, maf, miss)
         if snps_indices is not None:
-            sel = np.zeros_like(keep)
-            sel[np.asarray(snps_indices, dtype=np.int64)] = True
-            keep &= sel
+            apply_snp_list_mask(keep, snps_indices, keep.size, "SNP list filter")
         if hwe_threshold > 0:
             hom0 = counts[:, 0] - counts[:, 2] - counts[:, 3]
             keep &= hwe_pvalues(hom0, counts[:, 2], counts[:, 3]) >= hwe_threshold
@@ -143,16 +142,31 @@ def associate_records(cohort: eng.DeviceCohort, records, n_file: int, sample_idx
     has_missing = True if n_miss is None else bool(np.any(np.asarray(n_miss) > 0))
     main = torch.cuda.current_stream()
     side = torch.cuda.Stream()
-    graph = eng.ChunkGraph(cohort, step, n_file, sidx, has_missing=has_missing)
     pin_rec = [torch.empty((step, bps), dtype=torch.uint8, pin_memory=True) for _ in range(2)]
     pin_mu = [torch.empty((step,), dtype=torch.float64, pin_memory=True) for _ in range(2)]
     dev_rec = [torch.empty((step, bps), dtype=torch.uint8, device="cuda") for _ in range(2)]
     dev_mu = [torch.empty((step,), dtype=torch.float64, device="cuda") for _ in range(2)]
-    pin_out = [{k: torch.empty((cohort.phi, step), dtype=torch.float64, pin_memory=True)
-                for k in graph.out} for _ in range(2)]
-    copied = [None, None]    # side stream: pinned buffer b read, staging buffer b filled
+    copied = [None, None]    # pinned buffer b read, staging buffer b filled
     consumed = [None, None]  # replay stream: staging buffer b copied into the graph inputs
     returned = [None, None]  # replay stream: results of the chunk in buffer b are in pin_out[b]
+
+    def fill(b: int, s: int, e: int) -> None:
+        if callable(records):
+            records(s, e, pin_rec[b].numpy()[: e - s])
+        else:
+            pin_rec[b].numpy()[: e - s] = records[s:e]
+        pin_mu[b].numpy()[: e - s] = means[s:e]
+
+    def first_chunk(g: eng.ChunkGraph) -> None:
+        # the graph's eager warm-up run computes chunk 0
+        fill(0, 0, step)
+        g.packed.copy_(pin_rec[0], non_blocking=True)
+        g.means.copy_(pin_mu[0], non_blocking=True)
+
+    graph = eng.ChunkGraph(cohort, step, n_file, sidx, has_missing=has_missing,
+                           prefill=first_chunk)
+    pin_out = [{k: torch.empty((cohort.phi, step), dtype=torch.float64, pin_memory=True)
+                for k in graph.out} for _ in range(2)]
 
     def collect(b: int, s: int, e: int) -> None:
         returned[b].synchronize()
@@ -161,17 +175,22 @@ def associate_records(cohort: eng.DeviceCohort, records, n_file: int, sample_idx
         if on_chunk is not None:
             on_chunk(s, e)
 
-    pending = None
-    for ci, s in enumerate(range(0, m, step)):
+    def send_back(b: int, rows: int) -> None:
+        for k, v in graph.out.items():
+            pin_out[b][k][:, :rows].copy_(v[:, :rows], non_blocking=True)
+        returned[b] = torch.cuda.Event()
+        returned[b].record(main)
+
+    copied[0] = torch.cuda.Event()
+    copied[0].record(main)  # the constructor's copies from pin_rec[0] precede this
+    send_back(0, step)
+    pending = (0, 0, step)
+    for ci, s in enumerate(range(step, m, step), start=1):
         e = min(s + step, m)
         b, rows = ci % 2, e - s
         if copied[b] is not None:
             copied[b].synchronize()  # chunk ci-2's upload has read pin_rec[b]
-        if callable(records):
-            records(s, e, pin_rec[b].numpy()[:rows])
-        else:
-            pin_rec[b].numpy()[:rows] = records[s:e]
-        pin_mu[b].numpy()[:rows] = means[s:e]
+        fill(b, s, e)
         with torch.cuda.stream(side):
             if consumed[b] is not None:
                 side.wait_event(consumed[b])
@@ -184,13 +203,9 @@ def associate_records(cohort: eng.DeviceCohort, records, n_file: int, sample_idx
         graph.means[:rows].copy_(dev_mu[b][:rows], non_blocking=True)
         consumed[b] = torch.cuda.Event()
         consumed[b].record(main)
-        out = graph.replay()
-        for k, v in out.items():
-            pin_out[b][k][:, :rows].copy_(v[:, :rows], non_blocking=True)
-        returned[b] = torch.cuda.Event()
-        returned[b].record(main)
-        if pending is not None:
-            collect(*pending)
+        graph.replay()
+        send_back(b, rows)
+        collect(*pending)
         pending = (b, s, e)
     collect(*pending)
     if cohort.precision == "mixed" and (status := cohort.rotate_status()):
@@ -253,11 +268,7 @@ def run_lmm_association_streaming(
 
     # pass 1: per-SNP counts on the device (float32 means, as jamma's streaming path)
     sidx = None if sample_idx is None else torch.from_numpy(sample_idx).to("cuda")
-    counts = np.empty((p, 4), dtype=np.int32)
-    for s in range(0, p, chunk_size):
-        e = min(s + chunk_size, p)
-        _, c = eng.decode_packed(torch.from_numpy(bed.read(s, e)).to("cuda"), n_file, sidx, n)
-        counts[s:e] = c.cpu().numpy()
+    counts = eng.pass1_counts(bed, sidx, n, max(chunk_size, 16384))
     st = _Stats(counts, n, np.float32, maf_threshold, miss_threshold, snps_indices, hwe_threshold)
     t1 = time.perf_counter()
     if st.idx.size == 0:

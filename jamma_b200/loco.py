@@ -28,6 +28,7 @@ from jamma_b200.io import (
     AssocResult,
     BedFile,
     IncrementalAssocWriter,
+    apply_snp_list_mask,
     format_assoc_line,
     get_plink_metadata,
     snp_info_from_meta,
@@ -46,13 +47,7 @@ def chromosome_partitions(chroms) -> dict[str, np.ndarray]:
 
 
 def _counts_all(bed: BedFile, chunk: int) -> np.ndarray:
-    out = np.empty((bed.n_snps, 4), dtype=np.int32)
-    for s in range(0, bed.n_snps, chunk):
-        e = min(s + chunk, bed.n_snps)
-        _, c = eng.decode_packed(torch.from_numpy(bed.read(s, e)).cuda(), bed.n_samples, None,
-                                 bed.n_samples)
-        out[s:e] = c.cpu().numpy()
-    return out
+    return eng.pass1_counts(bed, None, bed.n_samples, max(chunk, 16384))
 
 
 def compute_loco_kinship(bfile, maf_threshold: float = 0.0, miss_threshold: float = 1.0,
@@ -70,9 +65,7 @@ def compute_loco_kinship(bfile, maf_threshold: float = 0.0, miss_threshold: floa
     mean, miss, poly = snp_stats_from_counts(counts, n, np.float32)
     keep, _ = filter_mask(mean, miss, poly, n, maf_threshold, miss_threshold)
     if ksnps_indices is not None:
-        sel = np.zeros_like(keep)
-        sel[np.asarray(ksnps_indices, dtype=np.int64)] = True
-        keep &= sel
+        apply_snp_list_mask(keep, ksnps_indices, keep.size, "Kinship SNP list")
     idx = np.where(keep)[0]
     if idx.size == 0:
         raise ValueError("No SNPs passed filtering")

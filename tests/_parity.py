@@ -71,11 +71,17 @@ def assert_mixed_parity(got: dict, ref: dict, keys):
 
 def strict_fp64_report(got: dict, ref: dict, keys=("beta", "se", "logl_h1", "p_wald"),
                        lam_key: str = "lambda_remle", lam_tol: float = 1e-12,
-                       tol: float = 1e-10) -> dict:
+                       tol: float = 1e-10, tols: dict | None = None) -> dict:
     """The plain FP64 form at the north-star tolerance: on every SNP whose REML lambda
     matches the oracle's to ``lam_tol`` relative (every golden-section decision taken the
-    same way), each field in ``keys`` must agree to ``tol`` relative.  Returns the fraction
-    of SNPs that qualify and the worst error among them per field."""
+    same way), each field in ``keys`` must agree to ``tol`` relative (``tols`` overrides it
+    per field).  Returns the fraction of SNPs that qualify and the worst error among them
+    per field.
+
+    The rest of the SNPs took a golden-section step differently: in the last steps the two
+    probes' log-likelihoods differ by less than the FP64 rounding of their length-n sums,
+    so any two FP64 implementations (GPU and NumPy, or jamma's own NumPy and JAX paths)
+    can branch differently there; lambda then stays within the final bracket."""
     la, lb = np.asarray(got[lam_key], float), np.asarray(ref[lam_key], float)
     same = np.isfinite(la) & np.isfinite(lb) & (_rel(la, lb) <= lam_tol)
     out = {"frac_lambda_matched": float(np.mean(same)), "n": int(same.size)}
@@ -88,5 +94,6 @@ def strict_fp64_report(got: dict, ref: dict, keys=("beta", "se", "logl_h1", "p_w
         r = _rel(a[ok], b[ok])
         worst = float(r.max()) if r.size else 0.0
         out[k] = worst
-        assert worst <= tol, f"{k}: {worst:.3e} > {tol} on a SNP whose lambda matches the oracle"
+        t = (tols or {}).get(k, tol)
+        assert worst <= t, f"{k}: {worst:.3e} > {t} on a SNP whose lambda matches the oracle"
     return out
