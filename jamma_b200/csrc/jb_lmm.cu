@@ -1092,29 +1092,31 @@ __global__ void lmm_gemm_tables_kernel(int64_t n, int n_grid, int phi, const dou
 
 // ---------------------------------------------------------------- squared x-sums
 // CQ[j*ldcq + r] = sum_i A[i, r] x_ij^2 (r < rows) for every SNP j of a rotated chunk X
-// (column-major, ld ldx): the squared weighted sums of every table row.  One fused FP64
-// kernel reads each rotated genotype once, squares it in shared memory and forms the
-// product with the row table, so X^2 never goes to HBM.
+// (column-major, ld ldx): the squared weighted sums of every table row.  One fused kernel
+// reads each rotated genotype once, squares it in shared memory and forms the product with
+// the row table on the FP64 tensor cores (mma.sync m8n8k4 .f64), so X^2 never goes to HBM.
 //   * A is held transposed, AT[i*ldt + r] (ldt a multiple of the row tile, zero for
 //     r >= rows), so a slice of kSqTK samples is one contiguous block per row tile;
-//   * a CTA owns TR rows x kSqTN SNPs for one range of samples; each thread keeps an
-//     8-row x 4-SNP block of FP64 accumulators in registers (SNPs tx, tx+16, tx+32, tx+48,
-//     conflict-free reads of the padded X slice; A rows broadcast within a half-warp);
+//   * a CTA owns TR rows x kSqTN SNPs for one range of samples; warp w owns SNPs
+//     16w..16w+15 (two 8-column MMA tiles) for all TR/8 row tiles of the CTA;
+//   * shared layouts As[k][TR] (TR = 8 mod 16 doubles) and Xs[j][kSqXLD] (kSqXLD = 4 mod
+//     16) make every 32-lane fragment load two conflict-free wavefronts;
 //   * slices are double-buffered with cp.async; out-of-range samples and SNPs read as zero;
 //   * the samples are split over kz = blockIdx.z ranges when the SNP tiles alone cannot
 //     fill the GPU; partial sums go to P[(kz*m + j)*ldt + r] and sq_reduce_kernel adds
 //     them in kz order, so every sum has a fixed order (bit-reproducible).
-constexpr int kSqTK = 32;  // samples per slice
-constexpr int kSqTN = 64;  // SNPs per CTA
+constexpr int kSqTK = 32;   // samples per slice
+constexpr int kSqTN = 64;   // SNPs per CTA (4 warps x 16)
+constexpr int kSqXLD = 36;  // padded sample stride of a slice's SNP
+constexpr int kSqThreads = 128;
 constexpr int kSqSplitTarget = 148 * 4;  // CTAs to aim for (2 waves at 2 CTAs per SM)
 
 template <int TR>
 struct SqCfg {
-    static constexpr int TY = TR / 8;              // thread rows (8 table rows each)
-    static constexpr int NT = TY * 16;             // threads: 16 thread columns x 4 SNPs
-    static constexpr int XLD = kSqTK + 1;          // padded sample stride of a slice's SNP
+    static_assert(TR % 16 == 8, "row tile must be 8 mod 16 doubles (conflict-free fragments)");
+    static constexpr int RT = TR / 8;              // 8-row MMA tiles
     static constexpr int A_ELEMS = kSqTK * TR;
-    static constexpr int X_ELEMS = kSqTN * XLD;
+    static constexpr int X_ELEMS = kSqTN * kSqXLD;
     static constexpr int STAGE = A_ELEMS + X_ELEMS;  // doubles (even: stages stay 16-byte aligned)
     static constexpr int SMEM = 2 * STAGE * 8;
 };
@@ -1152,14 +1154,22 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// D (8 x 8) += A (8 x 4) B (4 x 8) in FP64; lane l holds A[l/4][l%4], B[l%4][l/4] and
+// D[l/4][2(l%4)], D[l/4][2(l%4)+1].
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
 template <int TR>
-__global__ void __launch_bounds__(SqCfg<TR>::NT, 2)
+__global__ void __launch_bounds__(kSqThreads, 2)
     sq_sums_kernel(const double* __restrict__ AT, int64_t ldt, const double* __restrict__ X,
                    int64_t ldx, int64_t n, int64_t m, int64_t klen, int rows,
                    double* __restrict__ out, int64_t ldo, int64_t zstride) {
     using Cfg = SqCfg<TR>;
     extern __shared__ __align__(16) double sq_smem[];
-    const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int64_t j0 = (int64_t)blockIdx.x * kSqTN;
     const int64_t r0 = (int64_t)blockIdx.y * TR;
     const int64_t kbeg = (int64_t)blockIdx.z * klen;
@@ -1169,25 +1179,26 @@ __global__ void __launch_bounds__(SqCfg<TR>::NT, 2)
     auto issue = [&](int st, int64_t k) {
         double* As = sq_smem + st * Cfg::STAGE;
         double* Xs = As + Cfg::A_ELEMS;
-        for (int e = tid; e < kSqTK * (TR / 2); e += Cfg::NT) {  // A: 16-byte chunks
+        for (int e = tid; e < kSqTK * (TR / 2); e += kSqThreads) {  // A: 16-byte chunks
             const int kk = e / (TR / 2), c = e % (TR / 2);
             const bool ok = k + kk < kend;
             cp_async16(As + kk * TR + 2 * c, AT + (ok ? (k + kk) * ldt : 0) + r0 + 2 * c, ok);
         }
-        for (int e = tid; e < kSqTN * kSqTK; e += Cfg::NT) {  // X: one double per copy
+        for (int e = tid; e < kSqTN * kSqTK; e += kSqThreads) {  // X: one double per copy
             const int jj = e / kSqTK, kk = e % kSqTK;
             const bool ok = (k + kk < kend) && (j0 + jj < m);
-            cp_async8(Xs + jj * Cfg::XLD + kk, X + (ok ? (j0 + jj) * ldx + k + kk : 0), ok);
+            cp_async8(Xs + jj * kSqXLD + kk, X + (ok ? (j0 + jj) * ldx + k + kk : 0), ok);
         }
         cp_async_commit();
     };
 
-    double acc[8][4];
+    double acc[Cfg::RT][2][2];
 #pragma unroll
-    for (int a = 0; a < 8; ++a)
+    for (int a = 0; a < Cfg::RT; ++a)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) acc[a][q] = 0.0;
+        for (int q = 0; q < 2; ++q) acc[a][q][0] = acc[a][q][1] = 0.0;
 
+    const int fr = lane >> 2, fk = lane & 3;  // fragment row (or column) and k of this lane
     if (nsl > 0) issue(0, kbeg);
     for (int s = 0; s < nsl; ++s) {
         if (s + 1 < nsl) {
@@ -1196,43 +1207,40 @@ __global__ void __launch_bounds__(SqCfg<TR>::NT, 2)
         } else {
             cp_async_wait<0>();
         }
-        double* As = sq_smem + (s & 1) * Cfg::STAGE;
-        double* Xs = As + Cfg::A_ELEMS;
+        const double* As = sq_smem + (s & 1) * Cfg::STAGE;
+        double* Xs = sq_smem + (s & 1) * Cfg::STAGE + Cfg::A_ELEMS;
         // square the X elements this thread copied (its own copies have landed)
-        for (int e = tid; e < kSqTN * kSqTK; e += Cfg::NT) {
-            double* v = Xs + (e / kSqTK) * Cfg::XLD + e % kSqTK;
+        for (int e = tid; e < kSqTN * kSqTK; e += kSqThreads) {
+            double* v = Xs + (e / kSqTK) * kSqXLD + e % kSqTK;
             *v = *v * *v;
         }
         __syncthreads();
-#pragma unroll 4
-        for (int kk = 0; kk < kSqTK; ++kk) {
-            const double2* ap = reinterpret_cast<const double2*>(As + kk * TR + ty * 8);
-            double a[8];
+        const double* xb = Xs + (warp * 16 + fr) * kSqXLD + fk;
+        const double* ab = As + fk * TR + fr;
+#pragma unroll 2
+        for (int k0 = 0; k0 < kSqTK; k0 += 4) {
+            const double b0 = xb[k0], b1 = xb[8 * kSqXLD + k0];
 #pragma unroll
-            for (int h = 0; h < 4; ++h) {
-                const double2 v = ap[h];
-                a[2 * h] = v.x;
-                a[2 * h + 1] = v.y;
+            for (int rt = 0; rt < Cfg::RT; ++rt) {
+                const double a = ab[k0 * TR + rt * 8];
+                dmma_8x8x4(acc[rt][0][0], acc[rt][0][1], a, b0);
+                dmma_8x8x4(acc[rt][1][0], acc[rt][1][1], a, b1);
             }
-            double x[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) x[q] = Xs[(tx + 16 * q) * Cfg::XLD + kk];
-#pragma unroll
-            for (int a2 = 0; a2 < 8; ++a2)
-#pragma unroll
-                for (int q = 0; q < 4; ++q) acc[a2][q] = fma(a[a2], x[q], acc[a2][q]);
         }
         __syncthreads();  // the next issue overwrites this stage
     }
     double* o = out + (int64_t)blockIdx.z * zstride;
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int64_t j = j0 + tx + 16 * q;
-        if (j >= m) continue;
+    for (int nt = 0; nt < 2; ++nt) {
 #pragma unroll
-        for (int a = 0; a < 8; ++a) {
-            const int64_t r = r0 + ty * 8 + a;
-            if (r < rows) o[j * ldo + r] = acc[a][q];
+        for (int e = 0; e < 2; ++e) {
+            const int64_t j = j0 + warp * 16 + nt * 8 + 2 * fk + e;
+            if (j >= m) continue;
+#pragma unroll
+            for (int rt = 0; rt < Cfg::RT; ++rt) {
+                const int64_t r = r0 + rt * 8 + fr;
+                if (r < rows) o[j * ldo + r] = acc[rt][nt][e];
+            }
         }
     }
 }
@@ -1653,12 +1661,12 @@ int32_t launch_sq_sums(const double* AT, int64_t rows, const double* X, int64_t 
     if (tr == 56) {
         JB_CUDA(cudaFuncSetAttribute(sq_sums_kernel<56>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      SqCfg<56>::SMEM));
-        sq_sums_kernel<56><<<grid, SqCfg<56>::NT, SqCfg<56>::SMEM, st>>>(
+        sq_sums_kernel<56><<<grid, kSqThreads, SqCfg<56>::SMEM, st>>>(
             AT, ldt, X, ldx, n, m, klen, (int)rows, out, ldo, m * ldt);
     } else {
         JB_CUDA(cudaFuncSetAttribute(sq_sums_kernel<104>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      SqCfg<104>::SMEM));
-        sq_sums_kernel<104><<<grid, SqCfg<104>::NT, SqCfg<104>::SMEM, st>>>(
+        sq_sums_kernel<104><<<grid, kSqThreads, SqCfg<104>::SMEM, st>>>(
             AT, ldt, X, ldx, n, m, klen, (int)rows, out, ldo, m * ldt);
     }
     JB_LAUNCH_CHECK("sq_sums_kernel");

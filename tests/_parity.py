@@ -95,5 +95,14 @@ def strict_fp64_report(got: dict, ref: dict, keys=("beta", "se", "logl_h1", "p_w
         worst = float(r.max()) if r.size else 0.0
         out[k] = worst
         t = (tols or {}).get(k, tol)
-        assert worst <= t, f"{k}: {worst:.3e} > {t} on a SNP whose lambda matches the oracle"
+        if worst > t:
+            out.setdefault("violations", []).append(
+                f"{k}: {worst:.3e} > {t} on a SNP whose lambda matches the oracle")
     return out
+
+
+def assert_strict(rep: dict, min_frac: float = 0.5, label: str = "") -> None:
+    """Fail on a report of :func:`strict_fp64_report` with violations, or with fewer than
+    ``min_frac`` of the SNPs taking every golden-section step as the oracle."""
+    assert not rep.get("violations"), f"{label} {rep['violations']}"
+    assert rep["frac_lambda_matched"] >= min_frac, f"{label} {rep}"

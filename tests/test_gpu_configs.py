@@ -36,7 +36,7 @@ import torch
 from jamma_b200 import synth
 from oracle import lmm as OL
 from oracle import plink as OP
-from _parity import strict_fp64_report
+from _parity import assert_strict, strict_fp64_report
 
 pytestmark = pytest.mark.gpu
 
@@ -139,21 +139,21 @@ def test_forms_against_oracle_and_each_other(name):
         if mode in (1, 4):
             strict["reml"] = strict_fp64_report(plain, ref.stats)
         if mode in (2, 4):
-            # p_lrt also carries logl_H0, whose null lambda0 may sit at a near tie
+            # p_lrt also carries logl_H0: where the null model's own golden search ended one
+            # step apart (a tie below FP64 rounding), logl_H0 moves by ~1e-9
             strict["mle"] = strict_fp64_report(plain, ref.stats, keys=("logl_mle", "p_lrt"),
-                                               lam_key="lambda_mle", tols={"p_lrt": 1e-9})
+                                               lam_key="lambda_mle", tols={"p_lrt": 1e-8})
         if mode in (3, 4):
             lam0 = float(null["fp64"][f])
             strict["null_lambda_rel"] = abs(lam0 - ref.lam0) / ref.lam0
             if strict["null_lambda_rel"] <= 1e-12:
                 a, b = np.asarray(plain["p_score"]), ref.stats["p_score"]
                 ok = np.isfinite(a) & np.isfinite(b)
-                worst = float((np.abs(a[ok] - b[ok]) / np.abs(b[ok])).max())
-                strict["p_score"] = worst
-                assert worst <= 1e-10, f"{name} p_score {worst:.2e} with the oracle's lambda0"
-    for rep in strict_tables.values():
-        for part in ("reml", "mle"):
-            if part in rep:  # at least half the searches take every step as the oracle
-                assert rep[part]["frac_lambda_matched"] >= 0.5, f"{name} {part}: {rep[part]}"
+                strict["p_score"] = float((np.abs(a[ok] - b[ok]) / np.abs(b[ok])).max())
     _TABLE[name] = {"n": n, "snps": p, "n_cvt": c, "phenotypes": phi, "lmm_mode": mode,
                     "comparisons": tables, "fp64_form_strict": strict_tables}
+    for f, rep in strict_tables.items():
+        for part in ("reml", "mle"):
+            if part in rep:  # at least half the searches take every step as the oracle
+                assert_strict(rep[part], 0.5, f"{name} phenotype {f} {part}")
+        assert rep.get("p_score", 0.0) <= 1e-10, f"{name} p_score with the oracle's lambda0: {rep}"

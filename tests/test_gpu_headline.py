@@ -9,8 +9,9 @@ tcgen05 rotation, series-interpolated lambda search) and jamma's path restated i
 
 * plain form: on every SNP whose REML (MLE) lambda matches the oracle's to 1e-12 -- every
   golden-section decision taken the same way, at least half of the SNPs -- beta, se,
-  logl_H1 and p_wald (logl_mle) agree to 1e-10 relative and p_lrt to 1e-9 (it also carries
-  the null model's logl_H0); with the oracle's null lambda0, every p_score agrees to 1e-10;
+  logl_H1 and p_wald (logl_mle) agree to 1e-10 relative and p_lrt to 1e-8 (it also carries
+  the null model's logl_H0, whose own golden search can end one step apart at an FP64 tie);
+  with the oracle's null lambda0, every p_score agrees to 1e-10;
   lambda itself always within the golden bracket; identical calls at 5e-8.
 * mixed form: every |log10 p| error below 1e-4 and identical calls at 5e-8; p within 1e-6
   relative for at least 98 % of SNPs (the rest are golden-section steps on flat
@@ -23,7 +24,7 @@ import numpy as np
 import pytest
 import torch
 
-from _parity import strict_fp64_report
+from _parity import assert_strict, strict_fp64_report
 from jamma_b200 import synth
 from oracle import lmm as OL
 from oracle import plink as OP
@@ -89,9 +90,10 @@ def test_headline_fp64_form_matches_oracle(cohort20k):
     _pvalue_checks(got, ref, 0.98)
     reml = strict_fp64_report(got, ref.stats)
     mle = strict_fp64_report(got, ref.stats, keys=("logl_mle", "p_lrt"), lam_key="lambda_mle",
-                             tols={"p_lrt": 1e-9})
-    assert reml["frac_lambda_matched"] >= 0.5 and mle["frac_lambda_matched"] >= 0.5, (reml, mle)
+                             tols={"p_lrt": 1e-8})
     print(f"headline fp64 form vs oracle: {reml} {mle}")
+    assert_strict(reml, 0.5, "REML")
+    assert_strict(mle, 0.5, "MLE")
     for k in ("lambda_remle", "lambda_mle"):
         rel = np.abs(got[k] - ref.stats[k]) / ref.stats[k]
         assert rel.max() <= 1e-4, f"{k}: {rel.max():.2e} outside the golden bracket"
