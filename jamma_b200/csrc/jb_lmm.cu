@@ -1105,11 +1105,11 @@ __global__ void lmm_gemm_tables_kernel(int64_t n, int n_grid, int phi, const dou
 //   * the samples are split over kz = blockIdx.z ranges when the SNP tiles alone cannot
 //     fill the GPU; partial sums go to P[(kz*m + j)*ldt + r] and sq_reduce_kernel adds
 //     them in kz order, so every sum has a fixed order (bit-reproducible).
-constexpr int kSqTK = 32;   // samples per slice
+constexpr int kSqTK = 16;   // samples per slice
 constexpr int kSqTN = 64;   // SNPs per CTA (4 warps x 16)
-constexpr int kSqXLD = 36;  // padded sample stride of a slice's SNP
+constexpr int kSqXLD = 20;  // padded sample stride of a slice's SNP
 constexpr int kSqThreads = 128;
-constexpr int kSqSplitTarget = 148 * 4;  // CTAs to aim for (2 waves at 2 CTAs per SM)
+constexpr int kSqSlots = 148 * 3;  // CTAs resident at once on a B200 (3 per SM)
 
 template <int TR>
 struct SqCfg {
@@ -1127,13 +1127,26 @@ inline int64_t sq_ldt(int64_t rows) {
     const int tr = sq_tile_rows(rows);
     return ceil_div(rows, tr) * tr;
 }
-// Sample-range split: enough CTAs to fill the GPU, each range at least 8 slices long.
+// Sample-range split: at least four waves of CTAs, and among the splits up to twice that
+// the one whose last wave is fullest (every CTA does the same work, so a part-filled last
+// wave is idle hardware); each range at least four slices long.
 inline int sq_split(int64_t n, int64_t m, int64_t rows) {
     const int64_t tiles = ceil_div(m, kSqTN) * (sq_ldt(rows) / sq_tile_rows(rows));
-    int64_t ks = ceil_div(kSqSplitTarget, tiles);
-    const int64_t kmax = ceil_div(n, 8 * kSqTK);
-    if (ks > kmax) ks = kmax;
-    return (int)(ks < 1 ? 1 : ks);
+    const int64_t kmax = ceil_div(n, 4 * kSqTK);
+    int64_t k0 = ceil_div(4 * kSqSlots, tiles);
+    if (k0 > kmax) k0 = kmax;
+    if (k0 < 1) k0 = 1;
+    int64_t best = k0;
+    double best_eff = 0.0;
+    for (int64_t ks = k0; ks <= 2 * k0 && ks <= kmax; ++ks) {
+        const int64_t units = tiles * ks;
+        const double eff = (double)units / (double)(ceil_div(units, kSqSlots) * kSqSlots);
+        if (eff > best_eff + 1e-9) {
+            best_eff = eff;
+            best = ks;
+        }
+    }
+    return (int)best;
 }
 
 __device__ __forceinline__ void cp_async16(double* dst, const double* src, bool valid) {
@@ -1163,7 +1176,7 @@ __device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, dou
 }
 
 template <int TR>
-__global__ void __launch_bounds__(kSqThreads, 2)
+__global__ void __launch_bounds__(kSqThreads, 3)
     sq_sums_kernel(const double* __restrict__ AT, int64_t ldt, const double* __restrict__ X,
                    int64_t ldx, int64_t n, int64_t m, int64_t klen, int rows,
                    double* __restrict__ out, int64_t ldo, int64_t zstride) {
@@ -1217,7 +1230,7 @@ __global__ void __launch_bounds__(kSqThreads, 2)
         __syncthreads();
         const double* xb = Xs + (warp * 16 + fr) * kSqXLD + fk;
         const double* ab = As + fk * TR + fr;
-#pragma unroll 2
+#pragma unroll
         for (int k0 = 0; k0 < kSqTK; k0 += 4) {
             const double b0 = xb[k0], b1 = xb[8 * kSqXLD + k0];
 #pragma unroll
