@@ -353,7 +353,7 @@ def pass1_counts(bed, sample_idx: torch.Tensor | None, n: int, chunk: int = 1638
         b = ci % 2
         if rng[b] is not None:
             collect(b)  # chunk ci-2: its upload has read pin[b], its counts are back
-        pin[b].numpy()[: e - s] = bed.records[s:e]
+        bed.read_into(s, e, pin[b].numpy())
         dev[b][: e - s].copy_(pin[b][: e - s], non_blocking=True)
         _native.call("jb_decode_bed", ptr(dev[b]), bps, e - s, ptr(sample_idx), n, ptr(codes), n,
                      ptr(cnt), stream_handle())

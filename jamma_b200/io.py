@@ -7,6 +7,7 @@ Host-side text and byte handling only.  Layouts follow jamma:
 
 from __future__ import annotations
 
+import os
 from dataclasses import dataclass
 from pathlib import Path
 
@@ -73,6 +74,12 @@ class BedFile:
                 f"{self.n_samples} samples x {self.n_snps} SNPs"
             )
         self.records = raw[3:].reshape(self.n_snps, self.bytes_per_snp)
+        self._fd = os.open(self.path, os.O_RDONLY)
+
+    def __del__(self):
+        fd = getattr(self, "_fd", None)
+        if fd is not None:
+            os.close(fd)
 
     def read(self, start: int, end: int) -> np.ndarray:
         return np.ascontiguousarray(self.records[start:end])
@@ -80,10 +87,29 @@ class BedFile:
     def take(self, idx: np.ndarray) -> np.ndarray:
         return np.ascontiguousarray(self.records[np.asarray(idx)])
 
+    def read_into(self, start: int, end: int, out: np.ndarray) -> None:
+        """Records of SNPs start..end into the C-contiguous uint8 array ``out`` (e.g. a
+        pinned staging buffer) by positioned reads: far faster than touching the memory
+        map page by page."""
+        mv = memoryview(out).cast("B")[: (end - start) * self.bytes_per_snp]
+        off, done = 3 + start * self.bytes_per_snp, 0
+        while done < len(mv):
+            got = os.preadv(self._fd, [mv[done:]], off + done)
+            if got <= 0:
+                raise OSError(f"{self.path}: short read at byte {off + done}")
+            done += got
+
     def take_into(self, idx: np.ndarray, out: np.ndarray) -> None:
-        """Copy the records of SNPs ``idx`` into ``out`` (len(idx), bytes_per_snp), e.g. a
-        pinned staging buffer, without an intermediate array."""
-        np.take(self.records, np.asarray(idx), axis=0, out=out)
+        """Copy the records of SNPs ``idx`` into ``out`` (len(idx), bytes_per_snp), one
+        positioned read per run of consecutive SNPs."""
+        idx = np.asarray(idx, dtype=np.int64)
+        if idx.size == 0:
+            return
+        cut = np.flatnonzero(np.diff(idx) != 1) + 1
+        starts = np.concatenate(([0], cut))
+        ends = np.concatenate((cut, [idx.size]))
+        for a, b in zip(starts.tolist(), ends.tolist()):
+            self.read_into(int(idx[a]), int(idx[a]) + (b - a), out[a:b])
 
 
 def read_snp_list_file(path) -> set[str]:
