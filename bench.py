@@ -696,9 +696,11 @@ def run_ours(args) -> None:
         }
         n_tests_f = int(args.mode in (1, 4)) + int(args.mode in (3, 4))
         series = cohort_mixed.series_ws is not None
-        # own kernels per step: decode, [pack pairs], tiles + rotation GEMM, [tiles + series
-        # GEMM], square, search, F-test p-values (the cuBLAS DGEMM is not counted)
-        launches = (1 + int(has_missing) + 2 + 2 * int(series) + 2 + n_tests_f) * args.steps
+        # own kernels per step (no library kernel in the mixed form): decode, [pack pairs],
+        # tiles + rotation GEMM, [tiles + series GEMM], squared sums + their reduction,
+        # search, [F-test p-values]
+        launches = (1 + int(has_missing) + 2 + 2 * int(series) + 2 + 1 + int(n_tests_f > 0)) \
+            * args.steps
         line = {
             "metric": "lmm_assoc_snps_per_s", "value": value, "unit": "SNPs/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,

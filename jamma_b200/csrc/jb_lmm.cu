@@ -1094,13 +1094,13 @@ __global__ void lmm_gemm_tables_kernel(int64_t n, int n_grid, int phi, const dou
 // CQ[j*ldcq + r] = sum_i A[i, r] x_ij^2 (r < rows) for every SNP j of a rotated chunk X
 // (column-major, ld ldx): the squared weighted sums of every table row.  One fused kernel
 // reads each rotated genotype once, squares it in shared memory and forms the product with
-// the row table on the FP64 tensor cores (mma.sync m16n8k8 .f64), so X^2 never goes to HBM.
+// the row table on the FP64 tensor cores (mma.sync m8n8k4 .f64), so X^2 never goes to HBM.
 //   * A is held transposed, AT[i*ldt + r] (ldt a multiple of the row tile, zero for
 //     r >= rows), so a slice of kSqTK samples is one contiguous block per row tile;
 //   * a CTA owns TR rows x kSqTN SNPs for one range of samples; warp w owns SNPs
-//     16w..16w+15 (two 8-column MMA tiles) for all TR/16 row tiles of the CTA;
-//   * shared layouts As[k][TR + 8] (a row stride of 8 mod 16 doubles) and Xs[j][kSqXLD]
-//     (kSqXLD = 4 mod 16) make every 32-lane fragment load two conflict-free wavefronts;
+//     16w..16w+15 (two 8-column MMA tiles) for all TR/8 row tiles of the CTA;
+//   * shared layouts As[k][TR] (TR = 8 mod 16 doubles) and Xs[j][kSqXLD] (kSqXLD = 4 mod
+//     16) make every 32-lane fragment load two conflict-free wavefronts;
 //   * slices are double-buffered with cp.async; out-of-range samples and SNPs read as zero;
 //   * the samples are split over kz = blockIdx.z ranges when the SNP tiles alone cannot
 //     fill the GPU; partial sums go to P[(kz*m + j)*ldt + r] and sq_reduce_kernel adds
@@ -1113,17 +1113,16 @@ constexpr int kSqSlots = 148 * 3;  // CTAs resident at once on a B200 (3 per SM)
 
 template <int TR>
 struct SqCfg {
-    static_assert(TR % 16 == 0, "row tile must be a multiple of the 16-row MMA tile");
-    static constexpr int RT = TR / 16;             // 16-row MMA tiles
-    static constexpr int TRP = TR + 8;             // shared row stride: 8 mod 16 doubles
-    static constexpr int A_ELEMS = kSqTK * TRP;
+    static_assert(TR % 16 == 8, "row tile must be 8 mod 16 doubles (conflict-free fragments)");
+    static constexpr int RT = TR / 8;              // 8-row MMA tiles
+    static constexpr int A_ELEMS = kSqTK * TR;
     static constexpr int X_ELEMS = kSqTN * kSqXLD;
     static constexpr int STAGE = A_ELEMS + X_ELEMS;  // doubles (even: stages stay 16-byte aligned)
     static constexpr int SMEM = 2 * STAGE * 8;
 };
 
 // Row tile for a table of `rows` rows and the matching padded leading dimension of AT.
-inline int sq_tile_rows(int64_t rows) { return rows <= 64 ? 64 : 112; }
+inline int sq_tile_rows(int64_t rows) { return rows <= 56 ? 56 : 104; }
 inline int64_t sq_ldt(int64_t rows) {
     const int tr = sq_tile_rows(rows);
     return ceil_div(rows, tr) * tr;
@@ -1168,16 +1167,12 @@ __device__ __forceinline__ void cp_async_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// D (16 x 8) += A (16 x 8) B (8 x 8) in FP64.  With g = lane / 4 and t = lane % 4, a lane
-// holds A[g][t], A[g+8][t], A[g][t+4], A[g+8][t+4]; B[t][g], B[t+4][g]; and D[g][2t],
-// D[g][2t+1], D[g+8][2t], D[g+8][2t+1].
-__device__ __forceinline__ void dmma_16x8x8(double (&d)[4], const double (&a)[4], double b0,
-                                            double b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k8.row.col.f64.f64.f64.f64 {%0, %1, %2, %3}, {%4, %5, %6, %7}, "
-        "{%8, %9}, {%0, %1, %2, %3};"
-        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
-        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(b0), "d"(b1));
+// D (8 x 8) += A (8 x 4) B (4 x 8) in FP64; lane l holds A[l/4][l%4], B[l%4][l/4] and
+// D[l/4][2(l%4)], D[l/4][2(l%4)+1].
+__device__ __forceinline__ void dmma_8x8x4(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
 }
 
 template <int TR>
@@ -1200,7 +1195,7 @@ __global__ void __launch_bounds__(kSqThreads, 3)
         for (int e = tid; e < kSqTK * (TR / 2); e += kSqThreads) {  // A: 16-byte chunks
             const int kk = e / (TR / 2), c = e % (TR / 2);
             const bool ok = k + kk < kend;
-            cp_async16(As + kk * Cfg::TRP + 2 * c, AT + (ok ? (k + kk) * ldt : 0) + r0 + 2 * c, ok);
+            cp_async16(As + kk * TR + 2 * c, AT + (ok ? (k + kk) * ldt : 0) + r0 + 2 * c, ok);
         }
         for (int e = tid; e < kSqTN * kSqTK; e += kSqThreads) {  // X: one double per copy
             const int jj = e / kSqTK, kk = e % kSqTK;
@@ -1210,13 +1205,11 @@ __global__ void __launch_bounds__(kSqThreads, 3)
         cp_async_commit();
     };
 
-    double acc[Cfg::RT][2][4];
+    double acc[Cfg::RT][2][2];
 #pragma unroll
     for (int a = 0; a < Cfg::RT; ++a)
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) acc[a][q][e] = 0.0;
+        for (int q = 0; q < 2; ++q) acc[a][q][0] = acc[a][q][1] = 0.0;
 
     const int fr = lane >> 2, fk = lane & 3;  // fragment row (or column) and k of this lane
     if (nsl > 0) issue(0, kbeg);
@@ -1236,18 +1229,15 @@ __global__ void __launch_bounds__(kSqThreads, 3)
         }
         __syncthreads();
         const double* xb = Xs + (warp * 16 + fr) * kSqXLD + fk;
-        const double* ab = As + fk * Cfg::TRP + fr;
+        const double* ab = As + fk * TR + fr;
 #pragma unroll
-        for (int k0 = 0; k0 < kSqTK; k0 += 8) {
-            // B fragments of the warp's two 8-SNP tiles: X^2[k0 + t (+4)][SNP g]
-            const double b00 = xb[k0], b01 = xb[k0 + 4];
-            const double b10 = xb[8 * kSqXLD + k0], b11 = xb[8 * kSqXLD + k0 + 4];
+        for (int k0 = 0; k0 < kSqTK; k0 += 4) {
+            const double b0 = xb[k0], b1 = xb[8 * kSqXLD + k0];
 #pragma unroll
             for (int rt = 0; rt < Cfg::RT; ++rt) {
-                const double* ap = ab + k0 * Cfg::TRP + rt * 16;
-                const double a[4] = {ap[0], ap[8], ap[4 * Cfg::TRP], ap[4 * Cfg::TRP + 8]};
-                dmma_16x8x8(acc[rt][0], a, b00, b01);
-                dmma_16x8x8(acc[rt][1], a, b10, b11);
+                const double a = ab[k0 * TR + rt * 8];
+                dmma_8x8x4(acc[rt][0][0], acc[rt][0][1], a, b0);
+                dmma_8x8x4(acc[rt][1][0], acc[rt][1][1], a, b1);
             }
         }
         __syncthreads();  // the next issue overwrites this stage
@@ -1256,12 +1246,12 @@ __global__ void __launch_bounds__(kSqThreads, 3)
 #pragma unroll
     for (int nt = 0; nt < 2; ++nt) {
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-            const int64_t j = j0 + warp * 16 + nt * 8 + 2 * fk + (e & 1);
+        for (int e = 0; e < 2; ++e) {
+            const int64_t j = j0 + warp * 16 + nt * 8 + 2 * fk + e;
             if (j >= m) continue;
 #pragma unroll
             for (int rt = 0; rt < Cfg::RT; ++rt) {
-                const int64_t r = r0 + rt * 16 + fr + 8 * (e >> 1);
+                const int64_t r = r0 + rt * 8 + fr;
                 if (r < rows) o[j * ldo + r] = acc[rt][nt][e];
             }
         }
@@ -1681,15 +1671,15 @@ int32_t launch_sq_sums(const double* AT, int64_t rows, const double* X, int64_t 
     dim3 grid((unsigned)gx, (unsigned)(ldt / tr), (unsigned)ks);
     double* out = ks > 1 ? P : CQ;
     const int64_t ldo = ks > 1 ? ldt : ldcq;
-    if (tr == 64) {
-        JB_CUDA(cudaFuncSetAttribute(sq_sums_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     SqCfg<64>::SMEM));
-        sq_sums_kernel<64><<<grid, kSqThreads, SqCfg<64>::SMEM, st>>>(
+    if (tr == 56) {
+        JB_CUDA(cudaFuncSetAttribute(sq_sums_kernel<56>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     SqCfg<56>::SMEM));
+        sq_sums_kernel<56><<<grid, kSqThreads, SqCfg<56>::SMEM, st>>>(
             AT, ldt, X, ldx, n, m, klen, (int)rows, out, ldo, m * ldt);
     } else {
-        JB_CUDA(cudaFuncSetAttribute(sq_sums_kernel<112>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     SqCfg<112>::SMEM));
-        sq_sums_kernel<112><<<grid, kSqThreads, SqCfg<112>::SMEM, st>>>(
+        JB_CUDA(cudaFuncSetAttribute(sq_sums_kernel<104>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     SqCfg<104>::SMEM));
+        sq_sums_kernel<104><<<grid, kSqThreads, SqCfg<104>::SMEM, st>>>(
             AT, ldt, X, ldx, n, m, klen, (int)rows, out, ldo, m * ldt);
     }
     JB_LAUNCH_CHECK("sq_sums_kernel");

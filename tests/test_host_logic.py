@@ -123,3 +123,23 @@ def test_sd_from_counts_matches_imputed_variance():
     ref = np.sqrt(np.maximum(np.mean(gi**2, axis=0) - mu**2, 0))
     np.testing.assert_allclose(sd, ref, rtol=1e-13, atol=1e-15)
     assert sd[3] == 0.0
+
+
+def test_bed_positioned_reads_match_the_records(tmp_path):
+    """BedFile.read_into / take_into (positioned reads into a caller buffer, used to fill
+    the pinned staging buffers) return the same bytes as the memory-mapped records, for
+    runs of consecutive SNPs and scattered ones."""
+    from jamma_b200.io import BedFile, write_plink_records
+
+    rng = np.random.default_rng(3)
+    rec = rng.integers(0, 256, size=(700, 26), dtype=np.uint8)
+    write_plink_records(tmp_path / "c", rec, 101)
+    bed = BedFile(tmp_path / "c")
+    out = np.zeros((40, 26), dtype=np.uint8)
+    bed.read_into(650, 690, out)
+    np.testing.assert_array_equal(out, rec[650:690])
+    idx = np.array([0, 1, 2, 9, 10, 300, 698, 699])
+    got = np.zeros((idx.size, 26), dtype=np.uint8)
+    bed.take_into(idx, got)
+    np.testing.assert_array_equal(got, rec[idx])
+    np.testing.assert_array_equal(bed.records[idx], rec[idx])
