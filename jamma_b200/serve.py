@@ -16,6 +16,7 @@ per-job buffers and a fixed chunk width, so its results do not depend on what el
 
 from __future__ import annotations
 
+import functools
 import threading
 import time
 from collections import OrderedDict, deque
@@ -86,8 +87,19 @@ class _Active:
         self.bytes = 0
 
 
-def job_device_bytes(n: int, phi: int, n_cvt: int, chunk: int, resident: bool) -> int:
-    """Device bytes a job holds while it runs (cohort state counted when not resident)."""
+@functools.lru_cache(maxsize=256)
+def _eigh_workspace_bytes(n: int) -> int:
+    return int(_native.load().jb_eigh_workspace_size(n))
+
+
+def job_device_bytes(n: int, phi: int, n_cvt: int, chunk: int, resident: bool,
+                     n_snps: int = 0) -> int:
+    """Device bytes a job holds while it runs (cohort state counted when not resident).
+
+    A job that builds its cohort also needs, at the peak of its set-up, the largest of the
+    INT8 kinship's operands (n x p int8 calls + FP64 correction matrix + int32 Gram), the
+    finalisation (correction + Gram + kinship) and the eigendecomposition (matrix +
+    solver workspace), on top of the digit planes it keeps."""
     lib = _native.load()
     b = lib.jb_lmm_workspace_size(n, n_cvt, phi, 50) + lib.jb_lmm_chunk_workspace_size(
         n, n_cvt, phi, 50, chunk)
@@ -95,7 +107,10 @@ def job_device_bytes(n: int, phi: int, n_cvt: int, chunk: int, resident: bool) -
     b += 9 * phi * chunk * 8 + 2 * n * (n_cvt + phi) * 8
     b += lib.jb_lmm_series_workspace_size(n, n_cvt, phi)
     if not resident:
-        b += 8 * n * n * 2 + lib.jb_ozaki_workspace_size(n) + n * 8  # K / U, digits, evals
+        nn = n * n
+        build = max(n * ((n_snps + 127) // 128 * 128) + 12 * nn, 20 * nn,
+                    8 * nn + _eigh_workspace_bytes(n))
+        b += build + lib.jb_ozaki_workspace_size(n) + n * 8
     return int(b)
 
 
@@ -142,7 +157,8 @@ class GwasServer:
             c = 1 if job.covariates is None else job.covariates.shape[1]
             with self._lock:
                 known = job.cohort_id in self.cohorts or job.cohort_id in self._building
-                need = job_device_bytes(job.n_samples, phi, c, self.chunk, known)
+                need = job_device_bytes(job.n_samples, phi, c, self.chunk, known,
+                                        n_snps=int(np.shape(job.packed)[0]))
                 self._evict_for(need)
                 if self.used + self._resident_bytes() + need > self.budget:
                     if not self.active and not self.preparing:
