@@ -573,6 +573,24 @@ def run_ours(args) -> None:
     ms, kern_ms, clocks, outs = run_form("mixed", args.steps)
     if c_status := cohort_mixed.rotate_status():
         raise RuntimeError(f"INT8 rotation pipeline status {c_status}")
+    if args.traffic_sweep:  # one rotation per candidate tile schedule, as the profiler range
+        from jamma_b200 import autotune as _at
+
+        gm0, gn0 = np.zeros(1, np.int32), np.zeros(1, np.int32)
+        _native.call("jb_rotate_get_schedule", gm0.ctypes.data, gn0.ctypes.data)
+        k0 = _native.load().jb_rotate_get_kernel()
+        _native.call("jb_rotate_set_kernel", 0)
+        _native.call("jb_decode_bed", ptr(rec[:m]), bps, m, None, n, ptr(codes), ld, ptr(counts),
+                     stream_handle())
+        for gm, gn in _at.SCHEDULES:
+            _native.call("jb_rotate_set_schedule", gm, gn)
+            torch.cuda.synchronize()
+            torch.cuda.profiler.start()
+            cohort_mixed.rotate_codes_i8(codes, means[0], has_missing, out=UtG)
+            torch.cuda.synchronize()
+            torch.cuda.profiler.stop()
+        _native.call("jb_rotate_set_kernel", k0)
+        _native.call("jb_rotate_set_schedule", int(gm0[0]), int(gn0[0]))
     snps = args.steps * m * world
     value = snps / (ms / 1e3)
     fp64_steps = max(1, min(args.steps, args.fp64_steps))
@@ -916,7 +934,10 @@ def main():
     ap.add_argument("--pheno-chunk", type=int, default=2048)
     ap.add_argument("--pheno-mode", type=int, default=4)
     ap.add_argument("--no-autotune", action="store_true")
-    ap.add_argument("--profile-phase", choices=["assoc", "kinship", "multi"], default="assoc",
+    ap.add_argument("--traffic-sweep", action="store_true",
+                    help="after the timed steps, one rotation per candidate tile schedule (one-CTA "
+                         "kernel) as the profiler range, for ncu's DRAM byte counts")
+    ap.add_argument("--profile-phase", choices=["assoc", "kinship", "multi", "none"], default="assoc",
                     help="which phase torch.cuda.profiler.start/stop brackets")
     ap.add_argument("--rot-kernel", type=int, choices=[0, 1], default=None,
                     help="fix the INT8 rotation kernel (0 one CTA per tile, 1 CTA pairs)")
