@@ -50,6 +50,20 @@ def snp_info_from_meta(meta: dict) -> list[dict]:
     ]
 
 
+_READ_THREADS = 4
+_READ_SPLIT_BYTES = 8 << 20
+_READ_POOL = None
+
+
+def _read_pool():
+    global _READ_POOL
+    if _READ_POOL is None:
+        from concurrent.futures import ThreadPoolExecutor
+
+        _READ_POOL = ThreadPoolExecutor(max_workers=_READ_THREADS, thread_name_prefix="jb-bed")
+    return _READ_POOL
+
+
 class BedFile:
     """Memory-mapped SNP-major .bed records: ``records[j]`` is SNP j's packed bytes."""
 
@@ -87,17 +101,30 @@ class BedFile:
     def take(self, idx: np.ndarray) -> np.ndarray:
         return np.ascontiguousarray(self.records[np.asarray(idx)])
 
-    def read_into(self, start: int, end: int, out: np.ndarray) -> None:
-        """Records of SNPs start..end into the C-contiguous uint8 array ``out`` (e.g. a
-        pinned staging buffer) by positioned reads: far faster than touching the memory
-        map page by page."""
-        mv = memoryview(out).cast("B")[: (end - start) * self.bytes_per_snp]
-        off, done = 3 + start * self.bytes_per_snp, 0
+    def _pread(self, mv: memoryview, off: int) -> None:
+        done = 0
         while done < len(mv):
             got = os.preadv(self._fd, [mv[done:]], off + done)
             if got <= 0:
                 raise OSError(f"{self.path}: short read at byte {off + done}")
             done += got
+
+    def read_into(self, start: int, end: int, out: np.ndarray) -> None:
+        """Records of SNPs start..end into the C-contiguous uint8 array ``out`` (e.g. a
+        pinned staging buffer) by positioned reads -- far faster than touching the memory
+        map page by page -- split over a few threads for large reads (the reads release
+        the GIL)."""
+        mv = memoryview(out).cast("B")[: (end - start) * self.bytes_per_snp]
+        off = 3 + start * self.bytes_per_snp
+        parts = min(_READ_THREADS, len(mv) // _READ_SPLIT_BYTES)
+        if parts <= 1:
+            self._pread(mv, off)
+            return
+        step = -(-len(mv) // parts)
+        futs = [_read_pool().submit(self._pread, mv[a:a + step], off + a)
+                for a in range(0, len(mv), step)]
+        for f in futs:
+            f.result()
 
     def take_into(self, idx: np.ndarray, out: np.ndarray) -> None:
         """Copy the records of SNPs ``idx`` into ``out`` (len(idx), bytes_per_snp), one
