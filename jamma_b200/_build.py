@@ -11,6 +11,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
@@ -44,16 +45,17 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     nvcc = str(cuda / "bin" / "nvcc")
     out_dir = HERE / "_objs"
     out_dir.mkdir(exist_ok=True)
-    objs = []
     common = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
                      "-I", str(HERE.parent / "include")]
-    for src in srcs:
-        obj = out_dir / (src.stem + ".o")
-        cmd = [nvcc, "-c", str(src), "-o", str(obj)] + common
-        if verbose:
-            print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
-        objs.append(str(obj))
+    cmds = [[nvcc, "-c", str(src), "-o", str(out_dir / (src.stem + ".o"))] + common for src in srcs]
+    objs = [c[4] for c in cmds]
+    if verbose:
+        for c in cmds:
+            print(" ".join(c))
+    # the translation units are independent: compile them side by side
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as pool:
+        for f in [pool.submit(subprocess.run, c, check=True) for c in cmds]:
+            f.result()
     tmp = LIB.with_suffix(".so.tmp")
     link = [nvcc, "-shared", "-o", str(tmp)] + ARCH + objs + [
         "-L", str(cuda / "lib64"), "-lcublas", "-lcusolver", "-ldl",
