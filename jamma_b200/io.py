@@ -354,7 +354,7 @@ def write_gemma_log(output_dir, prefix: str, params: dict, timing: dict, command
     return path
 
 
-@dataclass
+@dataclass(slots=True)
 class AssocResult:
     """One SNP's association record (``AssocResult``, src/jamma/lmm/stats.py:39-64)."""
 

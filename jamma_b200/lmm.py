@@ -90,22 +90,34 @@ class _Stats:
         self.idx = np.where(keep)[0]
 
 
+_ORDER = ("beta", "se", "logl_H1", "l_remle", "p_wald", "p_score", "l_mle", "p_lrt")
+
+
 def _build_results(mode: int, snp_idx, af, n_miss, snp_info, arrays, f: int = 0):
-    """One AssocResult per tested SNP (``_build_results_*``, src/jamma/lmm/results.py:37-286)."""
-    cols = {field: arrays[key][f].tolist() for key, field in _FIELD.items()
-            if key in arrays and not (mode == 2 and field in ("beta", "se"))}
-    af_l, miss_l = np.asarray(af, dtype=np.float64).tolist(), np.asarray(n_miss).astype(int).tolist()
+    """One AssocResult per tested SNP (``_build_results_*``, src/jamma/lmm/results.py:37-286).
+
+    Built column-wise: each AssocResult field is one list over the SNPs, and the records
+    are made positionally from their zip (mode 2 has no beta/se: NaN; other absent
+    statistics are None)."""
+    idx = np.asarray(snp_idx).tolist()
+    k = len(idx)
+    info = [snp_info[j] for j in idx]
     nan = float("nan")
-    out = []
-    for k, j in enumerate(np.asarray(snp_idx).tolist()):
-        s = snp_info[j]
-        kw = dict(chr=s["chr"], rs=s["rs"], ps=s.get("pos", s.get("ps", 0)), n_miss=miss_l[k],
-                  allele1=s.get("a1", s.get("allele1", "")), allele0=s.get("a0", s.get("allele0", "")),
-                  af=af_l[k], beta=nan, se=nan)
-        for field, v in cols.items():
-            kw[field] = v[k]
-        out.append(AssocResult(**kw))
-    return out
+    stats = {field: arrays[key][f].tolist() for key, field in _FIELD.items()
+             if key in arrays and not (mode == 2 and field in ("beta", "se"))}
+    cols = [
+        [s["chr"] for s in info],
+        [s["rs"] for s in info],
+        [s.get("pos", s.get("ps", 0)) for s in info],
+        np.asarray(n_miss).astype(int).tolist(),
+        [s.get("a1", s.get("allele1", "")) for s in info],
+        [s.get("a0", s.get("allele0", "")) for s in info],
+        np.asarray(af, dtype=np.float64).tolist(),
+    ]
+    for field in _ORDER:
+        cols.append(stats[field] if field in stats else
+                    [nan] * k if field in ("beta", "se") else [None] * k)
+    return [AssocResult(*row) for row in zip(*cols)]
 
 
 def associate_records(cohort: eng.DeviceCohort, records, n_file: int, sample_idx, means: np.ndarray,
