@@ -763,7 +763,13 @@ def run_ours(args) -> None:
 
 def run_serving_only(args) -> None:
     """The serving configuration alone (``--serve-c4``): one JSON line with its latency
-    percentiles, phase split and aggregate throughput."""
+    percentiles, phase split and aggregate throughput.
+
+    Cohorts of 2 000 to 40 000 samples come and go, so the process runs PyTorch's caching
+    allocator with expandable segments: with fixed segments, the freed multi-GB kinship and
+    eigensolver buffers were cut up by later, smaller allocations until a 5 GB request
+    failed with 91 GB cached but unallocated."""
+    os.environ.setdefault("PYTORCH_CUDA_ALLOC_CONF", "expandable_segments:True")
     import torch
 
     from jamma_b200 import _build

@@ -827,6 +827,87 @@ __device__ __forceinline__ void beta_se(const PabOut<C>& pb, double px_yy, doubl
     se = valid ? sqrt(var) : jnan();
 }
 
+// Mixed form at large lambda.  The series' error in an x-dependent sum is fixed in absolute
+// terms (a small fraction of the sum's size at small lambda, where every weight
+// 1/(lambda e_i + 1) is near 1), while the sums the statistics use shrink like
+// 1/(lambda e): at lambda = 1e5 the projected P_xy, P_xx are ~1e-5 of their small-lambda
+// size and the score and LRT p-values moved by up to 2e-4 relative against the FP64 form
+// (n = 20 000, 64 phenotypes whose null lambda sat on the upper bound).  The error grows
+// about linearly in lambda (4e-8 at lambda = 10), so every final evaluation at
+// lambda >= kDirectLam -- the score at the null lambda, the MLE and REML optima -- reduces
+// its sums directly in FP64 over the rotated genotypes instead (one pass over x).  The
+// search itself stays on the series.
+constexpr double kDirectLam = 20.0;
+constexpr double kLogDirectLam = 2.995732273553991;  // log(kDirectLam)
+
+// Score statistic of the pairs whose null lambda is >= kDirectLam, from direct FP64 sums;
+// the whole warp evaluates each such pair of its 32 / GW groups in turn and the group's
+// lane 0 overwrites what the series evaluation wrote.
+template <int C, int GW>
+__device__ __forceinline__ void direct_score(const Params& p, int64_t j, int f, bool valid_pair) {
+#pragma unroll 1
+    for (int h = 0; h < 32 / GW; ++h) {
+        const int src = h * GW;
+        const int fh = __shfl_sync(kFull, f, src);
+        if (!(p.lam0[fh] >= kDirectLam)) continue;  // the same decision in every lane
+        const long long jh = __shfl_sync(kFull, (long long)j, src);
+        const bool vh = __shfl_sync(kFull, (int)valid_pair, src) != 0;
+        double row0[Lay<C>::NI], logdet;
+        eval_full<C>(p, p.G + jh * p.ldg, p.Y + (int64_t)fh * p.ldy, p.lam0[fh], row0, logdet);
+        const PabOut<C> pb = pab_reduce<C>(row0);
+        bool valid;
+        double beta, tau, se;
+        beta_se<C>(pb, clamp_pyy(pb.yy1), p.df, valid, beta, tau, se);
+        const double fstat = p.n_d * (pb.xy * pb.xy) / (pb.yy * (valid ? pb.xx : 1.0));
+        if ((int)(threadIdx.x & 31) == src && vh) {
+            const int64_t o = (int64_t)fh * p.m + jh;
+            if (p.out.p_score) p.out.p_score[o] = valid ? fstat : jnan();
+            if (p.mode == 3) {
+                if (p.out.beta) p.out.beta[o] = beta;
+                if (p.out.se) p.out.se[o] = se;
+            }
+        }
+    }
+}
+
+// Final MLE / REML evaluations of the pairs whose optimum is at lambda >= kDirectLam, from
+// direct FP64 sums; each group keeps its own pair's values.
+template <int C, int GW>
+__device__ __forceinline__ void direct_final(const Params& p, int64_t j, int f,
+                                             const double (&log_iab)[C + 1], bool need_mle,
+                                             bool need_reml, double s_m, double s_r, double& logl_m,
+                                             double& logl_r, PabOut<C>& pb_r) {
+    const int mine = (int)(threadIdx.x & 31) / GW;
+#pragma unroll 1
+    for (int h = 0; h < 32 / GW; ++h) {
+        const int src = h * GW;
+        const double sm = __shfl_sync(kFull, s_m, src), sr = __shfl_sync(kFull, s_r, src);
+        const bool dm = need_mle && sm >= kLogDirectLam;
+        const bool dr = need_reml && sr >= kLogDirectLam;
+        if (!dm && !dr) continue;
+        const int fh = __shfl_sync(kFull, f, src);
+        const long long jh = __shfl_sync(kFull, (long long)j, src);
+        double li[C + 1];
+#pragma unroll
+        for (int i = 0; i <= C; ++i) li[i] = __shfl_sync(kFull, log_iab[i], src);
+        const double* xh = p.G + jh * p.ldg;
+        const double* yh = p.Y + (int64_t)fh * p.ldy;
+        if (dm) {
+            PabOut<C> pb;
+            const double v = eval_logl<C, false>(p, xh, yh, sm, li, &pb);
+            if (mine == h) logl_m = v;
+        }
+        if (dr) {
+            PabOut<C> pb;
+            const double v = eval_logl<C, true>(p, xh, yh, sr, li, &pb);
+            if (mine == h) {
+                logl_r = v;
+                pb_r = pb;
+            }
+        }
+    }
+}
+
 // 4 warps per block; with one covariate at least 5 blocks per SM (<= 102 registers, 20
 // resident warps to hide FP64 and shuffle latency), fewer for wider covariate sets whose
 // per-warp state would otherwise spill.
@@ -916,6 +997,7 @@ __global__ void __launch_bounds__(kPairsThreads, GW == 16 ? PairsOccupancy<C>::k
                 if (p.out.se) p.out.se[o] = se;
             }
         }
+        if constexpr (INTERP) direct_score<C, GW>(p, j, f, valid_pair);
     }
     if (!need_reml && !need_mle) return;
 
@@ -941,10 +1023,10 @@ __global__ void __launch_bounds__(kPairsThreads, GW == 16 ? PairsOccupancy<C>::k
 
     // ---------------- phase 3: golden sections + statistics
     double lam_m = 0.0, logl_m = 0.0, lam_r = 0.0, logl_r = 0.0;
+    double s_m = 0.0, s_r = 0.0;  // mixed form: log-lambda of the optima
     PabOut<C> pb_r;
     if constexpr (INTERP && GW == 16) {
         BracketCoefV<C> bm, br;
-        double s_m = 0.0, s_r = 0.0;
         if (need_mle) s_m = golden_coop_v<C, false>(p, gcv, best_mle.idx, f, log_iab, bm);
         if (need_reml) s_r = golden_coop_v<C, true>(p, gcv, best_reml.idx, f, log_iab, br);
         lam_m = exp(s_m);
@@ -956,7 +1038,6 @@ __global__ void __launch_bounds__(kPairsThreads, GW == 16 ? PairsOccupancy<C>::k
         if (need_reml) logl_r = coop_eval_v<C, true>(p, gcv, br, s_r, log_iab, pb_r);
     } else if (INTERP) {
         BracketCoef<C> bm, br;
-        double s_m = 0.0, s_r = 0.0;
         if (need_mle) s_m = golden_coop<C, false>(p, gc, best_mle.idx, f, log_iab, bm);
         if (need_reml) s_r = golden_coop<C, true>(p, gc, best_reml.idx, f, log_iab, br);
         lam_m = exp(s_m);
@@ -973,6 +1054,8 @@ __global__ void __launch_bounds__(kPairsThreads, GW == 16 ? PairsOccupancy<C>::k
         }
         if (need_reml) golden<C, true>(p, x, y, best_reml.idx, log_iab, lam_r, logl_r, pb_r);
     }
+    if constexpr (INTERP)
+        direct_final<C, GW>(p, j, f, log_iab, need_mle, need_reml, s_m, s_r, logl_m, logl_r, pb_r);
     if (need_mle && lane == 0 && valid_pair) {
         if (p.out.lambda_mle) p.out.lambda_mle[o] = lam_m;
         if (p.out.logl_mle) p.out.logl_mle[o] = logl_m;

@@ -114,7 +114,33 @@ def job_device_bytes(n: int, phi: int, n_cvt: int, chunk: int, resident: bool,
     return int(b)
 
 
+def _retry_out_of_memory(fn, attempts: int = 3, pause_s: float = 0.5):
+    """Run ``fn``; when the caching allocator cannot place one of its large transient
+    buffers (the kinship operands, the eigensolver workspace), return the allocator's
+    unused cached blocks to the device and try again, after a pause in which other jobs'
+    chunks finish.  The budget accounting counts bytes in use, not how the allocator's
+    cache is cut up, so one large request can fail while the budget still has room."""
+    for attempt in range(attempts):
+        try:
+            return fn()
+        except torch.OutOfMemoryError:
+            if attempt == attempts - 1:
+                raise
+            torch.cuda.empty_cache()
+            time.sleep(pause_s * (attempt + 1))
+    raise AssertionError("unreachable")
+
+
 class GwasServer:
+    """Continuous-batching job server (see the module docstring).
+
+    A long-running server whose cohorts differ widely in size should run with PyTorch's
+    expandable allocator segments (``PYTORCH_CUDA_ALLOC_CONF=expandable_segments:True``,
+    set before CUDA is first used): the budget counts bytes in use, and with fixed
+    segments the freed multi-GB kinship and eigensolver buffers get cut up by smaller
+    allocations until a large request fails while much memory sits cached but unused.
+    """
+
     def __init__(self, hbm_budget_bytes: int, max_active: int = 4, chunk: int = 4096,
                  precision: str = "mixed", setup_workers: int = 2):
         require_cuda()
@@ -200,7 +226,7 @@ class GwasServer:
                 return self.cohorts[job.cohort_id]
         with self._lock:
             b = self._building[job.cohort_id]
-        try:  # new cohort: INT8 kinship + FP64 eigendecomposition on the device
+        def build_state():
             n = job.n_samples
             acc = _KinshipI8(n, int(poly.sum()))
             kidx = np.where(poly)[0]
@@ -210,10 +236,14 @@ class GwasServer:
                     bool(np.any(cc[:, 0] < n)), n_missing=int((n - cc[:, 0]).sum()))
             acc.add_sum_mu2(cc[:, 1] / np.maximum(cc[:, 0], 1))
             K = acc.finish()
+            del acc
             evals, U = eng.eigh_device(K)
             oz = eng.ozaki_split(U) if self.precision == "mixed" else None
             torch.cuda.current_stream().synchronize()  # resident state complete for other streams
-            res = _Resident(evals, U, oz)
+            return _Resident(evals, U, oz)
+
+        try:  # new cohort: INT8 kinship + FP64 eigendecomposition on the device
+            res = _retry_out_of_memory(build_state)
         except BaseException as e:
             with self._lock:
                 b.error = e

@@ -147,3 +147,56 @@ def test_all_snps_filtered_returns_no_results(tmp_path, precision):
     res = run_lmm_association_streaming(tmp_path / "none", y, kinship=K, lmm_mode=4,
                                         precision=precision, show_progress=False)
     assert res == []
+
+
+def test_mixed_form_at_the_upper_lambda_bound():
+    """Phenotypes whose variance is all genetic drive the null and alternative lambdas to
+    the upper bound 1e5, where the weighted sums the statistics use shrink by ~1/(lambda e)
+    and the series' fixed absolute error would dominate them; the mixed form evaluates
+    those optima with direct FP64 sums and must keep every p-value within 1e-6 of the
+    plain FP64 form (before, 3-5 % of such pairs were off by up to 2e-4)."""
+    from jamma_b200 import _native
+    from jamma_b200 import engine as eng
+    from jamma_b200.device import ptr, stream_handle
+
+    n, m = 3000, 512
+    g_k = synth.genotypes(n, 6000, 0.0, seed=21)
+    K = OK.centered_kinship(g_k)
+    w, U = np.linalg.eigh(K)
+    w = np.where(np.abs(w) < 1e-10, 0.0, w)
+    rng = np.random.default_rng(22)
+    genetic = U @ (np.sqrt(np.maximum(w, 0))[:, None] * rng.standard_normal((n, 2)))
+    mixed_h2 = genetic[:, :1] + 0.5 * rng.standard_normal((n, 1))
+    Y = np.column_stack([genetic, mixed_h2, rng.standard_normal(n)])
+    g = synth.genotypes(n, m, 0.01, seed=23)
+    packed = torch.from_numpy(OP.encode_genotypes(g)).cuda()
+    mu = torch.from_numpy(np.nan_to_num(np.nanmean(g, 0)).astype(np.float32).astype(np.float64)).cuda()
+    out = {}
+    for precision in ("fp64", "mixed"):
+        coh = eng.DeviceCohort(w, U, None, Y, lmm_mode=4, precision=precision)
+        codes, _ = eng.decode_packed(packed, n, None, n, ld=coh.code_ld)
+        if precision == "mixed":
+            assert coh.search == 1
+            X = coh.rotate_codes_i8(codes, mu, True)
+        else:
+            G = eng.empty((m, n))
+            _native.call("jb_impute_f64", ptr(codes), coh.code_ld, n, m, ptr(mu), ptr(G), n,
+                         stream_handle())
+            X = eng.rotate(coh.U, G)
+        out[precision] = ({k: v.cpu().numpy() for k, v in coh.associate_rotated(X).items()},
+                          coh.null_model()[0])
+    (a, lam0), (b, _) = out["mixed"], out["fp64"]
+    assert np.all(lam0[:2] > 1e4), f"the all-genetic phenotypes should reach the bound: {lam0}"
+    assert np.all(a["lambda_mle"][:2] > 1e4)
+    # score and LRT: the null lambda is the plain form's and the MLE optimum sits on the
+    # bound in both forms, so every pair must agree; Wald: the REML optimum is searched on
+    # the series, and a golden-section step decided differently (a near tie) moves a few
+    # p-values by ~1e-6, as between any two FP64 summation orders
+    for k, frac in (("p_wald", 0.99), ("p_lrt", 0.998), ("p_score", 0.998)):
+        for f in range(Y.shape[1]):
+            x, y = a[k][f], b[k][f]
+            rel = np.abs(x - y) / np.abs(y)
+            assert np.mean(rel <= 1e-6) >= frac, f"{k} phenotype {f}: worst {rel.max():.2e}"
+            assert np.max(np.abs(np.log10(x) - np.log10(y))) < 1e-4, (k, f)
+            for t in (0.05, 1e-3, 5e-8):
+                np.testing.assert_array_equal(x < t, y < t)
