@@ -765,11 +765,12 @@ def run_serving_only(args) -> None:
     """The serving configuration alone (``--serve-c4``): one JSON line with its latency
     percentiles, phase split and aggregate throughput.
 
-    Cohorts of 2 000 to 40 000 samples come and go, so the process runs PyTorch's caching
-    allocator with expandable segments: with fixed segments, the freed multi-GB kinship and
-    eigensolver buffers were cut up by later, smaller allocations until a 5 GB request
-    failed with 91 GB cached but unallocated."""
-    os.environ.setdefault("PYTORCH_CUDA_ALLOC_CONF", "expandable_segments:True")
+    Cohorts of 2 000 to 40 000 samples come and go, so the process keeps PyTorch's caching
+    allocator from splitting blocks above 256 MB: with splitting, the freed multi-GB
+    kinship and eigensolver buffers were cut up by later, smaller allocations until a 5 GB
+    request failed with 91 GB cached but unallocated.  (Expandable segments avoided that
+    but invalidated a concurrent chunk-graph capture.)"""
+    os.environ.setdefault("PYTORCH_CUDA_ALLOC_CONF", "max_split_size_mb:256")
     import torch
 
     from jamma_b200 import _build

@@ -840,69 +840,108 @@ __device__ __forceinline__ void beta_se(const PabOut<C>& pb, double px_yy, doubl
 constexpr double kDirectLam = 20.0;
 constexpr double kLogDirectLam = 2.995732273553991;  // log(kDirectLam)
 
-// Score statistic of the pairs whose null lambda is >= kDirectLam, from direct FP64 sums;
-// the whole warp evaluates each such pair of its 32 / GW groups in turn and the group's
-// lane 0 overwrites what the series evaluation wrote.
-template <int C, int GW>
-__device__ __forceinline__ void direct_score(const Params& p, int64_t j, int f, bool valid_pair) {
-#pragma unroll 1
-    for (int h = 0; h < 32 / GW; ++h) {
-        const int src = h * GW;
-        const int fh = __shfl_sync(kFull, f, src);
-        if (!(p.lam0[fh] >= kDirectLam)) continue;  // the same decision in every lane
-        const long long jh = __shfl_sync(kFull, (long long)j, src);
-        const bool vh = __shfl_sync(kFull, (int)valid_pair, src) != 0;
-        double row0[Lay<C>::NI], logdet;
-        eval_full<C>(p, p.G + jh * p.ldg, p.Y + (int64_t)fh * p.ldy, p.lam0[fh], row0, logdet);
-        const PabOut<C> pb = pab_reduce<C>(row0);
-        bool valid;
-        double beta, tau, se;
-        beta_se<C>(pb, clamp_pyy(pb.yy1), p.df, valid, beta, tau, se);
-        const double fstat = p.n_d * (pb.xy * pb.xy) / (pb.yy * (valid ? pb.xx : 1.0));
-        if ((int)(threadIdx.x & 31) == src && vh) {
-            const int64_t o = (int64_t)fh * p.m + jh;
-            if (p.out.p_score) p.out.p_score[o] = valid ? fstat : jnan();
-            if (p.mode == 3) {
-                if (p.out.beta) p.out.beta[o] = beta;
-                if (p.out.se) p.out.se[o] = se;
-            }
+// The x-dependent sums of one pair at up to three lambdas (the score's null lambda, the
+// MLE and REML optima; on[q] the same in every lane) in one warp-cooperative pass over the
+// rotated genotypes, each term formed as full_accumulate forms it.
+template <int C>
+__device__ __forceinline__ void direct_xsums3(const Params& p, const double* __restrict__ x,
+                                              const double* __restrict__ y,
+                                              const double (&lam)[3], const bool (&on)[3],
+                                              double (&xs)[3][Lay<C>::NX]) {
+    using L = Lay<C>;
+    double acc[3][L::NX];
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+#pragma unroll
+        for (int k = 0; k < L::NX; ++k) acc[q][k] = 0.0;
+    auto term = [&](double ev, double xv, double yv, const double (&w)[C > 0 ? C : 1]) {
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            if (!on[q]) continue;
+            const double hi = __drcp_rn(__dadd_rn(__dmul_rn(lam[q], ev), 1.0));
+#pragma unroll
+            for (int a = 0; a < C; ++a) acc[q][a] = fma(hi * w[a], xv, acc[q][a]);
+            const double t = hi * xv;
+            acc[q][C] = fma(t, xv, acc[q][C]);
+            acc[q][C + 1] = fma(t, yv, acc[q][C + 1]);
         }
+    };
+    // UNR consecutive strided samples' loads issued together (memory-level parallelism)
+    int64_t i = threadIdx.x & 31;
+    for (; i + 32 * (UNR - 1) < p.n; i += 32 * UNR) {
+        double ev[UNR], xv[UNR], yv[UNR], w[UNR][C > 0 ? C : 1];
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) {
+            ev[u] = __ldg(p.evals + i + 32 * u);
+            xv[u] = x[i + 32 * u];
+            yv[u] = __ldg(y + i + 32 * u);
+#pragma unroll
+            for (int a = 0; a < C; ++a) w[u][a] = __ldg(p.W + a * p.ldw + i + 32 * u);
+        }
+#pragma unroll
+        for (int u = 0; u < UNR; ++u) term(ev[u], xv[u], yv[u], w[u]);
     }
+    for (; i < p.n; i += 32) {
+        double w[C > 0 ? C : 1];
+#pragma unroll
+        for (int a = 0; a < C; ++a) w[a] = __ldg(p.W + a * p.ldw + i);
+        term(__ldg(p.evals + i), x[i], __ldg(y + i), w);
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+#pragma unroll
+        for (int k = 0; k < L::NX; ++k) xs[q][k] = on[q] ? warp_sum(acc[q][k]) : 0.0;
 }
 
-// Final MLE / REML evaluations of the pairs whose optimum is at lambda >= kDirectLam, from
-// direct FP64 sums; each group keeps its own pair's values.
+// Pairs with a final lambda >= kDirectLam: the whole warp takes each such pair of its
+// 32 / GW groups in turn and reduces its x-dependent sums directly.  The score statistic
+// is recomputed and rewritten here (the group's lane 0 overwrites the series value); the
+// MLE / REML sums replace xs_m / xs_r of the owning group, which then evaluates them with
+// its bracket-expanded x-free sums and log-determinant as before.
 template <int C, int GW>
-__device__ __forceinline__ void direct_final(const Params& p, int64_t j, int f,
-                                             const double (&log_iab)[C + 1], bool need_mle,
-                                             bool need_reml, double s_m, double s_r, double& logl_m,
-                                             double& logl_r, PabOut<C>& pb_r) {
+__device__ __forceinline__ void direct_fix(const Params& p, int64_t j, int f, bool valid_pair,
+                                           bool need_score, bool need_mle, bool need_reml,
+                                           double s_m, double s_r, double (&xs_m)[Lay<C>::NX],
+                                           double (&xs_r)[Lay<C>::NX]) {
+    using L = Lay<C>;
     const int mine = (int)(threadIdx.x & 31) / GW;
 #pragma unroll 1
     for (int h = 0; h < 32 / GW; ++h) {
         const int src = h * GW;
-        const double sm = __shfl_sync(kFull, s_m, src), sr = __shfl_sync(kFull, s_r, src);
-        const bool dm = need_mle && sm >= kLogDirectLam;
-        const bool dr = need_reml && sr >= kLogDirectLam;
-        if (!dm && !dr) continue;
         const int fh = __shfl_sync(kFull, f, src);
+        const double sm = __shfl_sync(kFull, s_m, src), sr = __shfl_sync(kFull, s_r, src);
+        const double lam0 = need_score ? p.lam0[fh] : 0.0;
+        const bool on[3] = {need_score && lam0 >= kDirectLam, need_mle && sm >= kLogDirectLam,
+                            need_reml && sr >= kLogDirectLam};
+        if (!on[0] && !on[1] && !on[2]) continue;  // the same decision in every lane
         const long long jh = __shfl_sync(kFull, (long long)j, src);
-        double li[C + 1];
-#pragma unroll
-        for (int i = 0; i <= C; ++i) li[i] = __shfl_sync(kFull, log_iab[i], src);
-        const double* xh = p.G + jh * p.ldg;
-        const double* yh = p.Y + (int64_t)fh * p.ldy;
-        if (dm) {
-            PabOut<C> pb;
-            const double v = eval_logl<C, false>(p, xh, yh, sm, li, &pb);
-            if (mine == h) logl_m = v;
+        const bool vh = __shfl_sync(kFull, (int)valid_pair, src) != 0;
+        const double lam[3] = {lam0, exp(sm), exp(sr)};
+        double xs[3][L::NX];
+        direct_xsums3<C>(p, p.G + jh * p.ldg, p.Y + (int64_t)fh * p.ldy, lam, on, xs);
+        if (on[0]) {
+            double row0[L::NI];
+            assemble<C>(row0, p.S + (int64_t)(p.n_grid + 1 + fh) * p.phi * L::NS + (int64_t)fh * L::NS,
+                        xs[0]);
+            const PabOut<C> pb = pab_reduce<C>(row0);
+            bool valid;
+            double beta, tau, se;
+            beta_se<C>(pb, clamp_pyy(pb.yy1), p.df, valid, beta, tau, se);
+            const double fstat = p.n_d * (pb.xy * pb.xy) / (pb.yy * (valid ? pb.xx : 1.0));
+            if ((int)(threadIdx.x & 31) == src && vh) {
+                const int64_t o = (int64_t)fh * p.m + jh;
+                if (p.out.p_score) p.out.p_score[o] = valid ? fstat : jnan();
+                if (p.mode == 3) {
+                    if (p.out.beta) p.out.beta[o] = beta;
+                    if (p.out.se) p.out.se[o] = se;
+                }
+            }
         }
-        if (dr) {
-            PabOut<C> pb;
-            const double v = eval_logl<C, true>(p, xh, yh, sr, li, &pb);
-            if (mine == h) {
-                logl_r = v;
-                pb_r = pb;
+        if (mine == h) {
+#pragma unroll
+            for (int k = 0; k < L::NX; ++k) {
+                if (on[1]) xs_m[k] = xs[1][k];
+                if (on[2]) xs_r[k] = xs[2][k];
             }
         }
     }
@@ -997,9 +1036,14 @@ __global__ void __launch_bounds__(kPairsThreads, GW == 16 ? PairsOccupancy<C>::k
                 if (p.out.se) p.out.se[o] = se;
             }
         }
-        if constexpr (INTERP) direct_score<C, GW>(p, j, f, valid_pair);
     }
-    if (!need_reml && !need_mle) return;
+    if (!need_reml && !need_mle) {
+        if constexpr (INTERP) {  // score only: the large-lambda rewrite happens here
+            double xs_m[L::NX], xs_r[L::NX];
+            direct_fix<C, GW>(p, j, f, valid_pair, need_score, false, false, 0.0, 0.0, xs_m, xs_r);
+        }
+        return;
+    }
 
     // ---------------- phase 2: shared lambda grid
     ArgMax best_reml, best_mle;
@@ -1025,28 +1069,50 @@ __global__ void __launch_bounds__(kPairsThreads, GW == 16 ? PairsOccupancy<C>::k
     double lam_m = 0.0, logl_m = 0.0, lam_r = 0.0, logl_r = 0.0;
     double s_m = 0.0, s_r = 0.0;  // mixed form: log-lambda of the optima
     PabOut<C> pb_r;
-    if constexpr (INTERP && GW == 16) {
-        BracketCoefV<C> bm, br;
-        if (need_mle) s_m = golden_coop_v<C, false>(p, gcv, best_mle.idx, f, log_iab, bm);
-        if (need_reml) s_r = golden_coop_v<C, true>(p, gcv, best_reml.idx, f, log_iab, br);
+    if constexpr (INTERP) {
+        // final evaluations at the optima: x-dependent sums from the series (or, at large
+        // lambda, directly), x-free sums and log|H^-1| from the bracket's expansions
+        double xs_m[L::NX], xs_r[L::NX], sh_m[L::NS], sh_r[L::NS], ld_m = 0.0, ld_r = 0.0;
+        if constexpr (GW == 16) {
+            BracketCoefV<C> bm, br;
+            if (need_mle) s_m = golden_coop_v<C, false>(p, gcv, best_mle.idx, f, log_iab, bm);
+            if (need_reml) s_r = golden_coop_v<C, true>(p, gcv, best_reml.idx, f, log_iab, br);
+            if (need_mle) {
+                coop_xsums_v<C>(p, gcv, s_m, xs_m);
+                coop_shared_v<C>(bm, s_m, ld_m, sh_m);
+            }
+            if (need_reml) {
+                coop_xsums_v<C>(p, gcv, s_r, xs_r);
+                coop_shared_v<C>(br, s_r, ld_r, sh_r);
+            }
+        } else {
+            BracketCoef<C> bm, br;
+            if (need_mle) s_m = golden_coop<C, false>(p, gc, best_mle.idx, f, log_iab, bm);
+            if (need_reml) s_r = golden_coop<C, true>(p, gc, best_reml.idx, f, log_iab, br);
+            if (need_mle) {
+                coop_xsums<C>(p, gc, s_m, xs_m);
+                coop_shared<C>(bm, s_m, ld_m, sh_m);
+            }
+            if (need_reml) {
+                coop_xsums<C>(p, gc, s_r, xs_r);
+                coop_shared<C>(br, s_r, ld_r, sh_r);
+            }
+        }
         lam_m = exp(s_m);
         lam_r = exp(s_r);
+        direct_fix<C, GW>(p, j, f, valid_pair, need_score, need_mle, need_reml, s_m, s_r, xs_m,
+                          xs_r);
+        double row0[L::NI];
         if (need_mle) {
-            PabOut<C> pb;
-            logl_m = coop_eval_v<C, false>(p, gcv, bm, s_m, log_iab, pb);
+            assemble<C>(row0, sh_m, xs_m);
+            const PabOut<C> pb = pab_reduce<C>(row0);
+            logl_m = mle_logl<C>(pb, ld_m, p);
         }
-        if (need_reml) logl_r = coop_eval_v<C, true>(p, gcv, br, s_r, log_iab, pb_r);
-    } else if (INTERP) {
-        BracketCoef<C> bm, br;
-        if (need_mle) s_m = golden_coop<C, false>(p, gc, best_mle.idx, f, log_iab, bm);
-        if (need_reml) s_r = golden_coop<C, true>(p, gc, best_reml.idx, f, log_iab, br);
-        lam_m = exp(s_m);
-        lam_r = exp(s_r);
-        if (need_mle) {
-            PabOut<C> pb;
-            logl_m = coop_eval<C, false>(p, gc, bm, s_m, log_iab, pb);
+        if (need_reml) {
+            assemble<C>(row0, sh_r, xs_r);
+            pb_r = pab_reduce<C>(row0);
+            logl_r = reml_logl<C>(pb_r, log_iab, ld_r, p);
         }
-        if (need_reml) logl_r = coop_eval<C, true>(p, gc, br, s_r, log_iab, pb_r);
     } else {
         if (need_mle) {
             PabOut<C> pb;
@@ -1054,8 +1120,6 @@ __global__ void __launch_bounds__(kPairsThreads, GW == 16 ? PairsOccupancy<C>::k
         }
         if (need_reml) golden<C, true>(p, x, y, best_reml.idx, log_iab, lam_r, logl_r, pb_r);
     }
-    if constexpr (INTERP)
-        direct_final<C, GW>(p, j, f, log_iab, need_mle, need_reml, s_m, s_r, logl_m, logl_r, pb_r);
     if (need_mle && lane == 0 && valid_pair) {
         if (p.out.lambda_mle) p.out.lambda_mle[o] = lam_m;
         if (p.out.logl_mle) p.out.logl_mle[o] = logl_m;
@@ -1777,10 +1841,14 @@ int32_t launch_sq_sums(const double* AT, int64_t rows, const double* X, int64_t 
 template <int C>
 int32_t launch_pairs(const Params& p, cudaStream_t st) {
     const int64_t pairs = p.m * p.phi;
-    if (p.cheb && C == 1)  // two pairs per warp (bit-identical to one per warp)
-        lmm_pairs_kernel<C, true, (C == 1 ? 16 : 32)>
-            <<<(unsigned)ceil_div(pairs * 16, kPairsThreads), kPairsThreads, 0, st>>>(p);
-    else if (p.cheb)
+    if constexpr (C == 1) {
+        if (p.cheb)  // two pairs per warp (bit-identical to one per warp)
+            lmm_pairs_kernel<C, true, 16>
+                <<<(unsigned)ceil_div(pairs * 16, kPairsThreads), kPairsThreads, 0, st>>>(p);
+        else
+            lmm_pairs_kernel<C, false, 32>
+                <<<(unsigned)ceil_div(pairs * 32, kPairsThreads), kPairsThreads, 0, st>>>(p);
+    } else if (p.cheb)
         lmm_pairs_kernel<C, true, 32><<<(unsigned)ceil_div(pairs * 32, kPairsThreads), kPairsThreads, 0, st>>>(p);
     else
         lmm_pairs_kernel<C, false, 32><<<(unsigned)ceil_div(pairs * 32, kPairsThreads), kPairsThreads, 0, st>>>(p);

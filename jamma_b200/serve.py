@@ -114,6 +114,16 @@ def job_device_bytes(n: int, phi: int, n_cvt: int, chunk: int, resident: bool,
     return int(b)
 
 
+def _device_room(need: int) -> bool:
+    """True when the device has ``need`` bytes free, after returning the caching
+    allocator's unused blocks if it does not at first."""
+    free, _ = torch.cuda.mem_get_info()
+    if free >= need:
+        return True
+    torch.cuda.empty_cache()
+    return torch.cuda.mem_get_info()[0] >= need
+
+
 def _retry_out_of_memory(fn, attempts: int = 3, pause_s: float = 0.5):
     """Run ``fn``; when the caching allocator cannot place one of its large transient
     buffers (the kinship operands, the eigensolver workspace), return the allocator's
@@ -134,11 +144,13 @@ def _retry_out_of_memory(fn, attempts: int = 3, pause_s: float = 0.5):
 class GwasServer:
     """Continuous-batching job server (see the module docstring).
 
-    A long-running server whose cohorts differ widely in size should run with PyTorch's
-    expandable allocator segments (``PYTORCH_CUDA_ALLOC_CONF=expandable_segments:True``,
-    set before CUDA is first used): the budget counts bytes in use, and with fixed
-    segments the freed multi-GB kinship and eigensolver buffers get cut up by smaller
-    allocations until a large request fails while much memory sits cached but unused.
+    A long-running server whose cohorts differ widely in size should keep PyTorch's caching
+    allocator from splitting large blocks (``PYTORCH_CUDA_ALLOC_CONF=max_split_size_mb:256``,
+    set before CUDA is first used): the budget counts bytes in use, and with splitting the
+    freed multi-GB kinship and eigensolver buffers get cut up by smaller allocations until
+    a large request fails while much memory sits cached but unused.  Admission of a job
+    that builds a cohort also checks the device's free memory, returning the allocator's
+    unused cached blocks first if needed.
     """
 
     def __init__(self, hbm_budget_bytes: int, max_active: int = 4, chunk: int = 4096,
@@ -189,6 +201,10 @@ class GwasServer:
                 if self.used + self._resident_bytes() + need > self.budget:
                     if not self.active and not self.preparing:
                         raise MemoryError(f"job {job.job_id} needs {need} bytes, over the HBM budget")
+                    return
+                # a cohort build also needs the device to have that much free in fact: the
+                # caching allocator may hold more than the bytes in use
+                if not known and (self.active or self.preparing) and not _device_room(need):
                     return
                 self.queue.popleft()
                 # reserve the cohort now so that eviction cannot take it before set-up

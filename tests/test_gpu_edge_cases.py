@@ -149,7 +149,8 @@ def test_all_snps_filtered_returns_no_results(tmp_path, precision):
     assert res == []
 
 
-def test_mixed_form_at_the_upper_lambda_bound():
+@pytest.mark.parametrize("mode", [4, 3])
+def test_mixed_form_at_the_upper_lambda_bound(mode):
     """Phenotypes whose variance is all genetic drive the null and alternative lambdas to
     the upper bound 1e5, where the weighted sums the statistics use shrink by ~1/(lambda e)
     and the series' fixed absolute error would dominate them; the mixed form evaluates
@@ -173,7 +174,7 @@ def test_mixed_form_at_the_upper_lambda_bound():
     mu = torch.from_numpy(np.nan_to_num(np.nanmean(g, 0)).astype(np.float32).astype(np.float64)).cuda()
     out = {}
     for precision in ("fp64", "mixed"):
-        coh = eng.DeviceCohort(w, U, None, Y, lmm_mode=4, precision=precision)
+        coh = eng.DeviceCohort(w, U, None, Y, lmm_mode=mode, precision=precision)
         codes, _ = eng.decode_packed(packed, n, None, n, ld=coh.code_ld)
         if precision == "mixed":
             assert coh.search == 1
@@ -187,12 +188,15 @@ def test_mixed_form_at_the_upper_lambda_bound():
                           coh.null_model()[0])
     (a, lam0), (b, _) = out["mixed"], out["fp64"]
     assert np.all(lam0[:2] > 1e4), f"the all-genetic phenotypes should reach the bound: {lam0}"
-    assert np.all(a["lambda_mle"][:2] > 1e4)
+    if mode == 4:
+        assert np.all(a["lambda_mle"][:2] > 1e4)
     # score and LRT: the null lambda is the plain form's and the MLE optimum sits on the
     # bound in both forms, so every pair must agree; Wald: the REML optimum is searched on
     # the series, and a golden-section step decided differently (a near tie) moves a few
     # p-values by ~1e-6, as between any two FP64 summation orders
-    for k, frac in (("p_wald", 0.99), ("p_lrt", 0.998), ("p_score", 0.998)):
+    checks = (("p_wald", 0.99), ("p_lrt", 0.998), ("p_score", 0.998)) if mode == 4 else \
+        (("p_score", 0.998),)
+    for k, frac in checks:
         for f in range(Y.shape[1]):
             x, y = a[k][f], b[k][f]
             rel = np.abs(x - y) / np.abs(y)
