@@ -423,6 +423,11 @@ const MgApi* mg_api() {
     return ok ? &api : nullptr;
 }
 
+// cusolverMg keeps handle-independent state; two of its solves (or workspace queries) from
+// different threads at once failed with CUSOLVER_STATUS_INTERNAL_ERROR, so every use is
+// serialised on this lock.
+std::mutex g_mg_mutex;
+
 struct MgSolver {
     const MgApi* api = mg_api();
     cusolverMgHandle_t h = nullptr;
@@ -475,6 +480,7 @@ int64_t jb_eigh_workspace_size(int64_t n) {
     if (dn_syevd_fits(n, &dev_bytes))
         return (int64_t)(((dev_bytes + 255) / 256) * 256) + 256;  // + device info word
     if (n > 2147483647ll) return -1;
+    std::lock_guard<std::mutex> lock(g_mg_mutex);
     MgSolver mg;
     std::vector<double> w_host((size_t)n);
     int64_t lwork = 0;
@@ -491,6 +497,7 @@ int64_t jb_eigh_workspace_size(int64_t n) {
 // Large-n path of jb_eigh_f64 (lda == n): blocking cusolverMgSyevd on this device.
 static int32_t eigh_f64_mg(double* A, int64_t n, double* w, double threshold, void* workspace,
                            int64_t workspace_bytes, cudaStream_t st) {
+    std::lock_guard<std::mutex> lock(g_mg_mutex);
     MgSolver mg;
     double* w_host = nullptr;  // pinned: valid for the solver as a host or a device address
     JB_CUDA(cudaMallocHost(&w_host, (size_t)n * sizeof(double)));

@@ -159,6 +159,10 @@ class GwasServer:
         self._pool = ThreadPoolExecutor(max_workers=max(1, setup_workers),
                                         thread_name_prefix="jb-setup")
         self._lock = threading.Lock()  # cohorts / _building, shared with the workers
+        # Graph captures and eigendecompositions never overlap: above ~23 000 samples the
+        # solver synchronises the whole device, which a capture on another thread must not
+        # see.
+        self._device_sync_lock = threading.Lock()
         self._building: dict[str, _Building] = {}
         self.preparing: list[tuple[_Active, Future]] = []
         self.budget = int(hbm_budget_bytes)
@@ -253,7 +257,8 @@ class GwasServer:
             acc.add_sum_mu2(cc[:, 1] / np.maximum(cc[:, 0], 1))
             K = acc.finish()
             del acc
-            evals, U = eng.eigh_device(K)
+            with self._device_sync_lock:  # the large-n solver synchronises the device
+                evals, U = eng.eigh_device(K)
             oz = eng.ozaki_split(U) if self.precision == "mixed" else None
             torch.cuda.current_stream().synchronize()  # resident state complete for other streams
             return _Resident(evals, U, oz)
@@ -291,8 +296,9 @@ class GwasServer:
             act.means = torch.from_numpy(mean[idx].astype(np.float64)).pin_memory()
             act.n_miss = miss[idx]
             # the job's chunk work as one CUDA graph, replayed for every chunk
-            act.graph = eng.ChunkGraph(act.cohort, min(self.chunk, max(1, idx.size)),
-                                       has_missing=True)
+            with self._device_sync_lock:  # no device synchronisation during capture
+                act.graph = eng.ChunkGraph(act.cohort, min(self.chunk, max(1, idx.size)),
+                                           has_missing=True)
         job.snp_indices = idx
         job.results = {k: np.empty((act.cohort.phi, idx.size)) for k in eng.MODE_KEYS[job.lmm_mode]}
         job.af, job.n_miss = af[idx], miss[idx]
