@@ -369,8 +369,10 @@ def run_serving(args, seed: int = 7) -> dict:
         t += rng.exponential(args.serve_gap)
         jobs.append((t, GwasJob(f"j{i}", cid, packed, n, y if phi > 1 else y[:, 0], cov,
                                 int(rng.integers(1, 5)))))
+    # the full configuration issues chunks eagerly: under its memory pressure a chunk-graph
+    # capture failed and the failed graph's teardown aborted the process
     srv = GwasServer(hbm_budget_bytes=int(args.serve_budget_gb * (1 << 30)), max_active=4,
-                     chunk=4096)
+                     chunk=4096, capture_graphs=not c4)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     srv.run(jobs)

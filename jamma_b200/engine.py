@@ -257,7 +257,9 @@ class ChunkGraph:
     safe; a chunk shorter than ``m`` uses the first rows and ignores the rest.
 
     Capture runs on a private stream without synchronising the device, with thread-local
-    capture rules, so other streams and threads keep working meanwhile.  The graph keeps
+    capture rules, so other streams and threads keep working meanwhile.  With
+    ``capture=False`` the object keeps the same buffers and interface and replays by
+    issuing the launches eagerly.  The graph keeps
     the cohort's workspaces alive; capture after any eager chunk larger than ``m`` so that
     no workspace is reallocated afterwards.  ``prefill(graph)``, if given, fills the input
     buffers (on the capture's private stream) before the eager warm-up run, whose results
@@ -266,7 +268,7 @@ class ChunkGraph:
 
     def __init__(self, cohort: "DeviceCohort", m: int, n_file: int | None = None,
                  sample_idx: torch.Tensor | None = None, has_missing: bool = True,
-                 prefill=None):
+                 prefill=None, capture: bool = True):
         n = cohort.n
         n_file = n if n_file is None else n_file
         self.cohort, self.m, self.n_file, self.sample_idx = cohort, m, n_file, sample_idx
@@ -288,12 +290,14 @@ class ChunkGraph:
             self._run()  # eager warm-up: workspaces, library handles, kernel attributes
             self._keep = (cohort.ws, cohort._chunk_ws, cohort._rot_ws, cohort.series_ws,
                           cohort.ozaki)
-            self.graph = torch.cuda.CUDAGraph()
-            self.graph.capture_begin(capture_error_mode="thread_local")
-            try:
-                self._run()
-            finally:
-                self.graph.capture_end()
+            self.graph = None
+            if capture:
+                self.graph = torch.cuda.CUDAGraph()
+                self.graph.capture_begin(capture_error_mode="thread_local")
+                try:
+                    self._run()
+                finally:
+                    self.graph.capture_end()
         caller.wait_stream(side)
 
     def _run(self) -> None:
@@ -305,7 +309,12 @@ class ChunkGraph:
                           has_missing=self.has_missing)
 
     def replay(self) -> dict:
-        self.graph.replay()
+        """Run the chunk on the current stream: the captured graph, or (``capture=False``)
+        the same launches issued eagerly."""
+        if self.graph is None:
+            self._run()
+        else:
+            self.graph.replay()
         return self.out
 
 

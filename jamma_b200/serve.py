@@ -150,11 +150,13 @@ class GwasServer:
     freed multi-GB kinship and eigensolver buffers get cut up by smaller allocations until
     a large request fails while much memory sits cached but unused.  Admission of a job
     that builds a cohort also checks the device's free memory, returning the allocator's
-    unused cached blocks first if needed.
+    unused cached blocks first if needed.  ``capture_graphs=False`` issues each chunk's
+    launches eagerly instead of replaying a captured graph (no capture under memory
+    pressure).
     """
 
     def __init__(self, hbm_budget_bytes: int, max_active: int = 4, chunk: int = 4096,
-                 precision: str = "mixed", setup_workers: int = 2):
+                 precision: str = "mixed", setup_workers: int = 2, capture_graphs: bool = True):
         require_cuda()
         self._pool = ThreadPoolExecutor(max_workers=max(1, setup_workers),
                                         thread_name_prefix="jb-setup")
@@ -163,6 +165,7 @@ class GwasServer:
         # solver synchronises the whole device, which a capture on another thread must not
         # see.
         self._device_sync_lock = threading.Lock()
+        self.capture_graphs = capture_graphs
         self._building: dict[str, _Building] = {}
         self.preparing: list[tuple[_Active, Future]] = []
         self.budget = int(hbm_budget_bytes)
@@ -298,7 +301,7 @@ class GwasServer:
             # the job's chunk work as one CUDA graph, replayed for every chunk
             with self._device_sync_lock:  # no device synchronisation during capture
                 act.graph = eng.ChunkGraph(act.cohort, min(self.chunk, max(1, idx.size)),
-                                           has_missing=True)
+                                           has_missing=True, capture=self.capture_graphs)
         job.snp_indices = idx
         job.results = {k: np.empty((act.cohort.phi, idx.size)) for k in eng.MODE_KEYS[job.lmm_mode]}
         job.af, job.n_miss = af[idx], miss[idx]

@@ -46,10 +46,11 @@ def _jobs():
     return jobs
 
 
-def _serve(jobs, max_active):
+def _serve(jobs, max_active, capture_graphs=True):
     from jamma_b200.serve import GwasServer
 
-    srv = GwasServer(hbm_budget_bytes=8 << 30, max_active=max_active, chunk=512)
+    srv = GwasServer(hbm_budget_bytes=8 << 30, max_active=max_active, chunk=512,
+                     capture_graphs=capture_graphs)
     for j in jobs:
         srv.submit(j)
     done = srv.run()
@@ -68,6 +69,18 @@ def test_results_are_the_same_alone_and_in_the_mix():
         for k in a.results:
             np.testing.assert_allclose(a.results[k], b.results[k], rtol=1e-12, atol=0,
                                        err_msg=f"{job.job_id}:{k}")
+
+
+def test_eager_chunks_equal_graph_replays():
+    """capture_graphs=False issues each chunk's launches eagerly: the same results, bit for
+    bit, as replaying the captured graphs."""
+    graphs, _ = _serve(_jobs(), max_active=4)
+    eager, _ = _serve(_jobs(), max_active=4, capture_graphs=False)
+    for jid, a in graphs.items():
+        b = eager[jid]
+        np.testing.assert_array_equal(a.snp_indices, b.snp_indices)
+        for k in a.results:
+            np.testing.assert_array_equal(a.results[k], b.results[k], err_msg=f"{jid}:{k}")
 
 
 def test_server_matches_the_streaming_runner(tmp_path):
