@@ -35,7 +35,11 @@ BF16_PEAK_FALLBACK = 1590.0
 # (dram__bytes_read.sum + dram__bytes_write.sum) for the configuration in the key:
 # (n, SNPs per launch, missing calls present, rotation kernel variant, tile schedule).
 # Any other configuration reports traffic null rather than a stale figure.
-ROT_DRAM_BYTES = {(20000, 8192, True, 0, (9, 16)): 30.40e9}
+ROT_DRAM_BYTES = {(20000, 8192, True, 0, (9, 16)): 30.39e9,
+                  (20000, 8192, True, 0, (5, 32)): 36.25e9,
+                  (20000, 8192, True, 0, (17, 8)): 25.26e9,
+                  (20000, 8192, True, 0, (3, 64)): 56.31e9,
+                  (20000, 8192, True, 0, (36, 4)): 32.89e9}
 
 
 def _peaks() -> dict:
