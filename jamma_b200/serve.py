@@ -114,17 +114,29 @@ def job_device_bytes(n: int, phi: int, n_cvt: int, chunk: int, resident: bool,
     return int(b)
 
 
-def _device_room(need: int) -> bool:
+def _release_cached(sync_lock: threading.Lock) -> bool:
+    """Return the caching allocator's unused blocks to the device, unless a graph capture
+    or an eigendecomposition holds ``sync_lock`` (freeing device memory synchronises the
+    device, which neither may see, and would stall the caller behind a long solve).
+    Returns whether it released."""
+    if not sync_lock.acquire(blocking=False):
+        return False
+    try:
+        torch.cuda.empty_cache()
+    finally:
+        sync_lock.release()
+    return True
+
+
+def _device_room(need: int, sync_lock: threading.Lock) -> bool:
     """True when the device has ``need`` bytes free, after returning the caching
-    allocator's unused blocks if it does not at first."""
-    free, _ = torch.cuda.mem_get_info()
-    if free >= need:
+    allocator's unused blocks if it does not at first (when that is possible now)."""
+    if torch.cuda.mem_get_info()[0] >= need:
         return True
-    torch.cuda.empty_cache()
-    return torch.cuda.mem_get_info()[0] >= need
+    return _release_cached(sync_lock) and torch.cuda.mem_get_info()[0] >= need
 
 
-def _retry_out_of_memory(fn, attempts: int = 3, pause_s: float = 0.5):
+def _retry_out_of_memory(fn, sync_lock: threading.Lock, attempts: int = 3, pause_s: float = 0.5):
     """Run ``fn``; when the caching allocator cannot place one of its large transient
     buffers (the kinship operands, the eigensolver workspace), return the allocator's
     unused cached blocks to the device and try again, after a pause in which other jobs'
@@ -136,8 +148,8 @@ def _retry_out_of_memory(fn, attempts: int = 3, pause_s: float = 0.5):
         except torch.OutOfMemoryError:
             if attempt == attempts - 1:
                 raise
-            torch.cuda.empty_cache()
             time.sleep(pause_s * (attempt + 1))
+            _release_cached(sync_lock)
     raise AssertionError("unreachable")
 
 
@@ -211,7 +223,8 @@ class GwasServer:
                     return
                 # a cohort build also needs the device to have that much free in fact: the
                 # caching allocator may hold more than the bytes in use
-                if not known and (self.active or self.preparing) and not _device_room(need):
+                if not known and (self.active or self.preparing) and \
+                        not _device_room(need, self._device_sync_lock):
                     return
                 self.queue.popleft()
                 # reserve the cohort now so that eviction cannot take it before set-up
@@ -267,7 +280,7 @@ class GwasServer:
             return _Resident(evals, U, oz)
 
         try:  # new cohort: INT8 kinship + FP64 eigendecomposition on the device
-            res = _retry_out_of_memory(build_state)
+            res = _retry_out_of_memory(build_state, self._device_sync_lock)
         except BaseException as e:
             with self._lock:
                 b.error = e
