@@ -226,7 +226,10 @@ int32_t jb_kinship_loco_f64(const double* S_full, const double* S_chr, int64_t n
  * holds the eigenvectors as columns and w the eigenvalues in ascending order, with
  * |w| < threshold set to 0.  Replaces np.linalg.eigh + thresholding
  * (src/jamma/lmm/eigen.py:94,118).  workspace: jb_eigh_workspace_size bytes.
- * Synchronises the stream (cuSOLVER reports convergence on the host).
+ * Synchronises the stream (cuSOLVER reports convergence on the host).  Above the
+ * single-GPU solver's size limit (n ~ 23 000) it runs cusolverMgSyevd on a one-device
+ * grid, which synchronises the whole device; those calls (and their workspace queries)
+ * are serialised process-wide, since two at once failed inside the library.
  */
 int64_t jb_eigh_workspace_size(int64_t n);
 int32_t jb_eigh_f64(double* A, int64_t n, int64_t lda, double* w, double threshold,
