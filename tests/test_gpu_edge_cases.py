@@ -149,13 +149,14 @@ def test_all_snps_filtered_returns_no_results(tmp_path, precision):
     assert res == []
 
 
-@pytest.mark.parametrize("mode", [4, 3])
-def test_mixed_form_at_the_upper_lambda_bound(mode):
+@pytest.mark.parametrize("mode,n_cov", [(4, 1), (3, 1), (4, 2)])
+def test_mixed_form_at_the_upper_lambda_bound(mode, n_cov):
     """Phenotypes whose variance is all genetic drive the null and alternative lambdas to
     the upper bound 1e5, where the weighted sums the statistics use shrink by ~1/(lambda e)
     and the series' fixed absolute error would dominate them; the mixed form evaluates
     those optima with direct FP64 sums and must keep every p-value within 1e-6 of the
-    plain FP64 form (before, 3-5 % of such pairs were off by up to 2e-4)."""
+    plain FP64 form (before, 3-5 % of such pairs were off by up to 2e-4).  With a second
+    covariate column the mixed form runs one pair per warp instead of two."""
     from jamma_b200 import _native
     from jamma_b200 import engine as eng
     from jamma_b200.device import ptr, stream_handle
@@ -169,12 +170,13 @@ def test_mixed_form_at_the_upper_lambda_bound(mode):
     genetic = U @ (np.sqrt(np.maximum(w, 0))[:, None] * rng.standard_normal((n, 2)))
     mixed_h2 = genetic[:, :1] + 0.5 * rng.standard_normal((n, 1))
     Y = np.column_stack([genetic, mixed_h2, rng.standard_normal(n)])
+    W = None if n_cov == 1 else np.column_stack([np.ones(n), rng.standard_normal(n)])
     g = synth.genotypes(n, m, 0.01, seed=23)
     packed = torch.from_numpy(OP.encode_genotypes(g)).cuda()
     mu = torch.from_numpy(np.nan_to_num(np.nanmean(g, 0)).astype(np.float32).astype(np.float64)).cuda()
     out = {}
     for precision in ("fp64", "mixed"):
-        coh = eng.DeviceCohort(w, U, None, Y, lmm_mode=mode, precision=precision)
+        coh = eng.DeviceCohort(w, U, W, Y, lmm_mode=mode, precision=precision)
         codes, _ = eng.decode_packed(packed, n, None, n, ld=coh.code_ld)
         if precision == "mixed":
             assert coh.search == 1
