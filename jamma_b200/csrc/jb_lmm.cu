@@ -515,8 +515,9 @@ __device__ __forceinline__ void coop_shared(const BracketCoef<C>& b, double s, d
 
 // Mixed-form log-likelihood at log-lambda s with no length-n pass: the x-dependent sums
 // from the SNP's global series, log|H^-1| and the x-free sums from the bracket's expansions
-// (exact FP64 node values).  The golden-section probes and the final evaluation at the
-// optimum both use it; pb receives the Pab rows for the statistics.
+// (exact FP64 node values).  The golden-section probes use it; the final evaluation at
+// the optimum takes the same steps in lmm_pairs_kernel, where direct_fix may replace the
+// x-dependent sums by direct ones at large lambda.  pb receives the Pab rows.
 template <int C, bool REML>
 __device__ __forceinline__ double coop_eval(const Params& p, const GlobalCoef<C>& g,
                                             const BracketCoef<C>& b, double s,
