@@ -32,11 +32,9 @@ from jamma_b200.lmm import run_lmm_association_jax, run_lmm_association_streamin
 
 __version__ = "0.1.0"
 
-
-def gwas(*args, **kwargs):
-    from jamma_b200.gwas import gwas as _gwas
-
-    return _gwas(*args, **kwargs)
+# Imported eagerly: importing the submodule later would rebind the package attribute
+# ``gwas`` to the module and break a second call of the function.
+from jamma_b200.gwas import gwas  # noqa: E402
 
 
 __all__ = [

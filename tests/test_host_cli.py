@@ -39,3 +39,29 @@ def test_unknown_precision_is_an_argument_error(capsys, tmp_path):
     with pytest.raises(SystemExit) as e:
         cli.main(["gk", "-bfile", str(tmp_path / "x"), "-precision", "fp16"])
     assert e.value.code == 2
+
+
+@pytest.mark.parametrize("kwargs,msg", [
+    ({"precision": "fp16"}, "precision must be"),
+    ({"lmm_mode": 5}, "lmm_mode must be 1, 2, 3 or 4"),
+    ({"loco": True, "kinship_file": "k.cXX.txt"}, "mutually exclusive"),
+    ({"eigenvalue_file": "d.txt"}, "provided together"),
+])
+def test_gwas_argument_errors(kwargs, msg, tmp_path):
+    """gwas() rejects inconsistent arguments with ValueError before reading any file
+    (src/jamma/gwas.py:40-167)."""
+    from jamma_b200.gwas import gwas
+
+    with pytest.raises(ValueError, match=msg):
+        gwas(tmp_path / "x", **kwargs)
+
+
+def test_package_gwas_can_be_called_repeatedly(tmp_path):
+    """``jamma_b200.gwas`` stays the function after the submodule has been imported (a
+    lazily imported submodule would rebind the package attribute to itself)."""
+    import jamma_b200
+    import jamma_b200.gwas  # noqa: F401
+
+    for _ in range(2):
+        with pytest.raises(ValueError, match="lmm_mode"):
+            jamma_b200.gwas(tmp_path / "x", lmm_mode=9)
