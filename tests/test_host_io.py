@@ -77,3 +77,41 @@ def test_int8_code_layout():
     np.testing.assert_array_equal(codes, [[0, 2], [1, 3], [3, 1]])
     with pytest.raises(ValueError, match="allele counts"):
         jio.encode_codes(np.array([[0.5]]))
+
+
+def test_chromosome_partitions_keep_first_appearance_order():
+    from jamma_b200.loco import chromosome_partitions
+
+    parts = chromosome_partitions(["2", "2", "10", "1", "10", "2"])
+    assert list(parts) == ["2", "10", "1"]
+    np.testing.assert_array_equal(parts["2"], [0, 1, 5])
+    np.testing.assert_array_equal(parts["10"], [2, 4])
+    assert sorted(parts) == ["1", "10", "2"]  # the string order LOCO processes them in
+
+
+def test_eigen_warnings():
+    import warnings
+
+    from jamma_b200.eigen import _warn
+
+    with warnings.catch_warnings(record=True) as w:
+        warnings.simplefilter("always")
+        _warn(np.array([-1e-3, 0.0, 0.0, 1.0]), 1e-10)
+    msgs = [str(x.message) for x in w]
+    assert any("1 negative eigenvalue" in m for m in msgs)
+    assert any("2 eigenvalues close to zero" in m for m in msgs)
+    with warnings.catch_warnings(record=True) as w:
+        warnings.simplefilter("always")
+        _warn(np.array([0.0, 0.5, 1.0]), 1e-10)  # one zero eigenvalue: no warning
+    assert not w
+
+
+def test_autotune_cache_survives_a_corrupt_file(tmp_path, monkeypatch):
+    from jamma_b200 import autotune
+
+    monkeypatch.setenv("JAMMA_B200_CACHE", str(tmp_path / "t" / "tune.json"))
+    assert autotune._load() == {}
+    autotune._store({"k": {"chunk": 4096}})
+    assert autotune._load() == {"k": {"chunk": 4096}}
+    autotune.cache_path().write_text("{not json")
+    assert autotune._load() == {}
