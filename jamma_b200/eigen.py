@@ -36,10 +36,10 @@ def _warn(evals: np.ndarray, threshold: float) -> None:
 def eigendecompose_kinship(K: np.ndarray, threshold: float = 1e-10, *,
                            check_memory: bool = True) -> tuple[np.ndarray, np.ndarray]:
     """(eigenvalues ascending (n,), eigenvectors (n, n) as columns), FP64 on device."""
-    require_cuda()
     K = np.asarray(K, dtype=np.float64)
     if K.ndim != 2 or K.shape[0] != K.shape[1]:
         raise ValueError(f"Kinship matrix must be square, got shape {K.shape}")
+    require_cuda()
     # K is symmetric, so its row-major bytes are already the column-major layout.
     dk = torch.from_numpy(np.ascontiguousarray(K)).to("cuda")
     w, U = eigh_device(dk, threshold)

@@ -252,7 +252,6 @@ def run_lmm_association_streaming(
     ``use_gpu`` is accepted for signature compatibility: the computation always runs on
     the GPU.  ``timing`` (optional dict) receives per-stage seconds.
     """
-    require_cuda()
     t0 = time.perf_counter()
     if (eigenvalues is None) != (eigenvectors is None):
         raise ValueError(
@@ -264,7 +263,10 @@ def run_lmm_association_streaming(
                          "eigenvectors) must be provided")
     if lmm_mode not in (1, 2, 3, 4):
         raise ValueError(f"lmm_mode must be 1, 2, 3 or 4, got {lmm_mode}")
+    if precision not in ("fp64", "mixed"):
+        raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
     meta = get_plink_metadata(bed_path)
+    require_cuda()  # after the argument checks, so they raise as jamma's do on any host
     n_file, p = meta["n_samples"], meta["n_snps"]
     if snp_info is None:
         snp_info = snp_info_from_meta(meta)
@@ -315,11 +317,13 @@ def run_lmm_association_jax(
 ) -> list[AssocResult]:
     """In-memory genotype runner (runner_jax.py:52-481): statistics and imputation means
     in the genotype array's own dtype (float64 means for float64 input)."""
-    require_cuda()
     if (eigenvalues is None) != (eigenvectors is None):
         raise ValueError("Must provide both eigenvalues and eigenvectors, or neither.")
     if lmm_mode not in (1, 2, 3, 4):
         raise ValueError(f"lmm_mode must be 1, 2, 3 or 4, got {lmm_mode}")
+    if precision not in ("fp64", "mixed"):
+        raise ValueError(f"precision must be 'fp64' or 'mixed', got {precision!r}")
+    require_cuda()
     g = np.asarray(genotypes)
     y = np.asarray(phenotypes, dtype=np.float64)
     valid = valid_sample_mask(y, covariates)

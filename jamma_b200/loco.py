@@ -54,9 +54,9 @@ def compute_loco_kinship(bfile, maf_threshold: float = 0.0, miss_threshold: floa
                          chunk_size: int = 10000, precision: str = "int8",
                          ksnps_indices: np.ndarray | None = None):
     """Yield (chromosome, K_loco) device tensors (n x n, all samples), sorted by name."""
-    require_cuda()
     if precision not in ("int8", "fp64"):
         raise ValueError("precision must be 'int8' or 'fp64'")
+    require_cuda()
     meta = get_plink_metadata(bfile)
     chroms = np.asarray(meta["chromosome"]).astype(str)
     bed = BedFile(bfile, meta["n_samples"], meta["n_snps"])
@@ -125,7 +125,6 @@ def run_lmm_loco(bed_path, phenotypes: np.ndarray, covariates: np.ndarray | None
                  snps_indices: np.ndarray | None = None, ksnps_indices: np.ndarray | None = None,
                  precision: str = "fp64", kinship_precision: str = "int8") -> list[AssocResult]:
     """LOCO association; results in sorted-chromosome order (empty when written to disk)."""
-    require_cuda()
     if lmm_mode not in (1, 2, 3, 4):
         raise ValueError(f"lmm_mode must be 1, 2, 3 or 4, got {lmm_mode}")
     meta = get_plink_metadata(bed_path)
@@ -138,6 +137,7 @@ def run_lmm_loco(bed_path, phenotypes: np.ndarray, covariates: np.ndarray | None
     valid = valid_sample_mask(y, covariates)
     if not np.any(valid):
         raise ValueError("No samples with valid phenotypes")
+    require_cuda()  # after the argument and file checks, which raise as jamma's do
     n_file = meta["n_samples"]
     sample_idx = None if np.all(valid) else np.where(valid)[0].astype(np.int32)
     sidx = None if sample_idx is None else torch.from_numpy(sample_idx).cuda()

@@ -65,3 +65,31 @@ def test_package_gwas_can_be_called_repeatedly(tmp_path):
     for _ in range(2):
         with pytest.raises(ValueError, match="lmm_mode"):
             jamma_b200.gwas(tmp_path / "x", lmm_mode=9)
+
+
+def test_runner_argument_errors_come_before_the_device(tmp_path):
+    """The association runners and the eigendecomposition check their arguments first, so
+    a bad call raises jamma's ValueError (or FileNotFoundError) on any host."""
+    import numpy as np
+
+    from jamma_b200 import eigendecompose_kinship, run_lmm_association_jax
+    from jamma_b200 import run_lmm_association_streaming as stream
+    from jamma_b200.loco import run_lmm_loco
+
+    y = np.zeros(4)
+    with pytest.raises(ValueError, match="both eigenvalues and eigenvectors"):
+        stream(tmp_path / "x", y, eigenvalues=np.ones(4))
+    with pytest.raises(ValueError, match="Either kinship or pre-computed"):
+        stream(tmp_path / "x", y)
+    with pytest.raises(ValueError, match="lmm_mode"):
+        stream(tmp_path / "x", y, kinship=np.eye(4), lmm_mode=0)
+    with pytest.raises(ValueError, match="precision"):
+        stream(tmp_path / "x", y, kinship=np.eye(4), precision="bf16")
+    with pytest.raises(FileNotFoundError):
+        stream(tmp_path / "x", y, kinship=np.eye(4))
+    with pytest.raises(ValueError, match="lmm_mode"):
+        run_lmm_association_jax(np.zeros((4, 2)), y, np.eye(4), [], lmm_mode=7)
+    with pytest.raises(ValueError, match="square"):
+        eigendecompose_kinship(np.ones((3, 4)))
+    with pytest.raises(ValueError, match="lmm_mode"):
+        run_lmm_loco(tmp_path / "x", y, lmm_mode=5)
