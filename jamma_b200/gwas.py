@@ -66,6 +66,9 @@ def gwas(bfile, *, kinship_file=None, covariate_file=None, lmm_mode: int = 1, ma
     meta = get_plink_metadata(bfile)
     n = meta["n_samples"]
     y = read_phenotypes(bfile, phenotype_column)
+    n_analyzed = int(np.sum(~np.isnan(y) & (y != -9.0)))
+    if n_analyzed == 0:  # pipeline.py:286-291
+        raise ValueError("No samples with valid phenotypes")
     sid = list(meta["sid"])
     snps_idx = None
     if snps_file is not None:
@@ -82,7 +85,7 @@ def gwas(bfile, *, kinship_file=None, covariate_file=None, lmm_mode: int = 1, ma
     if loco:
         pass
     elif eigenvalue_file is not None:
-        evals, evecs = read_eigen_files(eigenvalue_file, eigenvector_file)
+        evals, evecs = read_eigen_files(eigenvalue_file, eigenvector_file, n_samples=n_analyzed)
     else:
         if kinship_file is not None:
             K = read_kinship_matrix(kinship_file, n_samples=n)

@@ -93,3 +93,22 @@ def test_runner_argument_errors_come_before_the_device(tmp_path):
         eigendecompose_kinship(np.ones((3, 4)))
     with pytest.raises(ValueError, match="lmm_mode"):
         run_lmm_loco(tmp_path / "x", y, lmm_mode=5)
+
+
+def test_gwas_file_checks_before_the_device(tmp_path):
+    """No valid phenotype, or eigen files of the wrong size, are errors before any device
+    work (jamma's pipeline.py:286-291 and its n_samples cross-check of the eigen files)."""
+    import numpy as np
+
+    from jamma_b200.gwas import gwas
+    from jamma_b200.io import write_eigen_files
+    from oracle import plink as OP
+
+    g = np.random.default_rng(0).binomial(2, 0.3, (6, 5)).astype(float)
+    OP.write_plink(tmp_path / "a", g, phenotypes=np.full(6, -9.0))
+    with pytest.raises(ValueError, match="No samples with valid phenotypes"):
+        gwas(tmp_path / "a", kinship_file=tmp_path / "k.cXX.txt")
+    OP.write_plink(tmp_path / "b", g, phenotypes=np.array([1.0, 2, np.nan, 4, 5, 6]))
+    d, u = write_eigen_files(np.ones(6), np.eye(6), tmp_path, "e")
+    with pytest.raises(ValueError, match="does not match expected"):
+        gwas(tmp_path / "b", eigenvalue_file=d, eigenvector_file=u)
