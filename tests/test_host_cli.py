@@ -112,3 +112,19 @@ def test_gwas_file_checks_before_the_device(tmp_path):
     d, u = write_eigen_files(np.ones(6), np.eye(6), tmp_path, "e")
     with pytest.raises(ValueError, match="does not match expected"):
         gwas(tmp_path / "b", eigenvalue_file=d, eigenvector_file=u)
+
+
+def test_no_cpu_fallback(tmp_path, monkeypatch):
+    """Without a CUDA device the product path raises instead of computing on the host."""
+    import numpy as np
+    import torch
+
+    from jamma_b200 import device
+    from jamma_b200.kinship import compute_centered_kinship
+
+    monkeypatch.setattr(device, "_checked", False)
+    monkeypatch.setattr(torch.cuda, "is_available", lambda: False)
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        device.require_cuda()
+    with pytest.raises(RuntimeError, match="no CPU fallback"):
+        compute_centered_kinship(np.zeros((4, 3)))
